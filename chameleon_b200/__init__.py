@@ -1,0 +1,320 @@
+"""chameleon_b200 -- B200-native tiled Cholesky (dposv) behind Chameleon's API.
+
+The compute lives in the in-tree CUDA library ``libchameleon_b200.so`` (C ABI,
+``include/chameleon_b200.h``).  This module is the Python host mirror of the
+reference's C interface (include/chameleon.h, include/chameleon/chameleon_z.h
+after z->d generation): same entry-point names, argument meaning, enum values
+and return codes.  There is no CPU fallback: importing works anywhere, but every
+compute call raises ``ChameleonError`` when the CUDA library is not built or no
+GPU is present.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libchameleon_b200.so")
+
+# include/chameleon/constants.h values
+ChamNoTrans, ChamTrans, ChamConjTrans = 111, 112, 113
+ChamUpper, ChamLower, ChamUpperLower = 121, 122, 123
+ChamNonUnit, ChamUnit = 131, 132
+ChamLeft, ChamRight = 141, 142
+ChamOneNorm, ChamFrobeniusNorm, ChamInfNorm, ChamMaxNorm = 171, 174, 175, 177
+ChamRealFloat, ChamRealDouble = (1 << 2) | 2, (1 << 2) | 3
+CHAMELEON_MAT_ALLOC_TILE = ctypes.c_void_p(-1 & 0xFFFFFFFFFFFFFFFF)
+CHAMELEON_TILE_SIZE = 2
+CHAMELEON_INNER_BLOCK_SIZE = 3
+CHAMELEON_B200_PRECISION = 101
+CHAMELEON_B200_REFINE_MAXITER = 102
+CHAMELEON_B200_WAIT_BUDGET_MS = 103
+CHAMELEON_B200_WAIT_BUDGET_US = 104
+PREC_FP64, PREC_FP32, PREC_BF16X3 = 0, 1, 2
+CHAMELEON_SUCCESS = 0
+CHAMELEON_ERR_NOT_INITIALIZED = -101
+CHAMELEON_ERR_ILLEGAL_VALUE = -104
+CHAMELEON_ERR_NOT_SUPPORTED = -103
+CHAMELEON_ERR_OUT_OF_RESOURCES = -106
+CHAMELEON_ERR_UNEXPECTED = -110
+CHAMELEON_ERR_DEVICE_TIMEOUT = -120
+
+
+class ChameleonError(RuntimeError):
+    pass
+
+
+class CHAM_desc_t(ctypes.Structure):
+    _fields_ = [
+        ("name", ctypes.c_char_p),
+        ("get_blkaddr", ctypes.c_void_p),
+        ("get_blkldd", ctypes.c_void_p),
+        ("tiles", ctypes.c_void_p),
+        ("mat", ctypes.c_void_p),
+        ("host_mat", ctypes.c_void_p),
+        ("A21", ctypes.c_size_t), ("A12", ctypes.c_size_t), ("A22", ctypes.c_size_t),
+        ("styp", ctypes.c_int), ("dtyp", ctypes.c_int),
+        ("mb", ctypes.c_int), ("nb", ctypes.c_int), ("bsiz", ctypes.c_int),
+        ("i", ctypes.c_int), ("j", ctypes.c_int), ("m", ctypes.c_int), ("n", ctypes.c_int),
+        ("lm", ctypes.c_int), ("ln", ctypes.c_int),
+        ("mt", ctypes.c_int), ("nt", ctypes.c_int), ("lmt", ctypes.c_int), ("lnt", ctypes.c_int),
+        ("llm1", ctypes.c_int), ("lln1", ctypes.c_int),
+        ("lda", ctypes.c_int), ("alloc_mat", ctypes.c_int), ("id", ctypes.c_int),
+        ("schedopt", ctypes.c_void_p),
+    ]
+
+
+class RefineInfo(ctypes.Structure):
+    _fields_ = [("iterations", ctypes.c_int), ("fallback", ctypes.c_int), ("precision", ctypes.c_int),
+                ("backward_error", ctypes.c_double), ("seconds", ctypes.c_double)]
+
+
+class Task(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int16), ("sub", ctypes.c_int16), ("m", ctypes.c_int16),
+                ("n", ctypes.c_int16), ("k", ctypes.c_int16), ("bn", ctypes.c_int16), ("pad", ctypes.c_int32)]
+
+
+_D = ctypes.POINTER(CHAM_desc_t)
+_dp = ctypes.POINTER(ctypes.c_double)
+_vp = ctypes.c_void_p
+_i = ctypes.c_int
+_ull = ctypes.c_ulonglong
+
+# name -> (restype, argtypes); every symbol declared in include/chameleon_b200.h
+PROTOS = {
+    "__chameleon_init": (_i, [_i, _i]),
+    "__chameleon_finalize": (_i, []),
+    "CHAMELEON_Initialized": (_i, []),
+    "CHAMELEON_Set": (_i, [_i, _i]),
+    "CHAMELEON_Get": (_i, [_i, ctypes.POINTER(_i)]),
+    "CHAMELEON_Enable": (_i, [_i]),
+    "CHAMELEON_Disable": (_i, [_i]),
+    "CHAMELEON_B200_Strerror": (ctypes.c_char_p, [_i]),
+    "CHAMELEON_Desc_Create": (_i, [ctypes.POINTER(_D), _vp, _i, _i, _i, _i, _i, _i, _i, _i, _i, _i, _i, _i]),
+    "CHAMELEON_Desc_Destroy": (_i, [ctypes.POINTER(_D)]),
+    "CHAMELEON_Desc_Flush": (_i, [_D, _vp]),
+    "CHAMELEON_Desc_Acquire": (_i, [_D]),
+    "CHAMELEON_Desc_Release": (_i, [_D]),
+    "CHAMELEON_Lap2Desc": (_i, [_i, _vp, _i, _D]),
+    "CHAMELEON_Desc2Lap": (_i, [_i, _D, _vp, _i]),
+    "CHAMELEON_Sequence_Create": (_i, [ctypes.POINTER(_vp)]),
+    "CHAMELEON_Sequence_Destroy": (_i, [_vp]),
+    "CHAMELEON_Sequence_Wait": (_i, [_vp]),
+    "CHAMELEON_dposv": (_i, [_i, _i, _i, _vp, _i, _vp, _i]),
+    "CHAMELEON_dposv_Tile": (_i, [_i, _D, _D]),
+    "CHAMELEON_dposv_Tile_Async": (_i, [_i, _D, _D, _vp, _vp]),
+    "CHAMELEON_dpotrf": (_i, [_i, _i, _vp, _i]),
+    "CHAMELEON_dpotrf_Tile": (_i, [_i, _D]),
+    "CHAMELEON_dpotrf_Tile_Async": (_i, [_i, _D, _vp, _vp]),
+    "CHAMELEON_dpotrs": (_i, [_i, _i, _i, _vp, _i, _vp, _i]),
+    "CHAMELEON_dpotrs_Tile": (_i, [_i, _D, _D]),
+    "CHAMELEON_dpotrs_Tile_Async": (_i, [_i, _D, _D, _vp, _vp]),
+    "CHAMELEON_dpotrf_batch_Tile": (_i, [_i, _D]),
+    "CHAMELEON_dtrsm_batch_Tile": (_i, [_i, _i, _i, _i, ctypes.c_double, _D, _D]),
+    "CHAMELEON_dplgsy": (_i, [ctypes.c_double, _i, _i, _vp, _i, _ull]),
+    "CHAMELEON_dplgsy_Tile": (_i, [ctypes.c_double, _i, _D, _ull]),
+    "CHAMELEON_dplrnt": (_i, [_i, _i, _vp, _i, _ull]),
+    "CHAMELEON_dplrnt_Tile": (_i, [_D, _ull]),
+    "CHAMELEON_dlansy_Tile": (ctypes.c_double, [_i, _i, _D]),
+    "CHAMELEON_dlange_Tile": (ctypes.c_double, [_i, _D]),
+    "CHAM_B200_Handle_Create": (_i, [ctypes.POINTER(_vp), _vp]),
+    "CHAM_B200_Handle_Destroy": (_i, [_vp]),
+    "CUDA_dgemm": (_i, [_i, _i, _i, _i, _i, _dp, _vp, _i, _vp, _i, _dp, _vp, _i, _vp]),
+    "CUDA_dsyrk": (_i, [_i, _i, _i, _i, _dp, _vp, _i, _dp, _vp, _i, _vp]),
+    "CUDA_dtrsm": (_i, [_i, _i, _i, _i, _i, _i, _dp, _vp, _i, _vp, _i, _vp]),
+    "CUDA_dpotrf": (_i, [_i, _i, _vp, _i, _vp, _i, _vp, _vp]),
+    "CUDA_dplgsy": (_i, [_dp, _i, _i, _vp, _i, _i, _i, _i, _ull, _vp]),
+    "CUDA_dplrnt": (_i, [_i, _i, _vp, _i, _i, _i, _i, _ull, _vp]),
+    "CUDA_dlag2s": (_i, [_i, _i, _vp, _i, _vp, _i, _vp]),
+    "CUDA_slag2d": (_i, [_i, _i, _vp, _i, _vp, _i, _vp]),
+    "CHAM_B200_dposv_batch": (_i, [_i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+}
+# library extras (not in the public header): tracing, schedule inspection, timing
+EXTRAS = {
+    "CHAM_B200_Handle_Overflow": (_i, [_vp]),
+    "CHAM_B200_Trace_Enable": (_i, [_i]),
+    "CHAM_B200_Trace_Read": (_i, [_vp, _i]),
+    "CHAM_B200_Schedule_Size": (_i, [_i, _i, _i, _i, _i, _i]),
+    "CHAM_B200_Schedule_Build": (_i, [_i, _i, _i, _i, _i, _i, ctypes.POINTER(Task), _i]),
+    "CHAM_B200_dposv_timed": (_i, [_i, _i, _i, _vp, _i, _vp, _i, ctypes.POINTER(ctypes.c_float)]),
+}
+
+_lib = None
+
+
+def lib():
+    """Load the CUDA library; raise if it is missing (no fallback path exists)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ChameleonError("libchameleon_b200.so is not built (run `python -m chameleon_b200.build`)")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in {**PROTOS, **EXTRAS}.items():
+            f = getattr(L, name, None)
+            if f is None:
+                continue
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def missing_symbols():
+    L = lib()
+    return [n for n in PROTOS if not hasattr(L, n)]
+
+
+def check(rc, what=""):
+    if rc != 0:
+        msg = lib().CHAMELEON_B200_Strerror(rc).decode()
+        raise ChameleonError("%s returned %d (%s)" % (what, rc, msg))
+    return rc
+
+
+_initialized = False
+
+
+def init(ncpus=0, ngpus=1):
+    """CHAMELEON_Init (idempotent here)."""
+    global _initialized
+    L = lib()
+    if L.CHAMELEON_Initialized():
+        _initialized = True
+        return 0
+    rc = L.__chameleon_init(ncpus, ngpus)
+    if rc != 0:
+        raise ChameleonError("CHAMELEON_Init failed (%d): no usable CUDA device" % rc)
+    _initialized = True
+    return 0
+
+
+def finalize():
+    global _initialized
+    if _initialized:
+        lib().__chameleon_finalize()
+        _initialized = False
+
+
+def set_param(param, value):
+    return check(lib().CHAMELEON_Set(param, value), "CHAMELEON_Set")
+
+
+def get_param(param):
+    v = ctypes.c_int()
+    check(lib().CHAMELEON_Get(param, ctypes.byref(v)), "CHAMELEON_Get")
+    return v.value
+
+
+def _addr(x):
+    """Device/host address of a torch tensor or numpy array (column-major storage expected)."""
+    if hasattr(x, "data_ptr"):
+        return ctypes.c_void_p(x.data_ptr())
+    return ctypes.c_void_p(x.ctypes.data)
+
+
+class Desc:
+    """Owning wrapper of a CHAM_desc_t* (CHAMELEON_Desc_Create / Destroy)."""
+
+    def __init__(self, ptr, keep=None):
+        self.ptr = ptr
+        self._keep = keep
+
+    @classmethod
+    def create(cls, m, n, mb, nb=None, dtyp=ChamRealDouble, mat=None):
+        nb = mb if nb is None else nb
+        init()
+        p = _D()
+        matp = CHAMELEON_MAT_ALLOC_TILE if mat is None else _addr(mat)
+        check(lib().CHAMELEON_Desc_Create(ctypes.byref(p), matp, dtyp, mb, nb, mb * nb, m, n, 0, 0, m, n, 1, 1),
+              "CHAMELEON_Desc_Create")
+        return cls(p, keep=mat)
+
+    @property
+    def d(self):
+        return self.ptr.contents
+
+    def destroy(self):
+        if self.ptr:
+            lib().CHAMELEON_Desc_Destroy(ctypes.byref(self.ptr))
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+    def to_numpy(self, uplo=ChamUpperLower):
+        d = self.d
+        A = np.zeros((d.m, d.n), order="F")
+        check(lib().CHAMELEON_Desc2Lap(uplo, self.ptr, _addr(A), max(d.m, 1)), "CHAMELEON_Desc2Lap")
+        return A
+
+    def from_numpy(self, A, uplo=ChamUpperLower):
+        A = np.asfortranarray(A, dtype=np.float64)
+        check(lib().CHAMELEON_Lap2Desc(uplo, _addr(A), max(A.shape[0], 1), self.ptr), "CHAMELEON_Lap2Desc")
+
+
+# ---- reference-named entry points --------------------------------------------
+
+def dplgsy_Tile(bump, uplo, A, seed):
+    return lib().CHAMELEON_dplgsy_Tile(bump, uplo, A.ptr, seed)
+
+
+def dplrnt_Tile(A, seed):
+    return lib().CHAMELEON_dplrnt_Tile(A.ptr, seed)
+
+
+def dposv_Tile(uplo, A, B):
+    return lib().CHAMELEON_dposv_Tile(uplo, A.ptr, B.ptr)
+
+
+def dpotrf_Tile(uplo, A):
+    return lib().CHAMELEON_dpotrf_Tile(uplo, A.ptr)
+
+
+def dpotrs_Tile(uplo, A, B):
+    return lib().CHAMELEON_dpotrs_Tile(uplo, A.ptr, B.ptr)
+
+
+def dlansy_Tile(norm, uplo, A):
+    return lib().CHAMELEON_dlansy_Tile(norm, uplo, A.ptr)
+
+
+def dposv(uplo, N, NRHS, A, LDA, B, LDB):
+    """CHAMELEON_dposv on caller arrays (numpy host arrays or torch CUDA tensors, column-major)."""
+    init()
+    return lib().CHAMELEON_dposv(uplo, N, NRHS, _addr(A), LDA, _addr(B), LDB)
+
+
+def dpotrf(uplo, N, A, LDA):
+    init()
+    return lib().CHAMELEON_dpotrf(uplo, N, _addr(A), LDA)
+
+
+def dpotrs(uplo, N, NRHS, A, LDA, B, LDB):
+    init()
+    return lib().CHAMELEON_dpotrs(uplo, N, NRHS, _addr(A), LDA, _addr(B), LDB)
+
+
+def dplgsy(bump, uplo, N, A, LDA, seed):
+    init()
+    return lib().CHAMELEON_dplgsy(bump, uplo, N, _addr(A), LDA, seed)
+
+
+def dplrnt(M, N, A, LDA, seed):
+    init()
+    return lib().CHAMELEON_dplrnt(M, N, _addr(A), LDA, seed)
+
+
+def schedule(mode, N, NB, nrhs=0, NBB=None, workers=148):
+    """The executor's task list for a shape (host-only; no GPU needed)."""
+    L = lib()
+    NBB = NB if NBB is None else NBB
+    n = L.CHAM_B200_Schedule_Size(mode, N, NB, nrhs, NBB, workers)
+    buf = (Task * max(n, 1))()
+    got = L.CHAM_B200_Schedule_Build(mode, N, NB, nrhs, NBB, workers, buf, n)
+    if got != n:
+        raise ChameleonError("schedule build returned %d of %d" % (got, n))
+    arr = np.frombuffer(buf, dtype=np.int16).reshape(-1, 8)[:n]
+    return arr[:, :6].copy()   # kind, sub, m, n, k, bn

@@ -1,0 +1,590 @@
+// executor.cu -- persistent tile-DAG executor of the Cholesky factor/solve.
+//
+// Host side: record the sub-tile task DAG of chameleon_pdpotrf (compute/
+// pzpotrf.c:84-194) and of the two chameleon_pdtrsm solves of dpotrs
+// (compute/zpotrs.c:302-304 -> compute/pztrsm.c:58-200), order it by a
+// list-scheduling simulation with critical-path priorities (the reference's
+// task priorities `2*mt - 2*k - n - m`, compute/pzpotrf.c:90-124, play the same
+// role for StarPU), cache it per shape, and launch one persistent kernel.
+// Device side: dispatch by atomic cursor, bounded waits on per-tile counters,
+// tile operations from core.cuh, release by red.release.
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <memory>
+#include <queue>
+#include <unordered_map>
+#include <cstring>
+
+#include "core.cuh"
+#include "internal.h"
+
+namespace chb {
+
+// ---------------------------------------------------------------------------
+// Device
+// ---------------------------------------------------------------------------
+struct Dims {
+    const ExecParams &p;
+    __device__ int tm(int m) const { return (m == p.NT - 1) ? p.N - m * p.NB : p.NB; }
+    __device__ int nbi(int m) const { return (tm(m) + SUBB - 1) / SUBB; }
+    __device__ int S(int m, int n) const {
+        const int a = nbi(m), b = nbi(n);
+        return (m == n) ? a * (a + 1) / 2 : a * b;
+    }
+    __device__ int wB(int bn) const { return (bn == p.NTB - 1) ? p.nrhs - bn * p.NBB : p.NBB; }
+    // Logical lower tile (m,n), m >= n.
+    __device__ View A(int m, int n) const {
+        if (!p.upper) return View{p.A + p.a_off[m + p.NT * n], 1, p.a_ld[m]};
+        return View{p.A + p.a_off[n + p.NT * m], p.a_ld[n], 1};
+    }
+    __device__ View Bt(int m, int bn) const { return View{p.B + p.b_off[m + p.NT * bn], 1, p.b_ld[m]}; }
+    __device__ double *inv(int k) const { return p.invd + (int64_t)k * p.NIB * IB * IB; }
+};
+
+// Thread 0 only.  Returns false when the run aborted or the wait ran out.
+__device__ bool wait_geq(const int *ctr, int target, const ExecParams &p, int task) {
+    if (ld_acquire(ctr) >= target) return true;
+    const uint64_t t0 = globaltimer();
+    unsigned ns = 32;
+    while (true) {
+        if (ld_acquire(ctr) >= target) return true;
+        if (*(volatile int *)&p.st->abort) return false;
+        if (globaltimer() - t0 > p.wait_budget_ns) {
+            atomicCAS(&p.st->error, 0, CHAMELEON_ERR_DEVICE_TIMEOUT);
+            atomicExch(&p.st->stuck_task, task);
+            atomicExch(&p.st->abort, 1);
+            return false;
+        }
+        __nanosleep(ns);
+        if (ns < 1024) ns <<= 1;
+    }
+}
+
+__device__ bool task_wait(const Task &t, const ExecParams &p, const Dims &d, int ti) {
+    const bool fact = p.mode & MODE_FACT;
+    switch (t.kind) {
+    case TK_POTRF:
+        return wait_geq(&p.updA[t.k + p.NT * t.k], t.k * d.S(t.k, t.k), p, ti);
+    case TK_TRSM:
+        return wait_geq(&p.panA[t.k + p.NT * t.k], 1, p, ti) &&
+               wait_geq(&p.updA[t.m + p.NT * t.k], t.k * d.S(t.m, t.k), p, ti);
+    case TK_UPD:
+        return wait_geq(&p.panA[t.m + p.NT * t.k], d.nbi(t.m), p, ti) &&
+               wait_geq(&p.panA[t.n + p.NT * t.k], d.nbi(t.n), p, ti) &&
+               wait_geq(&p.updA[t.m + p.NT * t.n], t.k * d.S(t.m, t.n), p, ti);
+    case TK_INV:
+        return true;
+    case TK_FWD_TRSM:
+        return wait_geq(&p.panA[t.k + p.NT * t.k], 1, p, ti) &&
+               wait_geq(&p.fwdB[t.k + p.NT * t.bn], t.k * d.nbi(t.k), p, ti);
+    case TK_FWD_UPD:
+        return wait_geq(&p.fwdDone[t.k + p.NT * t.bn], 1, p, ti) &&
+               (!fact || wait_geq(&p.panA[t.m + p.NT * t.k], d.nbi(t.m), p, ti)) &&
+               wait_geq(&p.fwdB[t.m + p.NT * t.bn], t.k * d.nbi(t.m), p, ti);
+    case TK_BWD_TRSM:
+        return wait_geq(&p.fwdDone[t.k + p.NT * t.bn], 1, p, ti) &&
+               wait_geq(&p.bwdB[t.k + p.NT * t.bn], (p.NT - 1 - t.k) * d.nbi(t.k), p, ti);
+    case TK_BWD_UPD:
+        return wait_geq(&p.bwdDone[t.k + p.NT * t.bn], 1, p, ti) &&
+               wait_geq(&p.bwdB[t.m + p.NT * t.bn], (p.NT - 1 - t.k) * d.nbi(t.m), p, ti);
+    }
+    return false;
+}
+
+// Invert the inner diagonal blocks of an existing factor L(k,k) (potrs alone).
+__device__ void tile_inv(const View &T, int n, double *invd, double *smem, int *flag) {
+    double *sD = smem + Cfg12864::SMEM_ELEMS;
+    double *sInv = sD + IB * LDD;
+    for (int jb = 0; jb < n; jb += IB) {
+        const int nbk = min(IB, n - jb);
+        for (int idx = threadIdx.x; idx < nbk * nbk; idx += NT_CTA) {
+            const int r = idx % nbk, c = idx / nbk;
+            if (r >= c) sD[r + c * LDD] = *T.at(jb + r, jb + c);
+        }
+        __syncthreads();
+        blk_inv(sD, sInv, nbk);
+        store_inv(invd + (int64_t)(jb / IB) * IB * IB, sInv);
+        __syncthreads();
+    }
+    (void)flag;
+}
+
+__device__ void run_task(const Task &t, const ExecParams &p, const Dims &d, double *smem, int *flag) {
+    switch (t.kind) {
+    case TK_POTRF: {
+        const int info = tile_potrf(d.A(t.k, t.k), d.tm(t.k), d.inv(t.k), smem);
+        if (info && threadIdx.x == 0) {
+            atomicMin(&p.st->info, t.k * p.NB + info);
+            atomicExch(&p.st->abort, 1);
+        }
+        break;
+    }
+    case TK_INV:
+        tile_inv(d.A(t.k, t.k), d.tm(t.k), d.inv(t.k), smem, flag);
+        break;
+    case TK_TRSM: {
+        const int r0 = t.sub * SUBB;
+        const int rows = min(SUBB, d.tm(t.m) - r0);
+        trsm_rows(d.A(t.m, t.k).sub(r0, 0), rows, d.A(t.k, t.k), d.tm(t.k), d.inv(t.k), smem);
+        break;
+    }
+    case TK_UPD: {
+        const int bi = t.sub & 0xff, bj = (t.sub >> 8) & 0xff;
+        const int rows = min(SUBB, d.tm(t.m) - bi * SUBB), cols = min(SUBB, d.tm(t.n) - bj * SUBB);
+        const View C = d.A(t.m, t.n).sub(bi * SUBB, bj * SUBB);
+        Acc<Cfg128> acc;
+        acc.zero();
+        cta_gemm(acc, d.A(t.m, t.k).sub(bi * SUBB, 0), d.A(t.n, t.k).sub(bj * SUBB, 0), rows, cols,
+                 d.tm(t.k), smem);
+        const bool diag = (t.m == t.n) && (bi == bj);
+        acc.for_each([&](int r, int c, double v) {
+            if (r < rows && c < cols && (!diag || r >= c)) *C.at(r, c) -= v;
+        });
+        break;
+    }
+    case TK_FWD_TRSM:
+    case TK_BWD_TRSM: {
+        const View X = d.Bt(t.k, t.bn);
+        const int w = d.wB(t.bn);
+        for (int c0 = 0; c0 < w; c0 += IB)
+            trsm_left(X.sub(0, c0), min(IB, w - c0), d.A(t.k, t.k), d.tm(t.k), d.inv(t.k),
+                      t.kind == TK_BWD_TRSM, smem);
+        break;
+    }
+    case TK_FWD_UPD:
+    case TK_BWD_UPD: {
+        const int r0 = t.sub * SUBB;
+        const int rows = min(SUBB, d.tm(t.m) - r0);
+        const int w = d.wB(t.bn);
+        const View Bm = d.Bt(t.m, t.bn).sub(r0, 0);
+        const View Bk = d.Bt(t.k, t.bn);
+        const View L = (t.kind == TK_FWD_UPD) ? d.A(t.m, t.k).sub(r0, 0) : d.A(t.k, t.m).t().sub(r0, 0);
+        for (int c0 = 0; c0 < w; c0 += 64) {
+            const int wc = min(64, w - c0);
+            Acc<Cfg12864> acc;
+            acc.zero();
+            cta_gemm(acc, L, Bk.sub(0, c0).t(), rows, wc, d.tm(t.k), smem);
+            const View Bc = Bm.sub(0, c0);
+            acc.for_each([&](int r, int c, double v) {
+                if (r < rows && c < wc) *Bc.at(r, c) -= v;
+            });
+        }
+        break;
+    }
+    }
+}
+
+__device__ int *task_counter(const Task &t, const ExecParams &p) {
+    switch (t.kind) {
+    case TK_POTRF:
+    case TK_INV: return &p.panA[t.k + p.NT * t.k];
+    case TK_TRSM: return &p.panA[t.m + p.NT * t.k];
+    case TK_UPD: return &p.updA[t.m + p.NT * t.n];
+    case TK_FWD_TRSM: return &p.fwdDone[t.k + p.NT * t.bn];
+    case TK_FWD_UPD: return &p.fwdB[t.m + p.NT * t.bn];
+    case TK_BWD_TRSM: return &p.bwdDone[t.k + p.NT * t.bn];
+    case TK_BWD_UPD: return &p.bwdB[t.m + p.NT * t.bn];
+    }
+    return nullptr;
+}
+
+__global__ void __launch_bounds__(NT_CTA, 1) cholesky_dag_kernel(ExecParams p) {
+    extern __shared__ __align__(128) double smem[];
+    __shared__ int s_task;
+    __shared__ int s_ok;
+    __shared__ int s_flag;
+    const Dims d{p};
+    while (true) {
+        if (threadIdx.x == 0) {
+            int ti = -1;
+            if (!*(volatile int *)&p.st->abort) {
+                ti = atomicAdd(&p.st->next, 1);
+                if (ti >= p.ntasks) ti = -1;
+            }
+            s_task = ti;
+            s_ok = (ti >= 0) ? (int)task_wait(p.tasks[ti], p, d, ti) : 0;
+        }
+        __syncthreads();
+        const int ti = s_task;
+        if (ti < 0 || !s_ok) break;
+        __threadfence();
+        const Task t = p.tasks[ti];
+        uint64_t t0 = 0;
+        if (p.trace && threadIdx.x == 0) t0 = globaltimer();
+        run_task(t, p, d, smem, &s_flag);
+        __threadfence();
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            red_release_add(task_counter(t, p), 1);
+            atomicAdd(&p.st->done, 1);
+            if (p.trace) {
+                unsigned smid;
+                asm volatile("mov.u32 %0, %%smid;\n" : "=r"(smid));
+                p.trace[ti] = TraceRec{ti, (int)smid, t0, globaltimer()};
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Host: DAG recording and list-scheduling order
+// ---------------------------------------------------------------------------
+namespace {
+
+struct Shape {
+    int mode, N, NB, nrhs, NBB, P;
+    bool operator==(const Shape &o) const {
+        return mode == o.mode && N == o.N && NB == o.NB && nrhs == o.nrhs && NBB == o.NBB && P == o.P;
+    }
+};
+struct ShapeHash {
+    size_t operator()(const Shape &s) const {
+        size_t h = 1469598103934665603ull;
+        for (int v : {s.mode, s.N, s.NB, s.nrhs, s.NBB, s.P}) h = (h ^ (size_t)v) * 1099511628211ull;
+        return h;
+    }
+};
+
+struct Coarse {
+    int16_t kind, m, n, k, bn;
+    int nsub;
+    double dur;               // duration of one sub-task (model units)
+    std::vector<int> succ;
+    int npred = 0;
+    double blevel = 0;
+};
+
+struct Schedule {
+    std::vector<Task> tasks;
+    Task *d_tasks = nullptr;
+};
+
+std::vector<Task> build_order(const Shape &s) {
+    const int NT = (s.N + s.NB - 1) / s.NB;
+    const int NTB = s.nrhs > 0 ? (s.nrhs + s.NBB - 1) / s.NBB : 0;
+    auto tm = [&](int m) { return (m == NT - 1) ? s.N - m * s.NB : s.NB; };
+    auto nbi = [&](int m) { return (tm(m) + SUBB - 1) / SUBB; };
+    auto wB = [&](int bn) { return (bn == NTB - 1) ? s.nrhs - bn * s.NBB : s.NBB; };
+    const bool fact = s.mode & MODE_FACT, solve = s.mode & MODE_SOLVE;
+
+    std::vector<Coarse> ct;
+    ct.reserve(fact ? (size_t)NT * NT * NT / 6 + 4 * NT * NT : 4 * NT * NT + 8);
+    auto add = [&](int kind, int m, int n, int k, int bn, int nsub, double dur) {
+        Coarse c;
+        c.kind = kind; c.m = m; c.n = n; c.k = k; c.bn = bn; c.nsub = nsub; c.dur = dur;
+        ct.push_back(c);
+        return (int)ct.size() - 1;
+    };
+    auto edge = [&](int a, int b) {
+        if (a < 0 || b < 0) return;
+        ct[a].succ.push_back(b);
+        ct[b].npred++;
+    };
+    // ids: potrf[k], trsm[m,k], upd[m,n,k] (last update of tile (m,n) so far)
+    std::vector<int> P(NT, -1), Tr((size_t)NT * NT, -1), lastU((size_t)NT * NT, -1);
+    const double nb = s.NB;
+    if (fact) {
+        for (int k = 0; k < NT; ++k) {
+            const double tk = tm(k);
+            P[k] = add(TK_POTRF, k, k, k, 0, 1, 6.0 * tk * tk * tk / 3.0);
+            edge(lastU[k + (size_t)NT * k], P[k]);
+            for (int m = k + 1; m < NT; ++m) {
+                const int id = add(TK_TRSM, m, k, k, 0, nbi(m), 2.0 * SUBB * nb * nb);
+                edge(P[k], id);
+                edge(lastU[m + (size_t)NT * k], id);
+                Tr[m + (size_t)NT * k] = id;
+            }
+            for (int n = k + 1; n < NT; ++n) {
+                for (int m = n; m < NT; ++m) {
+                    const int sub = (m == n) ? nbi(m) * (nbi(m) + 1) / 2 : nbi(m) * nbi(n);
+                    const int id = add(TK_UPD, m, n, k, 0, sub, 1.0 * SUBB * SUBB * nb * 2.0);
+                    edge(Tr[m + (size_t)NT * k], id);
+                    if (m != n) edge(Tr[n + (size_t)NT * k], id);
+                    edge(lastU[m + (size_t)NT * n], id);
+                    lastU[m + (size_t)NT * n] = id;
+                }
+            }
+        }
+    } else if (solve) {
+        for (int k = 0; k < NT; ++k) P[k] = add(TK_INV, k, k, k, 0, 1, 1.0 * tm(k) * IB * IB);
+    }
+    if (solve) {
+        std::vector<int> F((size_t)NT * NTB, -1), lastFU((size_t)NT * NTB, -1);
+        std::vector<int> Bk((size_t)NT * NTB, -1), lastBU((size_t)NT * NTB, -1);
+        for (int bn = 0; bn < NTB; ++bn) {
+            const double w = wB(bn);
+            for (int k = 0; k < NT; ++k) {
+                const int f = add(TK_FWD_TRSM, k, k, k, bn, 1, 3.0 * tm(k) * tm(k) * w);
+                edge(P[k], f);
+                edge(lastFU[k + (size_t)NT * bn], f);
+                F[k + (size_t)NT * bn] = f;
+                for (int m = k + 1; m < NT; ++m) {
+                    const int u = add(TK_FWD_UPD, m, k, k, bn, nbi(m), 2.0 * SUBB * tm(k) * w);
+                    edge(f, u);
+                    if (fact) edge(Tr[m + (size_t)NT * k], u);
+                    edge(lastFU[m + (size_t)NT * bn], u);
+                    lastFU[m + (size_t)NT * bn] = u;
+                }
+            }
+            for (int k = NT - 1; k >= 0; --k) {
+                const int b = add(TK_BWD_TRSM, k, k, k, bn, 1, 3.0 * tm(k) * tm(k) * w);
+                edge(F[k + (size_t)NT * bn], b);
+                edge(lastBU[k + (size_t)NT * bn], b);
+                Bk[k + (size_t)NT * bn] = b;
+                for (int m = k - 1; m >= 0; --m) {
+                    const int u = add(TK_BWD_UPD, m, k, k, bn, nbi(m), 2.0 * SUBB * tm(k) * w);
+                    edge(b, u);
+                    edge(lastBU[m + (size_t)NT * bn], u);
+                    lastBU[m + (size_t)NT * bn] = u;
+                }
+            }
+        }
+    }
+    // bottom levels (generation order is topological)
+    for (int i = (int)ct.size() - 1; i >= 0; --i) {
+        double b = 0;
+        for (int sidx : ct[i].succ) b = std::max(b, ct[sidx].blevel);
+        ct[i].blevel = b + ct[i].dur;
+    }
+    // list scheduling on s.P workers
+    struct Ready {
+        double prio; int id;
+        bool operator<(const Ready &o) const { return prio < o.prio || (prio == o.prio && id > o.id); }
+    };
+    struct Fin {
+        double t; int id;
+        bool operator<(const Fin &o) const { return t > o.t; }
+    };
+    std::priority_queue<Ready> ready;
+    std::priority_queue<Fin> running;
+    std::vector<int> started(ct.size(), 0), finished(ct.size(), 0);
+    for (int i = 0; i < (int)ct.size(); ++i)
+        if (ct[i].npred == 0) ready.push({ct[i].blevel, i});
+    std::vector<Task> out;
+    size_t total = 0;
+    for (auto &c : ct) total += c.nsub;
+    out.reserve(total);
+    int free_w = s.P;
+    double now = 0;
+    auto emit = [&](const Coarse &c, int j) {
+        Task t{};
+        t.kind = c.kind; t.m = c.m; t.n = c.n; t.k = c.k; t.bn = c.bn; t.sub = 0;
+        if (c.kind == TK_UPD) {
+            const int a = nbi(c.m);
+            int bi = 0, bj = 0;
+            if (c.m == c.n) {   // j-th lower sub-block (row-major over bi >= bj)
+                int rem = j;
+                bi = 0;
+                while (rem > bi) { rem -= bi + 1; ++bi; }
+                bj = rem;
+            } else {
+                bi = j / nbi(c.n);
+                bj = j % nbi(c.n);
+            }
+            (void)a;
+            t.sub = (int16_t)(bi | (bj << 8));
+        } else if (c.kind == TK_TRSM || c.kind == TK_FWD_UPD || c.kind == TK_BWD_UPD) {
+            t.sub = (int16_t)j;
+        }
+        out.push_back(t);
+    };
+    while (out.size() < total) {
+        while (free_w > 0 && !ready.empty()) {
+            const int id = ready.top().id;
+            Coarse &c = ct[id];
+            emit(c, started[id]);
+            started[id]++;
+            if (started[id] == c.nsub) ready.pop();
+            running.push({now + c.dur, id});
+            --free_w;
+        }
+        if (running.empty()) break;   // cannot happen for a well-formed DAG
+        const Fin f = running.top();
+        running.pop();
+        now = f.t;
+        ++free_w;
+        if (++finished[f.id] == ct[f.id].nsub) {
+            for (int sidx : ct[f.id].succ)
+                if (--ct[sidx].npred == 0) ready.push({ct[sidx].blevel, sidx});
+        }
+    }
+    return out;
+}
+
+std::mutex g_sched_mu;
+std::unordered_map<Shape, std::unique_ptr<Schedule>, ShapeHash> g_sched;
+
+Schedule *get_schedule(const Shape &s) {
+    std::lock_guard<std::mutex> lk(g_sched_mu);
+    auto it = g_sched.find(s);
+    if (it != g_sched.end()) return it->second.get();
+    auto sch = std::make_unique<Schedule>();
+    sch->tasks = build_order(s);
+    if (!sch->tasks.empty()) {
+        if (cudaMalloc(&sch->d_tasks, sch->tasks.size() * sizeof(Task)) != cudaSuccess) return nullptr;
+        if (cudaMemcpy(sch->d_tasks, sch->tasks.data(), sch->tasks.size() * sizeof(Task),
+                       cudaMemcpyHostToDevice) != cudaSuccess)
+            return nullptr;
+    }
+    Schedule *raw = sch.get();
+    g_sched[s] = std::move(sch);
+    return raw;
+}
+
+// Per-shape device workspace (counters, inverted blocks, state).
+struct Workspace {
+    size_t ctr_bytes = 0, inv_bytes = 0;
+    void *ctr = nullptr;
+    double *inv = nullptr;
+    ExecState *st = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+};
+Workspace g_ws;
+
+int ensure_ws(size_t ctr_bytes, size_t inv_bytes) {
+    if (!g_ws.st) {
+        CHB_CUDA(cudaMalloc(&g_ws.st, sizeof(ExecState)));
+        CHB_CUDA(cudaEventCreate(&g_ws.e0));
+        CHB_CUDA(cudaEventCreate(&g_ws.e1));
+    }
+    if (ctr_bytes > g_ws.ctr_bytes) {
+        if (g_ws.ctr) cudaFree(g_ws.ctr);
+        g_ws.ctr = nullptr;
+        CHB_CUDA(cudaMalloc(&g_ws.ctr, ctr_bytes));
+        g_ws.ctr_bytes = ctr_bytes;
+    }
+    if (inv_bytes > g_ws.inv_bytes) {
+        if (g_ws.inv) cudaFree(g_ws.inv);
+        g_ws.inv = nullptr;
+        CHB_CUDA(cudaMalloc(&g_ws.inv, inv_bytes));
+        g_ws.inv_bytes = inv_bytes;
+    }
+    return 0;
+}
+
+}  // namespace
+
+TraceRec *g_trace_buf = nullptr;   // set by the tracing entry point (host-owned device buffer)
+int g_trace_cap = 0;
+
+int run_cholesky_dag(int mode, cham_uplo_t uplo, CHAM_desc_t *A, CHAM_desc_t *B, cudaStream_t s,
+                     ExecResult *res) {
+    Context &c = ctx();
+    const int N = A->n;
+    const int NB = A->nb;
+    const int NT = A->nt;
+    const int nrhs = (B && (mode & MODE_SOLVE)) ? B->n : 0;
+    const int NBB = B ? B->nb : NB;
+    const int NTB = nrhs ? B->nt : 0;
+    res->info = 0; res->error = 0; res->ms = 0.f;
+    if (N == 0) return 0;
+    static int smem_set = 0;
+    if (!smem_set) {
+        CHB_CUDA(cudaFuncSetAttribute(cholesky_dag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)TILE_KERNEL_SMEM_BYTES));
+        smem_set = 1;
+    }
+    const int grid = c.num_sms;
+    Shape sh{mode, N, NB, nrhs, NBB, grid};
+    Schedule *sch = get_schedule(sh);
+    if (!sch) return CHAMELEON_ERR_OUT_OF_RESOURCES;
+    const int NIB = (NB + IB - 1) / IB;
+    const size_t nctr = (size_t)2 * NT * NT + (size_t)4 * NT * std::max(NTB, 1);
+    int rc = ensure_ws(nctr * sizeof(int), (size_t)NT * NIB * IB * IB * sizeof(double));
+    if (rc) return rc;
+    int rcA = desc_upload(A);
+    if (rcA) return rcA;
+    if (nrhs) {
+        int rcB = desc_upload(B);
+        if (rcB) return rcB;
+    }
+    ExecParams p{};
+    p.tasks = sch->d_tasks;
+    p.ntasks = (int)sch->tasks.size();
+    p.mode = mode;
+    p.upper = (uplo == ChamUpper);
+    p.NT = NT; p.N = N; p.NB = NB;
+    p.A = (double *)A->mat;
+    p.a_off = priv(A)->dev.off;
+    p.a_ld = priv(A)->dev.ld;
+    p.NTB = NTB; p.nrhs = nrhs; p.NBB = NBB;
+    p.B = nrhs ? (double *)B->mat : nullptr;
+    p.b_off = nrhs ? priv(B)->dev.off : nullptr;
+    p.b_ld = nrhs ? priv(B)->dev.ld : nullptr;
+    int *ctr = (int *)g_ws.ctr;
+    p.updA = ctr;
+    p.panA = ctr + (size_t)NT * NT;
+    const size_t nb4 = (size_t)NT * std::max(NTB, 1);
+    p.fwdB = ctr + (size_t)2 * NT * NT;
+    p.fwdDone = p.fwdB + nb4;
+    p.bwdB = p.fwdDone + nb4;
+    p.bwdDone = p.bwdB + nb4;
+    p.invd = g_ws.inv;
+    p.NIB = NIB;
+    p.st = g_ws.st;
+    p.trace = (g_trace_buf && g_trace_cap >= p.ntasks) ? g_trace_buf : nullptr;
+    p.wait_budget_ns = (unsigned long long)c.wait_budget_us * 1000ull;
+    ExecState init{};
+    init.info = INT_MAX;
+    init.stuck_task = -1;
+    CHB_CUDA(cudaMemsetAsync(ctr, 0, nctr * sizeof(int), s));
+    CHB_CUDA(cudaMemcpyAsync(g_ws.st, &init, sizeof(init), cudaMemcpyHostToDevice, s));
+    CHB_CUDA(cudaEventRecord(g_ws.e0, s));
+    if (p.ntasks > 0)
+        cholesky_dag_kernel<<<grid, NT_CTA, TILE_KERNEL_SMEM_BYTES, s>>>(p);
+    CHB_CUDA(cudaGetLastError());
+    CHB_CUDA(cudaEventRecord(g_ws.e1, s));
+    ExecState out{};
+    CHB_CUDA(cudaMemcpyAsync(&out, g_ws.st, sizeof(out), cudaMemcpyDeviceToHost, s));
+    CHB_CUDA(cudaStreamSynchronize(s));
+    CHB_CUDA(cudaEventElapsedTime(&res->ms, g_ws.e0, g_ws.e1));
+    res->info = (out.info == INT_MAX) ? 0 : out.info;
+    res->error = out.error;
+    if (out.error) {
+        char msg[160];
+        snprintf(msg, sizeof msg, "device wait budget exhausted at task %d (%d of %d done)",
+                 out.stuck_task, out.done, p.ntasks);
+        warning("run_cholesky_dag", msg);
+    }
+    return 0;
+}
+
+}  // namespace chb
+
+// Trace hooks (tracing subsystem): size the per-task trace buffer, read it back.
+extern "C" int CHAM_B200_Trace_Enable(int capacity) {
+    using namespace chb;
+    if (g_trace_buf) { cudaFree(g_trace_buf); g_trace_buf = nullptr; g_trace_cap = 0; }
+    if (capacity <= 0) return 0;
+    if (cudaMalloc(&g_trace_buf, (size_t)capacity * sizeof(TraceRec)) != cudaSuccess) {
+        g_trace_buf = nullptr;
+        return CHAMELEON_ERR_OUT_OF_RESOURCES;
+    }
+    cudaMemset(g_trace_buf, 0, (size_t)capacity * sizeof(TraceRec));
+    g_trace_cap = capacity;
+    return 0;
+}
+extern "C" int CHAM_B200_Trace_Read(void *host_out, int count) {
+    using namespace chb;
+    if (!g_trace_buf || count > g_trace_cap) return CHAMELEON_ERR_ILLEGAL_VALUE;
+    return cudaMemcpy(host_out, g_trace_buf, (size_t)count * sizeof(TraceRec), cudaMemcpyDeviceToHost) ==
+                   cudaSuccess
+               ? 0
+               : CHAMELEON_ERR_UNEXPECTED;
+}
+// Copy the schedule of a shape into `out` (host only; used by the CPU tests of
+// the DAG logic and by the trace tooling).  Returns the task count written.
+extern "C" int CHAM_B200_Schedule_Build(int mode, int N, int NB, int nrhs, int NBB, int workers, void *out,
+                                        int cap) {
+    using namespace chb;
+    const std::vector<Task> t = build_order(Shape{mode, N, NB, nrhs, NBB, workers});
+    const int n = std::min<int>((int)t.size(), cap);
+    memcpy(out, t.data(), sizeof(Task) * (size_t)n);
+    return n;
+}
+// Number of tasks of the schedule of a given shape (for tests and tracing).
+extern "C" int CHAM_B200_Schedule_Size(int mode, int N, int NB, int nrhs, int NBB, int workers) {
+    using namespace chb;
+    return (int)build_order(Shape{mode, N, NB, nrhs, NBB, workers}).size();
+}

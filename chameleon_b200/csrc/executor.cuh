@@ -1,0 +1,75 @@
+// executor.cuh -- device-resident tile-DAG executor (shared declarations).
+//
+// The reference runs chameleon_pdpotrf / chameleon_pdtrsm (compute/pzpotrf.c:
+// 84-194, compute/pztrsm.c:58-200) by submitting one runtime task per tile
+// kernel to StarPU/OpenMP (runtime/*/codelets/codelet_z{potrf,trsm,syrk,gemm}.c).
+// Here the same DAG is recorded once on the host as a list of sub-tile tasks in
+// a topological order and run by ONE persistent kernel: each CTA takes the
+// next task index with an atomic, waits (bounded) on per-tile dependency
+// counters, runs the tile operation and releases its counter.  A task only
+// waits on tasks that precede it in the list, and a CTA only takes a task while
+// it is resident, so the launch cannot deadlock whatever the grid size.
+#pragma once
+#include <stdint.h>
+
+namespace chb {
+
+enum TaskKind : int16_t {
+    TK_POTRF = 1,     // factor diagonal tile k, invert its inner diagonal blocks
+    TK_TRSM = 2,      // panel row block: A(m,k) <- A(m,k) L(k,k)^{-T}
+    TK_UPD = 3,       // trailing sub-block: A(m,n) -= A(m,k) A(n,k)^T (SYRK when m == n)
+    TK_FWD_TRSM = 4,  // B(k) <- L(k,k)^{-1} B(k)
+    TK_FWD_UPD = 5,   // B(m) -= L(m,k) B(k)            (m > k)
+    TK_BWD_TRSM = 6,  // B(k) <- L(k,k)^{-T} B(k)
+    TK_BWD_UPD = 7,   // B(m) -= L(k,m)^T B(k)          (m < k)
+    TK_INV = 8,       // invert inner diagonal blocks of an existing factor (potrs alone)
+};
+
+struct Task {
+    int16_t kind, sub;   // sub: row block (TRSM / *_UPD on B) or (bi | bj << 8) (TK_UPD)
+    int16_t m, n, k, bn;
+    int32_t pad;
+};
+static_assert(sizeof(Task) == 16, "Task is 16 bytes");
+
+enum ExecMode : int { MODE_FACT = 1, MODE_SOLVE = 2 };
+
+constexpr int SUBB = 128;      // sub-block edge of trailing updates / row blocks
+
+struct ExecState {
+    int next;          // dispatch cursor
+    int abort;         // set on failure: remaining tasks are skipped
+    int info;          // min global 1-based index of a non-positive pivot (INT_MAX: none)
+    int error;         // 0 or a CHAMELEON_ERR_* code (device timeout)
+    int done;          // tasks completed
+    int stuck_task;    // task index whose wait ran out (-1)
+    int pad[2];
+};
+
+struct TraceRec {
+    int32_t task, smid;
+    uint64_t t0, t1;
+};
+
+struct ExecParams {
+    const Task *tasks;
+    int ntasks;
+    int mode;
+    int upper;
+    int NT, N, NB;          // A: NT x NT tiles, order N, tile size NB (square tiles)
+    double *A;
+    const int64_t *a_off;   // element offset of tile (m,n) at a_off[m + NT*n]
+    const int *a_ld;        // leading dimension of tile row m
+    int NTB, nrhs, NBB;     // B: NT x NTB tiles of NB x NBB
+    double *B;
+    const int64_t *b_off;   // b_off[m + NT*bn]
+    const int *b_ld;
+    int *updA, *panA, *fwdB, *fwdDone, *bwdB, *bwdDone;
+    double *invd;           // NT * NIB inverted IB x IB blocks
+    int NIB;
+    ExecState *st;
+    TraceRec *trace;        // optional per-task trace (nullptr: off)
+    unsigned long long wait_budget_ns;
+};
+
+}  // namespace chb

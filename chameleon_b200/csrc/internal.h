@@ -1,0 +1,77 @@
+// internal.h -- host-side internals shared by the library's translation units.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <map>
+#include <mutex>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "../../include/chameleon_b200.h"
+#include "executor.cuh"
+
+namespace chb {
+
+// Library context: the reference keeps one global context
+// (control/context.c:145-221); so does this library.
+struct Context {
+    bool initialized = false;
+    int device = 0;
+    int num_sms = 0;
+    cudaStream_t stream = nullptr;
+    int tile_size = 384;          // CHAMELEON_TILE_SIZE default (control/context.c:162)
+    int inner_block = 48;
+    int warnings = 1;
+    int precision = CHAM_B200_PREC_BF16X3;
+    int refine_maxiter = 30;
+    long long wait_budget_us = 20000000;
+    int desc_ids = 0;
+    std::mutex mu;
+};
+Context &ctx();
+
+#define CHB_CUDA(call)                                                                 \
+    do {                                                                               \
+        cudaError_t _e = (call);                                                       \
+        if (_e != cudaSuccess) {                                                       \
+            chb::report_cuda_error(#call, _e, __FILE__, __LINE__);                     \
+            return CHAMELEON_ERR_UNEXPECTED;                                           \
+        }                                                                              \
+    } while (0)
+
+void report_cuda_error(const char *what, cudaError_t e, const char *file, int line);
+void warning(const char *func, const char *msg);
+int ensure_init();
+
+// Device-resident view of a descriptor's tile addressing (cached per descriptor).
+struct DescDev {
+    int64_t *off = nullptr;   // mt*nt element offsets
+    int *ld = nullptr;        // mt leading dimensions
+};
+struct DescPriv {
+    DescDev dev;
+    int cm_view = 0;          // 1: column-major user array view (LAPACK-layout entry points)
+};
+DescPriv *priv(const CHAM_desc_t *d);
+int desc_tile_rows(const CHAM_desc_t *d, int m);
+int desc_tile_cols(const CHAM_desc_t *d, int n);
+int64_t desc_tile_off(const CHAM_desc_t *d, int m, int n);
+int desc_tile_ld(const CHAM_desc_t *d, int m);
+int desc_upload(CHAM_desc_t *d);
+// Create a descriptor viewing a device column-major array (ld = lda) with
+// tile size nb: tile (m,n) at A + m*nb + n*nb*lda (control/descriptor.h:238-252).
+int desc_create_cm(CHAM_desc_t **desc, double *dA, int lda, int m, int n, int nb);
+int desc_sync_to_host(CHAM_desc_t *d);
+
+// Executor entry (executor.cu).
+struct ExecResult {
+    int info = 0;     // >0: LAPACK-style order of the failing minor
+    int error = 0;    // CHAMELEON_ERR_*
+    float ms = 0.f;   // device time of the launch
+};
+int run_cholesky_dag(int mode, cham_uplo_t uplo, CHAM_desc_t *A, CHAM_desc_t *B, cudaStream_t s,
+                     ExecResult *res);
+
+}  // namespace chb

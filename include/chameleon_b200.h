@@ -1,0 +1,249 @@
+/*
+ * chameleon_b200.h -- public C ABI of the B200-native tiled Cholesky path.
+ *
+ * Drop-in for Chameleon's d-precision Cholesky factor/solve API
+ * (include/chameleon.h, include/chameleon/chameleon_z.h after z->d
+ * generation) and for its GPU tile-kernel ABI (gpucublas/include/gpucublas/
+ * gpucublas_z.h, gpucublas_zc.h after generation).  Enum values, argument
+ * order and error conventions are those of the reference; citations are given
+ * per entry point as `file:line` inside the reference project.
+ *
+ * Memory model: descriptor storage lives in device memory (HBM).  A descriptor
+ * created over a host pointer is staged to the device once and copied back
+ * after every synchronous call that writes it; one created over a device
+ * pointer is used in place.  All computation runs on the GPU; there is no CPU
+ * fallback -- every entry point returns CHAMELEON_ERR_NOT_INITIALIZED /
+ * CHAMELEON_ERR_UNEXPECTED when no CUDA device is usable.
+ */
+#ifndef CHAMELEON_B200_H
+#define CHAMELEON_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------------- */
+/* Constants (include/chameleon/constants.h:30-445; identical values)         */
+/* ------------------------------------------------------------------------- */
+typedef enum { Cham8 = 0, ChamHalf = 1, ChamSingle = 2, ChamDouble = 3 } cham_arithmetic_t;
+typedef enum { ChamInt = 0, ChamReal = 1, ChamComplex = 2 } cham_ftype_t;
+typedef enum {
+    ChamRealHalf   = (1 << 2) | 1,
+    ChamRealFloat  = (1 << 2) | 2,
+    ChamRealDouble = (1 << 2) | 3,
+} cham_flttype_t;
+typedef enum { ChamCM = 101, ChamRM = 102, ChamCCRB = 103, ChamCRRB = 104 } cham_storage_t;
+typedef enum { ChamNoTrans = 111, ChamTrans = 112, ChamConjTrans = 113 } cham_trans_t;
+typedef enum { ChamUpper = 121, ChamLower = 122, ChamUpperLower = 123 } cham_uplo_t;
+typedef enum { ChamNonUnit = 131, ChamUnit = 132 } cham_diag_t;
+typedef enum { ChamLeft = 141, ChamRight = 142 } cham_side_t;
+typedef enum {
+    ChamOneNorm = 171, ChamFrobeniusNorm = 174, ChamInfNorm = 175, ChamMaxNorm = 177
+} cham_normtype_t;
+
+#define CHAMELEON_FALSE 0
+#define CHAMELEON_TRUE  1
+
+/* CHAMELEON_Enable / Disable features (constants.h:357-369) */
+#define CHAMELEON_WARNINGS   1
+#define CHAMELEON_ERRORS     2
+#define CHAMELEON_AUTOTUNING 3
+/* CHAMELEON_Set / Get parameters (constants.h:374-382) */
+#define CHAMELEON_CONCURRENCY      1
+#define CHAMELEON_TILE_SIZE        2
+#define CHAMELEON_INNER_BLOCK_SIZE 3
+#define CHAMELEON_TRANSLATION_MODE 7
+#define CHAMELEON_LOOKAHEAD        8
+/* B200 additions to CHAMELEON_Set / Get */
+#define CHAMELEON_B200_PRECISION      101 /* factorization precision of the mixed solver */
+#define CHAMELEON_B200_REFINE_MAXITER 102 /* iterative-refinement iteration cap           */
+#define CHAMELEON_B200_WAIT_BUDGET_MS 103 /* bound on any device-side dependency wait     */
+#define CHAMELEON_B200_WAIT_BUDGET_US 104 /* the same bound in microseconds              */
+
+/* Factorization precisions for CHAMELEON_B200_PRECISION */
+#define CHAM_B200_PREC_FP64   0
+#define CHAM_B200_PREC_FP32   1
+#define CHAM_B200_PREC_BF16X3 2
+
+/* Descriptor allocation modes (constants.h:412-413) */
+#define CHAMELEON_MAT_ALLOC_GLOBAL NULL
+#define CHAMELEON_MAT_ALLOC_TILE   ((void *)-1)
+
+/* Return codes (constants.h:434-445) */
+#define CHAMELEON_SUCCESS               0
+#define CHAMELEON_ERR_NOT_INITIALIZED  -101
+#define CHAMELEON_ERR_REINITIALIZED    -102
+#define CHAMELEON_ERR_NOT_SUPPORTED    -103
+#define CHAMELEON_ERR_ILLEGAL_VALUE    -104
+#define CHAMELEON_ERR_NOT_FOUND        -105
+#define CHAMELEON_ERR_OUT_OF_RESOURCES -106
+#define CHAMELEON_ERR_INTERNAL_LIMIT   -107
+#define CHAMELEON_ERR_UNALLOCATED      -108
+#define CHAMELEON_ERR_FILESYSTEM       -109
+#define CHAMELEON_ERR_UNEXPECTED       -110
+#define CHAMELEON_ERR_SEQUENCE_FLUSHED -111
+/* B200 addition: a device-side dependency wait ran past its budget; the
+ * persistent executor drained and returned without faulting the device. */
+#define CHAMELEON_ERR_DEVICE_TIMEOUT   -120
+
+/* ------------------------------------------------------------------------- */
+/* Descriptor and tile (include/chameleon/struct.h:53-61,179-270)             */
+/* ------------------------------------------------------------------------- */
+typedef struct chameleon_tile_s {
+    void          *mat;     /* device address of the tile                 */
+    int            rank, m, n, ld;
+    int8_t         format;
+    cham_flttype_t flttype;
+} CHAM_tile_t;
+
+struct chameleon_desc_s;
+typedef struct chameleon_desc_s CHAM_desc_t;
+
+typedef void *(*blkaddr_fct_t)(const CHAM_desc_t *, int, int);
+typedef int   (*blkldd_fct_t)(const CHAM_desc_t *, int);
+
+struct chameleon_desc_s {
+    char          *name;
+    blkaddr_fct_t  get_blkaddr;  /* device address of tile (m, n)         */
+    blkldd_fct_t   get_blkldd;   /* leading dimension of tile row m       */
+    CHAM_tile_t   *tiles;        /* host array of mt*nt tile views        */
+    void          *mat;          /* device base of the tile storage       */
+    void          *host_mat;     /* caller host pointer staged in/out, or NULL */
+    size_t         A21, A12, A22;
+    cham_storage_t styp;
+    cham_flttype_t dtyp;
+    int mb, nb, bsiz;
+    int i, j, m, n, lm, ln;
+    int mt, nt, lmt, lnt;
+    int llm1, lln1;
+    int lda;                     /* ChamCM views only: leading dimension of the user array */
+    int alloc_mat;               /* 1 when the library owns `mat`         */
+    int id;
+    void *schedopt;              /* executor-private state                */
+};
+
+/* Sequences (control/async.c:33-85) -- every call here is synchronous on
+ * return, sequences carry status only. */
+typedef struct runtime_sequence_s {
+    int   status;
+    void *request;
+    void *schedopt;
+} RUNTIME_sequence_t;
+typedef struct runtime_request_s {
+    int status;
+} RUNTIME_request_t;
+#define RUNTIME_REQUEST_INITIALIZER { 0 }
+
+/* ------------------------------------------------------------------------- */
+/* Control (include/chameleon.h:120-200; control/context.c:145-571)           */
+/* ------------------------------------------------------------------------- */
+int  __chameleon_init(int nworkers, int ncudas);
+int  __chameleon_finalize(void);
+#define CHAMELEON_Init(_nworkers_, _ncudas_) __chameleon_init((_nworkers_), (_ncudas_))
+#define CHAMELEON_Finalize() __chameleon_finalize()
+int  CHAMELEON_Initialized(void);
+int  CHAMELEON_Set(int param, int value);
+int  CHAMELEON_Get(int param, int *value);
+int  CHAMELEON_Enable(int option);
+int  CHAMELEON_Disable(int option);
+const char *CHAMELEON_B200_Strerror(int code);
+
+/* control/descriptor.c:749-756 */
+int  CHAMELEON_Desc_Create(CHAM_desc_t **desc, void *mat, cham_flttype_t dtyp, int mb, int nb,
+                           int bsiz, int lm, int ln, int i, int j, int m, int n, int p, int q);
+int  CHAMELEON_Desc_Destroy(CHAM_desc_t **desc);
+int  CHAMELEON_Desc_Flush(const CHAM_desc_t *desc, const RUNTIME_sequence_t *sequence);
+int  CHAMELEON_Desc_Acquire(const CHAM_desc_t *desc);
+int  CHAMELEON_Desc_Release(const CHAM_desc_t *desc);
+/* include/chameleon.h:130-131: column-major host/device array <-> tiles */
+int  CHAMELEON_Lap2Desc(cham_uplo_t uplo, void *A, int LDA, CHAM_desc_t *descA);
+int  CHAMELEON_Desc2Lap(cham_uplo_t uplo, CHAM_desc_t *descA, void *A, int LDA);
+int  CHAMELEON_Sequence_Create(RUNTIME_sequence_t **sequence);
+int  CHAMELEON_Sequence_Destroy(RUNTIME_sequence_t *sequence);
+int  CHAMELEON_Sequence_Wait(RUNTIME_sequence_t *sequence);
+
+/* ------------------------------------------------------------------------- */
+/* Cholesky path (include/chameleon/chameleon_z.h after z->d generation)      */
+/* ------------------------------------------------------------------------- */
+/* compute/zposv.c:93 (LAPACK layout; A, B host or device column-major)      */
+int CHAMELEON_dposv(cham_uplo_t uplo, int N, int NRHS, double *A, int LDA, double *B, int LDB);
+/* compute/zposv.c:222 / :276 */
+int CHAMELEON_dposv_Tile(cham_uplo_t uplo, CHAM_desc_t *A, CHAM_desc_t *B);
+int CHAMELEON_dposv_Tile_Async(cham_uplo_t uplo, CHAM_desc_t *A, CHAM_desc_t *B,
+                               RUNTIME_sequence_t *sequence, RUNTIME_request_t *request);
+/* compute/zpotrf.c:81 / :192 / :246 */
+int CHAMELEON_dpotrf(cham_uplo_t uplo, int N, double *A, int LDA);
+int CHAMELEON_dpotrf_Tile(cham_uplo_t uplo, CHAM_desc_t *A);
+int CHAMELEON_dpotrf_Tile_Async(cham_uplo_t uplo, CHAM_desc_t *A,
+                                RUNTIME_sequence_t *sequence, RUNTIME_request_t *request);
+/* compute/zpotrs.c:78 / :198 / :253 */
+int CHAMELEON_dpotrs(cham_uplo_t uplo, int N, int NRHS, double *A, int LDA, double *B, int LDB);
+int CHAMELEON_dpotrs_Tile(cham_uplo_t uplo, CHAM_desc_t *A, CHAM_desc_t *B);
+int CHAMELEON_dpotrs_Tile_Async(cham_uplo_t uplo, CHAM_desc_t *A, CHAM_desc_t *B,
+                                RUNTIME_sequence_t *sequence, RUNTIME_request_t *request);
+/* compute/zpotrf_batch.c:89 -- every tile of A is an independent matrix */
+int CHAMELEON_dpotrf_batch_Tile(cham_uplo_t uplo, CHAM_desc_t *A);
+/* compute/ztrsm_batch.c:180 -- tile (m,n) of B solved with tile (m,n) of A */
+int CHAMELEON_dtrsm_batch_Tile(cham_side_t side, cham_uplo_t uplo, cham_trans_t trans,
+                               cham_diag_t diag, double alpha, CHAM_desc_t *A, CHAM_desc_t *B);
+/* Generators: compute/zplgsy.c:276 (pzplgsy.c:29-80), compute/zplrnt.c (pzplrnt.c) */
+int CHAMELEON_dplgsy(double bump, cham_uplo_t uplo, int N, double *A, int LDA,
+                     unsigned long long int seed);
+int CHAMELEON_dplgsy_Tile(double bump, cham_uplo_t uplo, CHAM_desc_t *A,
+                          unsigned long long int seed);
+int CHAMELEON_dplrnt(int M, int N, double *A, int LDA, unsigned long long int seed);
+int CHAMELEON_dplrnt_Tile(CHAM_desc_t *A, unsigned long long int seed);
+/* Norms used by the testing checks (compute/zlansy.c, compute/zlange.c) */
+double CHAMELEON_dlansy_Tile(cham_normtype_t norm, cham_uplo_t uplo, CHAM_desc_t *A);
+double CHAMELEON_dlange_Tile(cham_normtype_t norm, CHAM_desc_t *A);
+
+/* ------------------------------------------------------------------------- */
+/* GPU tile-kernel ABI (gpucublas/include/gpucublas/gpucublas_z.h:36-61,      */
+/* gpucublas_zc.h:22-23 after z->d / zc->ds generation).  The cuBLAS and      */
+/* cuSOLVER handle types are opaque handles of this library carrying the      */
+/* stream; no cuBLAS or cuSOLVER is linked.                                   */
+/* ------------------------------------------------------------------------- */
+typedef struct cham_b200_handle_s *cublasHandle_t;
+typedef struct cham_b200_handle_s *cusolverDnHandle_t;
+int CHAM_B200_Handle_Create(cublasHandle_t *handle, void *cuda_stream);
+int CHAM_B200_Handle_Destroy(cublasHandle_t handle);
+
+int CUDA_dgemm(cham_trans_t transa, cham_trans_t transb, int m, int n, int k,
+               const double *alpha, const double *A, int lda, const double *B, int ldb,
+               const double *beta, double *C, int ldc, cublasHandle_t handle);
+int CUDA_dsyrk(cham_uplo_t uplo, cham_trans_t trans, int n, int k, const double *alpha,
+               const double *A, int lda, const double *beta, double *C, int ldc,
+               cublasHandle_t handle);
+int CUDA_dtrsm(cham_side_t side, cham_uplo_t uplo, cham_trans_t transa, cham_diag_t diag,
+               int m, int n, const double *alpha, const double *A, int lda, double *B, int ldb,
+               cublasHandle_t handle);
+/* d_info: device int receiving LAPACK's info; WORK/lwork are accepted and unused */
+int CUDA_dpotrf(cham_uplo_t uplo, int n, double *A, int lda, double *WORK, int lwork,
+                int *d_info, cusolverDnHandle_t handle);
+int CUDA_dplgsy(const double *bump, int m, int n, double *A, int lda, int bigM, int m0, int n0,
+                unsigned long long int seed, cublasHandle_t handle);
+int CUDA_dplrnt(int m, int n, double *A, int lda, int bigM, int m0, int n0,
+                unsigned long long int seed, cublasHandle_t handle);
+int CUDA_dlag2s(int m, int n, const double *A, int lda, float *SA, int ldsa,
+                cublasHandle_t handle);
+int CUDA_slag2d(int m, int n, const float *SA, int ldsa, double *A, int lda,
+                cublasHandle_t handle);
+
+/* ------------------------------------------------------------------------- */
+/* Uneven batch (new; the reference batch API is uniform-size,                */
+/* compute/zpotrf_batch.c:66-118).  Matrix i is n[i] x n[i] column-major at   */
+/* A + a_off[i] (ld = n[i]); its right-hand sides are n[i] x nrhs[i] at        */
+/* B + b_off[i] (ld = n[i]), overwritten by the solution.  All arrays are      */
+/* device arrays; info[i] receives the LAPACK info of matrix i.               */
+/* ------------------------------------------------------------------------- */
+int CHAM_B200_dposv_batch(cham_uplo_t uplo, int count, const int *n, const int *nrhs,
+                          double *A, const int64_t *a_off, double *B, const int64_t *b_off,
+                          int *info, void *cuda_stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CHAMELEON_B200_H */

@@ -1,0 +1,171 @@
+"""Python access to the two CPU checkers (test infrastructure only).
+
+* ``port()``      -- the C restatement oracle/cham_oracle.c, built into
+                     oracle/liboracle.so by :func:`build_port`.
+* ``reference()`` -- the reference's own CPU library, built from the reference
+                     sources by oracle/build_ref.sh into oracle/_ref/libchamref.so.
+
+Only tests/, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline and
+reference arms import this module; the product never does.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PORT_SO = os.path.join(HERE, "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libchamref.so")
+
+UPPER, LOWER, UPPERLOWER = 121, 122, 123
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int)
+
+
+def _ptr(a):
+    assert a.dtype == np.float64 and (a.flags.f_contiguous or a.ndim == 1)
+    return a.ctypes.data_as(_dp)
+
+
+def build_port(force=False):
+    src = os.path.join(HERE, "cham_oracle.c")
+    if not force and os.path.exists(PORT_SO) and os.path.getmtime(PORT_SO) >= os.path.getmtime(src):
+        return PORT_SO
+    subprocess.check_call(["gcc", "-O2", "-fPIC", "-shared", "-std=c11", src, "-o", PORT_SO + ".tmp", "-lm"])
+    os.replace(PORT_SO + ".tmp", PORT_SO)
+    return PORT_SO
+
+
+def build_ref(force=False):
+    """Build the reference library (needs the reference sources; not on the GPU host)."""
+    if not force and os.path.exists(REF_SO):
+        return REF_SO
+    subprocess.check_call(["bash", os.path.join(HERE, "build_ref.sh")])
+    return REF_SO
+
+
+_port = None
+_ref = None
+
+
+def port():
+    global _port
+    if _port is None:
+        _port = ctypes.CDLL(build_port())
+        L = _port
+        L.orc_lcg_skip.restype = ctypes.c_ulonglong
+        L.orc_lcg_skip.argtypes = [ctypes.c_ulonglong, ctypes.c_ulonglong]
+        L.orc_dplgsy.argtypes = [ctypes.c_double, ctypes.c_int, _dp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                 ctypes.c_int, ctypes.c_ulonglong]
+        L.orc_dplrnt.argtypes = [ctypes.c_int, ctypes.c_int, _dp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                 ctypes.c_int, ctypes.c_ulonglong]
+        L.orc_dpotrf_tiled.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp, ctypes.c_int]
+        L.orc_dpotrs_tiled.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp, ctypes.c_int,
+                                       _dp, ctypes.c_int]
+        L.orc_check_factorization.restype = ctypes.c_double
+        L.orc_check_factorization.argtypes = [ctypes.c_int, ctypes.c_int, _dp, ctypes.c_int, _dp, ctypes.c_int]
+        L.orc_check_solve.restype = ctypes.c_double
+        L.orc_check_solve.argtypes = [ctypes.c_int, ctypes.c_int, _dp, ctypes.c_int, _dp, ctypes.c_int, _dp,
+                                      ctypes.c_int]
+    return _port
+
+
+def reference_available():
+    return os.path.exists(REF_SO)
+
+
+def reference(ncores=0):
+    global _ref
+    if _ref is None:
+        os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")
+        _ref = ctypes.CDLL(REF_SO)
+        L = _ref
+        L.chamref_init.argtypes = [ctypes.c_int]
+        L.chamref_dplgsy.argtypes = [ctypes.c_double, ctypes.c_int, ctypes.c_int, _dp, ctypes.c_int, ctypes.c_int,
+                                     ctypes.c_ulonglong]
+        L.chamref_dplrnt.argtypes = [ctypes.c_int, ctypes.c_int, _dp, ctypes.c_int, ctypes.c_int,
+                                     ctypes.c_ulonglong]
+        L.chamref_dposv.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp, ctypes.c_int, _dp,
+                                    ctypes.c_int, _dp]
+        L.chamref_dpotrf.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp, ctypes.c_int, _dp]
+        L.chamref_dpotrs.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp, ctypes.c_int, _dp,
+                                     ctypes.c_int]
+        L.chamref_dposv_tile_seeded.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                ctypes.c_ulonglong, ctypes.c_ulonglong, _dp, _dp, _dp]
+        L.chamref_dpotrf_batch.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp, _dp]
+        L.chamref_dtrsm_batch.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                          ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp, _dp]
+        L.chamref_lapacke_dsposv.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp, ctypes.c_int, _dp,
+                                             ctypes.c_int, _dp, ctypes.c_int, _ip, _dp]
+        L.chamref_init(ncores if ncores > 0 else (os.cpu_count() or 1))
+    return _ref
+
+
+# ---- convenience wrappers on numpy arrays (column-major) -------------------
+
+def lcg_skip(n, seed):
+    return port().orc_lcg_skip(n, seed)
+
+
+def dplgsy(bump, N, seed, bigM=None, m0=0, n0=0):
+    A = np.zeros((N, N), order="F")
+    port().orc_dplgsy(bump, N, _ptr(A), max(N, 1), N if bigM is None else bigM, m0, n0, seed)
+    return A
+
+
+def dplrnt(M, N, seed, bigM=None, m0=0, n0=0):
+    A = np.zeros((M, N), order="F")
+    port().orc_dplrnt(M, N, _ptr(A), max(M, 1), M if bigM is None else bigM, m0, n0, seed)
+    return A
+
+
+def dpotrf_tiled(uplo, A, NB):
+    F = np.asfortranarray(A.copy())
+    info = port().orc_dpotrf_tiled(uplo, F.shape[0], NB, _ptr(F), max(F.shape[0], 1))
+    return F, info
+
+
+def dpotrs_tiled(uplo, F, B, NB):
+    X = np.asfortranarray(B.copy())
+    N = F.shape[0]
+    port().orc_dpotrs_tiled(uplo, N, X.shape[1], NB, _ptr(F), max(N, 1), _ptr(X), max(N, 1))
+    return X
+
+
+def check_factorization(uplo, A0, F):
+    A0 = np.asfortranarray(A0)
+    F = np.asfortranarray(F)
+    N = A0.shape[0]
+    return port().orc_check_factorization(uplo, N, _ptr(A0), max(N, 1), _ptr(F), max(N, 1))
+
+
+def check_solve(A0, X, B):
+    A0, X, B = (np.asfortranarray(a) for a in (A0, X, B))
+    N = A0.shape[0]
+    return port().orc_check_solve(N, X.shape[1], _ptr(A0), max(N, 1), _ptr(X), max(N, 1), _ptr(B), max(N, 1))
+
+
+def ref_dposv(uplo, A, B, NB):
+    """Reference dposv (LAPACK layout) on copies; returns (F, X, info, seconds)."""
+    L = reference()
+    F = np.asfortranarray(A.copy())
+    X = np.asfortranarray(B.copy())
+    t = ctypes.c_double()
+    N = F.shape[0]
+    info = L.chamref_dposv(uplo, N, X.shape[1], NB, _ptr(F), max(N, 1), _ptr(X), max(N, 1), ctypes.byref(t))
+    return F, X, info, t.value
+
+
+def ref_dplgsy(bump, uplo, N, seed, NB=384):
+    L = reference()
+    A = np.zeros((N, N), order="F")
+    L.chamref_dplgsy(bump, uplo, N, _ptr(A), max(N, 1), NB, seed)
+    return A
+
+
+def ref_dplrnt(M, N, seed, NB=384):
+    L = reference()
+    A = np.zeros((M, N), order="F")
+    L.chamref_dplrnt(M, N, _ptr(A), max(M, 1), NB, seed)
+    return A

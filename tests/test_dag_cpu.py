@@ -1,0 +1,125 @@
+"""Host-side checks of the persistent executor's task DAG (no GPU).
+
+1. Deadlock freedom: walking the task list in order, every task's wait
+   predicate -- the exact counter conditions the device kernel spins on -- is
+   already satisfied by the tasks before it.  With dispatch by an atomic cursor
+   this proves the launch always progresses, whatever the number of CTAs.
+2. Data flow: executing the same list on the host with numpy (each task doing
+   the device task's sub-block arithmetic) reproduces the Cholesky factor and
+   the solution of the oracle.
+"""
+import numpy as np
+import pytest
+import scipy.linalg as sla
+
+TK_POTRF, TK_TRSM, TK_UPD, TK_FWD_TRSM, TK_FWD_UPD, TK_BWD_TRSM, TK_BWD_UPD, TK_INV = range(1, 9)
+SUBB = 128
+FACT, SOLVE = 1, 2
+
+
+def geometry(N, NB, nrhs, NBB):
+    NT = -(-N // NB)
+    NTB = -(-nrhs // NBB) if nrhs else 0
+    tm = lambda m: N - m * NB if m == NT - 1 else NB
+    nbi = lambda m: -(-tm(m) // SUBB)
+    S = lambda m, n: nbi(m) * (nbi(m) + 1) // 2 if m == n else nbi(m) * nbi(n)
+    return NT, NTB, tm, nbi, S
+
+
+def check_waits(tasks, mode, N, NB, nrhs, NBB):
+    NT, NTB, tm, nbi, S = geometry(N, NB, nrhs, NBB)
+    upd = np.zeros((NT, NT), int); pan = np.zeros((NT, NT), int)
+    fwdB = np.zeros((NT, max(NTB, 1)), int); fwdD = np.zeros_like(fwdB)
+    bwdB = np.zeros_like(fwdB); bwdD = np.zeros_like(fwdB)
+    fact = bool(mode & FACT)
+    for kind, sub, m, n, k, bn in tasks:
+        if kind == TK_POTRF:
+            ok = upd[k, k] >= k * S(k, k); pan[k, k] += 1
+        elif kind == TK_INV:
+            ok = True; pan[k, k] += 1
+        elif kind == TK_TRSM:
+            ok = pan[k, k] >= 1 and upd[m, k] >= k * S(m, k); pan[m, k] += 1
+        elif kind == TK_UPD:
+            ok = pan[m, k] >= nbi(m) and pan[n, k] >= nbi(n) and upd[m, n] >= k * S(m, n); upd[m, n] += 1
+        elif kind == TK_FWD_TRSM:
+            ok = pan[k, k] >= 1 and fwdB[k, bn] >= k * nbi(k); fwdD[k, bn] += 1
+        elif kind == TK_FWD_UPD:
+            ok = fwdD[k, bn] >= 1 and (not fact or pan[m, k] >= nbi(m)) and fwdB[m, bn] >= k * nbi(m)
+            fwdB[m, bn] += 1
+        elif kind == TK_BWD_TRSM:
+            ok = fwdD[k, bn] >= 1 and bwdB[k, bn] >= (NT - 1 - k) * nbi(k); bwdD[k, bn] += 1
+        elif kind == TK_BWD_UPD:
+            ok = bwdD[k, bn] >= 1 and bwdB[m, bn] >= (NT - 1 - k) * nbi(m); bwdB[m, bn] += 1
+        else:
+            raise AssertionError(kind)
+        assert ok, (kind, sub, m, n, k, bn)
+    # every tile got all of its updates / solves
+    if fact:
+        for m in range(NT):
+            for n in range(m + 1):
+                assert upd[m, n] == n * S(m, n)
+    if mode & SOLVE:
+        assert (fwdD[:, :NTB] == 1).all() and (bwdD[:, :NTB] == 1).all()
+
+
+def emulate(tasks, A, B, uplo, N, NB, NBB):
+    """Run the task list on host arrays with the device tasks' arithmetic."""
+    NT, NTB, tm, nbi, S = geometry(N, NB, B.shape[1] if B is not None else 0, NBB)
+    M = A if uplo == 122 else A.T          # logical lower view (writes land in A)
+    L = lambda m, n: M[m * NB:m * NB + tm(m), n * NB:n * NB + tm(n)]
+    Bt = lambda m, bn: B[m * NB:m * NB + tm(m), bn * NBB:min((bn + 1) * NBB, B.shape[1])]
+    for kind, sub, m, n, k, bn in tasks:
+        if kind == TK_POTRF:
+            T = L(k, k)
+            T[np.tril_indices(T.shape[0])] = np.linalg.cholesky(np.tril(T) + np.tril(T, -1).T)[
+                np.tril_indices(T.shape[0])]
+        elif kind == TK_TRSM:
+            X = L(m, k)[sub * SUBB:(sub + 1) * SUBB]
+            X[:] = sla.solve_triangular(np.tril(L(k, k)), X.T, lower=True).T
+        elif kind == TK_UPD:
+            bi, bj = sub & 0xFF, (sub >> 8) & 0xFF
+            C = L(m, n)[bi * SUBB:(bi + 1) * SUBB, bj * SUBB:(bj + 1) * SUBB]
+            upd = L(m, k)[bi * SUBB:(bi + 1) * SUBB] @ L(n, k)[bj * SUBB:(bj + 1) * SUBB].T
+            if m == n and bi == bj:
+                upd = np.tril(upd)
+            C -= upd
+        elif kind == TK_FWD_TRSM:
+            X = Bt(k, bn); X[:] = sla.solve_triangular(np.tril(L(k, k)), X, lower=True)
+        elif kind == TK_BWD_TRSM:
+            X = Bt(k, bn); X[:] = sla.solve_triangular(np.tril(L(k, k)), X, lower=True, trans=1)
+        elif kind == TK_FWD_UPD:
+            Bt(m, bn)[sub * SUBB:(sub + 1) * SUBB] -= L(m, k)[sub * SUBB:(sub + 1) * SUBB] @ Bt(k, bn)
+        elif kind == TK_BWD_UPD:
+            Bt(m, bn)[sub * SUBB:(sub + 1) * SUBB] -= L(k, m)[:, sub * SUBB:(sub + 1) * SUBB].T @ Bt(k, bn)
+
+
+SHAPES = [(15, 16, 1, 16), (37, 17, 22, 17), (300, 128, 5, 128), (700, 256, 70, 64), (1000, 384, 3, 384),
+          (1100, 512, 64, 512), (513, 512, 1, 512)]
+
+
+@pytest.mark.parametrize("N,NB,nrhs,NBB", SHAPES)
+@pytest.mark.parametrize("workers", [1, 7, 148])
+def test_schedule_is_deadlock_free(cb_host, N, NB, nrhs, NBB, workers):
+    for mode in (FACT, SOLVE, FACT | SOLVE):
+        t = cb_host.schedule(mode, N, NB, nrhs if mode & SOLVE else 0, NBB, workers)
+        check_waits(t, mode, N, NB, nrhs if mode & SOLVE else 0, NBB)
+
+
+@pytest.mark.parametrize("uplo", [121, 122])
+@pytest.mark.parametrize("N,NB,nrhs,NBB", SHAPES[:6])
+def test_schedule_dataflow_reproduces_cholesky(cb_host, orc, uplo, N, NB, nrhs, NBB):
+    A0 = orc.dplgsy(float(N), N, 51)
+    B0 = orc.dplrnt(N, nrhs, 5673)
+    A = A0.copy(); B = B0.copy()
+    emulate(cb_host.schedule(FACT | SOLVE, N, NB, nrhs, NBB, 13), A, B, uplo, N, NB, NBB)
+    F = np.tril(A) if uplo == 122 else np.triu(A)
+    assert orc.check_factorization(uplo, A0, F) < 60
+    assert orc.check_solve(A0, B, B0) < 60
+    Fo, _ = orc.dpotrf_tiled(uplo, A0, NB)
+    assert np.allclose(F, np.tril(Fo) if uplo == 122 else np.triu(Fo), atol=1e-12)
+
+
+@pytest.fixture(scope="module")
+def cb_host():
+    import chameleon_b200 as cb
+    return cb
