@@ -117,6 +117,9 @@ PROTOS = {
     "CHAMELEON_dplrnt_Tile": (_i, [_D, _ull]),
     "CHAMELEON_dlansy_Tile": (ctypes.c_double, [_i, _i, _D]),
     "CHAMELEON_dlange_Tile": (ctypes.c_double, [_i, _D]),
+    "CHAMELEON_dsposv": (_i, [_i, _i, _i, _vp, _i, _vp, _i, _vp, _i, ctypes.POINTER(_i)]),
+    "CHAMELEON_dsposv_Tile": (_i, [_i, _D, _D, _D, ctypes.POINTER(_i)]),
+    "CHAMELEON_B200_dposv_mixed_Tile": (_i, [_i, _i, _D, _D, _D, ctypes.POINTER(RefineInfo)]),
     "CHAM_B200_Handle_Create": (_i, [ctypes.POINTER(_vp), _vp]),
     "CHAM_B200_Handle_Destroy": (_i, [_vp]),
     "CUDA_dgemm": (_i, [_i, _i, _i, _i, _i, _dp, _vp, _i, _vp, _i, _dp, _vp, _i, _vp]),
@@ -137,6 +140,11 @@ EXTRAS = {
     "CHAM_B200_Schedule_Size": (_i, [_i, _i, _i, _i, _i, _i]),
     "CHAM_B200_Schedule_Build": (_i, [_i, _i, _i, _i, _i, _i, ctypes.POINTER(Task), _i]),
     "CHAM_B200_dposv_timed": (_i, [_i, _i, _i, _vp, _i, _vp, _i, ctypes.POINTER(ctypes.c_float)]),
+    "CHAM_B200_Event_Record": (_i, [_i]),
+    "CHAM_B200_Event_Elapsed": (ctypes.c_float, [_i, _i]),
+    "CHAM_B200_Launch_Count": (ctypes.c_ulonglong, []),
+    "CHAM_B200_Device_Sync": (_i, []),
+    "CHAM_B200_Mixed_Stats": (_i, [_dp]),
 }
 
 _lib = None
@@ -305,6 +313,27 @@ def dplgsy(bump, uplo, N, A, LDA, seed):
 def dplrnt(M, N, A, LDA, seed):
     init()
     return lib().CHAMELEON_dplrnt(M, N, _addr(A), LDA, seed)
+
+
+def dsposv_Tile(uplo, A, B, X):
+    """CHAMELEON_dsposv_Tile: returns (rc, ITER)."""
+    it = ctypes.c_int()
+    rc = lib().CHAMELEON_dsposv_Tile(uplo, A.ptr, B.ptr, X.ptr, ctypes.byref(it))
+    return rc, it.value
+
+
+def dposv_mixed_Tile(uplo, precision, A, B, X):
+    """CHAMELEON_B200_dposv_mixed_Tile: returns (rc, RefineInfo)."""
+    info = RefineInfo()
+    rc = lib().CHAMELEON_B200_dposv_mixed_Tile(uplo, precision, A.ptr, B.ptr, X.ptr, ctypes.byref(info))
+    return rc, info
+
+
+def dsposv(uplo, N, NRHS, A, LDA, B, LDB, X, LDX):
+    init()
+    it = ctypes.c_int()
+    rc = lib().CHAMELEON_dsposv(uplo, N, NRHS, _addr(A), LDA, _addr(B), LDB, _addr(X), LDX, ctypes.byref(it))
+    return rc, it.value
 
 
 def schedule(mode, N, NB, nrhs=0, NBB=None, workers=148):

@@ -44,14 +44,14 @@ __global__ void __launch_bounds__(NT_CTA, 1) dposv_batch_kernel(const BatchItem 
         if (i >= count) break;
         const BatchItem it = items[i];
         const View T = upper ? View{A + it.a_off, it.lda, 1} : View{A + it.a_off, 1, it.lda};
-        const int r = tile_potrf(T, it.n, invd, smem);
+        const int r = tile_potrf<double, SPLIT_BF16X3>(T, it.n, invd, smem);
         if (threadIdx.x == 0 && info) info[it.info_idx] = r;
         if (r == 0 && it.nrhs > 0) {
             const View X{B + it.b_off, 1, it.ldb};
             for (int c0 = 0; c0 < it.nrhs; c0 += IB) {
                 const int w = min(IB, it.nrhs - c0);
-                trsm_left(X.sub(0, c0), w, T, it.n, invd, false, smem);
-                trsm_left(X.sub(0, c0), w, T, it.n, invd, true, smem);
+                trsm_left<double, SPLIT_BF16X3>(X.sub(0, c0), w, T, it.n, invd, false, smem);
+                trsm_left<double, SPLIT_BF16X3>(X.sub(0, c0), w, T, it.n, invd, true, smem);
             }
         }
         cta_sync_global();
@@ -73,7 +73,7 @@ __global__ void __launch_bounds__(NT_CTA, 1) trsm_batch_kernel(const TrsmItem *i
     extern __shared__ __align__(128) double smem[];
     __shared__ int s_i;
     double *invd = scratch + (int64_t)blockIdx.x * nib * IB * IB;
-    double *sD = smem + Cfg12864::SMEM_ELEMS;
+    double *sD = smem + Cfg12864<double>::SMEM_ELEMS;
     double *sInv = sD + IB * LDD;
     while (true) {
         if (threadIdx.x == 0) s_i = atomicAdd(cursor, 1);
@@ -103,7 +103,7 @@ __global__ void __launch_bounds__(NT_CTA, 1) trsm_batch_kernel(const TrsmItem *i
         }
         cta_sync_global();
         for (int c0 = 0; c0 < it.w; c0 += IB)
-            trsm_left(X.sub(0, c0), min(IB, it.w - c0), L, it.na, invd, trans_eff != 0, smem);
+            trsm_left<double, SPLIT_BF16X3>(X.sub(0, c0), min(IB, it.w - c0), L, it.na, invd, trans_eff != 0, smem);
         cta_sync_global();
     }
 }
@@ -169,6 +169,7 @@ int launch_posv_batch(std::vector<BatchItem> &items, double *A, double *B, int u
         return rc;
     CHB_CUDA(cudaMemcpyAsync(g_bws.items, items.data(), items.size() * sizeof(BatchItem), cudaMemcpyHostToDevice, s));
     CHB_CUDA(cudaMemsetAsync(g_bws.cursor, 0, sizeof(int), s));
+    CHB_LAUNCHED(1);
     dposv_batch_kernel<<<grid, NT_CTA, TILE_KERNEL_SMEM_BYTES, s>>>((const BatchItem *)g_bws.items, (int)items.size(),
                                                                     A, B, upper, info, g_bws.cursor, g_bws.scratch,
                                                                     nib);
@@ -251,6 +252,7 @@ int CHAMELEON_dtrsm_batch_Tile(cham_side_t side, cham_uplo_t uplo, cham_trans_t 
         return rc;
     CHB_CUDA(cudaMemcpyAsync(g_bws.items, items.data(), items.size() * sizeof(TrsmItem), cudaMemcpyHostToDevice, s));
     CHB_CUDA(cudaMemsetAsync(g_bws.cursor, 0, sizeof(int), s));
+    CHB_LAUNCHED(1);
     trsm_batch_kernel<<<grid, NT_CTA, TILE_KERNEL_SMEM_BYTES, s>>>((const TrsmItem *)g_bws.items, (int)items.size(),
                                                                    (double *)A->mat, (double *)B->mat, up, !left,
                                                                    trans_eff, diag == ChamUnit, alpha, g_bws.cursor,

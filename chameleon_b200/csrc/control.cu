@@ -20,6 +20,9 @@ Context &ctx() {
     return c;
 }
 
+unsigned long long g_launch_count = 0;
+MixedStats g_mixed_stats;
+
 void report_cuda_error(const char *what, cudaError_t e, const char *file, int line) {
     fprintf(stderr, "[chameleon_b200] CUDA error %s (%d) in %s at %s:%d\n", cudaGetErrorString(e), (int)e,
             what, file, line);
@@ -397,7 +400,16 @@ int CHAMELEON_Desc_Create(CHAM_desc_t **descptr, void *mat, cham_flttype_t dtyp,
     d->schedopt = new DescPriv();
     d->id = ctx().desc_ids++;
     const size_t bytes = std::max<size_t>((size_t)lm * ln * elt_size(dtyp), 16);
-    if (mat == CHAMELEON_MAT_ALLOC_TILE || mat == CHAMELEON_MAT_ALLOC_GLOBAL) {
+    // As in the reference (control/descriptor.c:183-199), a caller-provided
+    // matrix is a column-major lm x ln array (ChamCM, ld = lm); only
+    // library-allocated storage uses the tile-major CCRB layout.
+    const bool user_mat = !(mat == CHAMELEON_MAT_ALLOC_TILE || mat == CHAMELEON_MAT_ALLOC_GLOBAL);
+    if (user_mat) {
+        d->styp = ChamCM;
+        d->lda = std::max(lm, 1);
+        priv(d)->cm_view = 1;
+    }
+    if (!user_mat) {
         if (cudaMalloc(&d->mat, bytes) != cudaSuccess) {
             cudaGetLastError();
             delete priv(d);
@@ -472,7 +484,8 @@ static int lap_desc_copy(cham_uplo_t uplo, void *A, int LDA, CHAM_desc_t *d, int
     }
     const int64_t total = (int64_t)d->m * d->n;
     if (total > 0)
-        lap2tile_kernel<<<grid_for(total), 256, 0, s>>>(tilemap(d), dA, LDA, d->m, d->n, (int)uplo, to_tile);
+        lap2tile_kernel<<<grid_for(total), 256, 0, s>>>(tilemap(d), dA, LDA, d->m, d->n, (int)uplo, to_tile),
+            CHB_LAUNCHED(1);
     CHB_CUDA(cudaGetLastError());
     if (tmp) {
         if (!to_tile) CHB_CUDA(cudaMemcpyAsync(A, tmp, bytes, cudaMemcpyDeviceToHost, s));
@@ -516,7 +529,8 @@ int CHAMELEON_dplgsy_Tile(double bump, cham_uplo_t uplo, CHAM_desc_t *A, unsigne
     const int64_t total = (int64_t)A->m * A->n;
     if (total > 0)
         plgsy_kernel<<<grid_for(total), 256, 0, ctx().stream>>>(tilemap(A), A->m, A->n, bump, A->m, 0, 0, seed,
-                                                                (int)uplo);
+                                                                (int)uplo),
+            CHB_LAUNCHED(1);
     CHB_CUDA(cudaGetLastError());
     CHB_CUDA(cudaStreamSynchronize(ctx().stream));
     return desc_sync_to_host(A);
@@ -530,7 +544,8 @@ int CHAMELEON_dplrnt_Tile(CHAM_desc_t *A, unsigned long long int seed) {
     if (rc) return rc;
     const int64_t total = (int64_t)A->m * A->n;
     if (total > 0)
-        plrnt_kernel<<<grid_for(total), 256, 0, ctx().stream>>>(tilemap(A), A->m, A->n, A->m, 0, 0, seed);
+        plrnt_kernel<<<grid_for(total), 256, 0, ctx().stream>>>(tilemap(A), A->m, A->n, A->m, 0, 0, seed),
+            CHB_LAUNCHED(1);
     CHB_CUDA(cudaGetLastError());
     CHB_CUDA(cudaStreamSynchronize(ctx().stream));
     return desc_sync_to_host(A);
@@ -697,6 +712,31 @@ int CHAMELEON_dposv_Tile(cham_uplo_t uplo, CHAM_desc_t *A, CHAM_desc_t *B) {
 // arrays are viewed in place through column-major tile addressing
 // (control/compute_z.h:471-506, InPlace translation); host arrays are staged
 // to the device and back.
+}  // extern "C"
+
+namespace chb {
+// Device staging buffers of the LAPACK-layout entry points (grow-only, kept
+// for the life of the process so repeated calls do not re-allocate).
+static double *g_stage[3] = {nullptr, nullptr, nullptr};
+static size_t g_stage_bytes[3] = {0, 0, 0};
+double *staging(int slot, size_t bytes) {
+    if (bytes > g_stage_bytes[slot]) {
+        if (g_stage[slot]) cudaFree(g_stage[slot]);
+        g_stage[slot] = nullptr;
+        g_stage_bytes[slot] = 0;
+        if (cudaMalloc(&g_stage[slot], bytes) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        g_stage_bytes[slot] = bytes;
+    }
+    return g_stage[slot];
+}
+bool is_device_ptr_pub(const void *p) { return is_device_ptr(p); }
+}  // namespace chb
+
+extern "C" {
+
 static int lapack_call(int mode, cham_uplo_t uplo, int N, int NRHS, double *A, int LDA, double *B, int LDB,
                        float *ms_out) {
     Context &c = ctx();
@@ -707,11 +747,11 @@ static int lapack_call(int mode, cham_uplo_t uplo, int N, int NRHS, double *A, i
     const size_t abytes = (size_t)LDA * N * sizeof(double);
     const size_t bbytes = (NRHS > 0) ? (size_t)LDB * NRHS * sizeof(double) : 0;
     if (!a_dev) {
-        CHB_CUDA(cudaMalloc(&dA, std::max<size_t>(abytes, 16)));
+        if (!(dA = staging(0, std::max<size_t>(abytes, 16)))) return CHAMELEON_ERR_OUT_OF_RESOURCES;
         CHB_CUDA(cudaMemcpyAsync(dA, A, abytes, cudaMemcpyHostToDevice, s));
     }
     if (!b_dev) {
-        CHB_CUDA(cudaMalloc(&dB, std::max<size_t>(bbytes, 16)));
+        if (!(dB = staging(1, std::max<size_t>(bbytes, 16)))) return CHAMELEON_ERR_OUT_OF_RESOURCES;
         CHB_CUDA(cudaMemcpyAsync(dB, B, bbytes, cudaMemcpyHostToDevice, s));
     }
     CHAM_desc_t *dAd = nullptr, *dBd = nullptr;
@@ -723,8 +763,6 @@ static int lapack_call(int mode, cham_uplo_t uplo, int N, int NRHS, double *A, i
     if (!a_dev && (mode & MODE_FACT)) cudaMemcpyAsync(A, dA, abytes, cudaMemcpyDeviceToHost, s);
     if (!b_dev && (mode & MODE_SOLVE)) cudaMemcpyAsync(B, dB, bbytes, cudaMemcpyDeviceToHost, s);
     cudaStreamSynchronize(s);
-    if (!a_dev) cudaFree(dA);
-    if (!b_dev) cudaFree(dB);
     CHAMELEON_Desc_Destroy(&dAd);
     if (dBd) CHAMELEON_Desc_Destroy(&dBd);
     if (rc) return rc;
@@ -772,6 +810,35 @@ int CHAM_B200_dposv_timed(cham_uplo_t uplo, int N, int NRHS, double *A, int LDA,
     int rc = ensure_init();
     if (rc) return rc;
     return lapack_call(MODE_FACT | MODE_SOLVE, uplo, N, NRHS, A, LDA, B, LDB, device_ms);
+}
+
+// ---- measurement hooks (benchmark) ------------------------------------------
+// Device events on the library's stream: slot 0..7.
+static cudaEvent_t g_ev[8] = {};
+int CHAM_B200_Event_Record(int slot) {
+    if (ensure_init() || slot < 0 || slot >= 8) return CHAMELEON_ERR_ILLEGAL_VALUE;
+    if (!g_ev[slot]) CHB_CUDA(cudaEventCreate(&g_ev[slot]));
+    CHB_CUDA(cudaEventRecord(g_ev[slot], ctx().stream));
+    return 0;
+}
+float CHAM_B200_Event_Elapsed(int a, int b) {
+    if (a < 0 || b < 0 || a >= 8 || b >= 8 || !g_ev[a] || !g_ev[b]) return -1.f;
+    cudaEventSynchronize(g_ev[b]);
+    float ms = -1.f;
+    cudaEventElapsedTime(&ms, g_ev[a], g_ev[b]);
+    return ms;
+}
+unsigned long long CHAM_B200_Launch_Count(void) { return g_launch_count; }
+int CHAM_B200_Device_Sync(void) {
+    return cudaStreamSynchronize(ctx().stream) == cudaSuccess ? 0 : CHAMELEON_ERR_UNEXPECTED;
+}
+// Phase breakdown of the last mixed solve: out[7] = {factor, refine_solve,
+// residual, cast, total (ms), iterations, fallback}.
+int CHAM_B200_Mixed_Stats(double *out) {
+    const MixedStats &m = g_mixed_stats;
+    out[0] = m.factor_ms; out[1] = m.refine_solve_ms; out[2] = m.residual_ms; out[3] = m.cast_ms;
+    out[4] = m.total_ms; out[5] = m.iterations; out[6] = m.fallback;
+    return 0;
 }
 
 }  // extern "C"

@@ -24,6 +24,7 @@ namespace chb {
 // ---------------------------------------------------------------------------
 // Device
 // ---------------------------------------------------------------------------
+template <class T>
 struct Dims {
     const ExecParams &p;
     __device__ int tm(int m) const { return (m == p.NT - 1) ? p.N - m * p.NB : p.NB; }
@@ -34,12 +35,15 @@ struct Dims {
     }
     __device__ int wB(int bn) const { return (bn == p.NTB - 1) ? p.nrhs - bn * p.NBB : p.NBB; }
     // Logical lower tile (m,n), m >= n.
-    __device__ View A(int m, int n) const {
-        if (!p.upper) return View{p.A + p.a_off[m + p.NT * n], 1, p.a_ld[m]};
-        return View{p.A + p.a_off[n + p.NT * m], p.a_ld[n], 1};
+    __device__ ViewT<T> A(int m, int n) const {
+        T *a = static_cast<T *>(p.A);
+        if (!p.upper) return ViewT<T>{a + p.a_off[m + p.NT * n], 1, p.a_ld[m]};
+        return ViewT<T>{a + p.a_off[n + p.NT * m], p.a_ld[n], 1};
     }
-    __device__ View Bt(int m, int bn) const { return View{p.B + p.b_off[m + p.NT * bn], 1, p.b_ld[m]}; }
-    __device__ double *inv(int k) const { return p.invd + (int64_t)k * p.NIB * IB * IB; }
+    __device__ ViewT<T> Bt(int m, int bn) const {
+        return ViewT<T>{static_cast<T *>(p.B) + p.b_off[m + p.NT * bn], 1, p.b_ld[m]};
+    }
+    __device__ T *inv(int k) const { return static_cast<T *>(p.invd) + (int64_t)k * p.NIB * IB * IB; }
 };
 
 // Thread 0 only.  Returns false when the run aborted or the wait ran out.
@@ -61,7 +65,8 @@ __device__ bool wait_geq(const int *ctr, int target, const ExecParams &p, int ta
     }
 }
 
-__device__ bool task_wait(const Task &t, const ExecParams &p, const Dims &d, int ti) {
+template <class T>
+__device__ bool task_wait(const Task &t, const ExecParams &p, const Dims<T> &d, int ti) {
     const bool fact = p.mode & MODE_FACT;
     switch (t.kind) {
     case TK_POTRF:
@@ -92,28 +97,12 @@ __device__ bool task_wait(const Task &t, const ExecParams &p, const Dims &d, int
     return false;
 }
 
-// Invert the inner diagonal blocks of an existing factor L(k,k) (potrs alone).
-__device__ void tile_inv(const View &T, int n, double *invd, double *smem, int *flag) {
-    double *sD = smem + Cfg12864::SMEM_ELEMS;
-    double *sInv = sD + IB * LDD;
-    for (int jb = 0; jb < n; jb += IB) {
-        const int nbk = min(IB, n - jb);
-        for (int idx = threadIdx.x; idx < nbk * nbk; idx += NT_CTA) {
-            const int r = idx % nbk, c = idx / nbk;
-            if (r >= c) sD[r + c * LDD] = *T.at(jb + r, jb + c);
-        }
-        __syncthreads();
-        blk_inv(sD, sInv, nbk);
-        store_inv(invd + (int64_t)(jb / IB) * IB * IB, sInv);
-        __syncthreads();
-    }
-    (void)flag;
-}
-
-__device__ void run_task(const Task &t, const ExecParams &p, const Dims &d, double *smem, int *flag) {
+template <class T, int SP>
+__device__ void run_task(const Task &t, const ExecParams &p, const Dims<T> &d, T *smem) {
+    using VT = ViewT<T>;
     switch (t.kind) {
     case TK_POTRF: {
-        const int info = tile_potrf(d.A(t.k, t.k), d.tm(t.k), d.inv(t.k), smem);
+        const int info = tile_potrf<T, SP>(d.A(t.k, t.k), d.tm(t.k), d.inv(t.k), smem);
         if (info && threadIdx.x == 0) {
             atomicMin(&p.st->info, t.k * p.NB + info);
             atomicExch(&p.st->abort, 1);
@@ -121,34 +110,34 @@ __device__ void run_task(const Task &t, const ExecParams &p, const Dims &d, doub
         break;
     }
     case TK_INV:
-        tile_inv(d.A(t.k, t.k), d.tm(t.k), d.inv(t.k), smem, flag);
+        tile_inv<T>(d.A(t.k, t.k), d.tm(t.k), d.inv(t.k), smem);
         break;
     case TK_TRSM: {
         const int r0 = t.sub * SUBB;
         const int rows = min(SUBB, d.tm(t.m) - r0);
-        trsm_rows(d.A(t.m, t.k).sub(r0, 0), rows, d.A(t.k, t.k), d.tm(t.k), d.inv(t.k), smem);
+        trsm_rows<T, SP>(d.A(t.m, t.k).sub(r0, 0), rows, d.A(t.k, t.k), d.tm(t.k), d.inv(t.k), smem);
         break;
     }
     case TK_UPD: {
         const int bi = t.sub & 0xff, bj = (t.sub >> 8) & 0xff;
         const int rows = min(SUBB, d.tm(t.m) - bi * SUBB), cols = min(SUBB, d.tm(t.n) - bj * SUBB);
-        const View C = d.A(t.m, t.n).sub(bi * SUBB, bj * SUBB);
-        Acc<Cfg128> acc;
+        const VT C = d.A(t.m, t.n).sub(bi * SUBB, bj * SUBB);
+        Acc<Cfg128<T, SP>> acc;
         acc.zero();
         cta_gemm(acc, d.A(t.m, t.k).sub(bi * SUBB, 0), d.A(t.n, t.k).sub(bj * SUBB, 0), rows, cols,
                  d.tm(t.k), smem);
         const bool diag = (t.m == t.n) && (bi == bj);
-        acc.for_each([&](int r, int c, double v) {
+        acc.for_each([&](int r, int c, T v) {
             if (r < rows && c < cols && (!diag || r >= c)) *C.at(r, c) -= v;
         });
         break;
     }
     case TK_FWD_TRSM:
     case TK_BWD_TRSM: {
-        const View X = d.Bt(t.k, t.bn);
+        const VT X = d.Bt(t.k, t.bn);
         const int w = d.wB(t.bn);
         for (int c0 = 0; c0 < w; c0 += IB)
-            trsm_left(X.sub(0, c0), min(IB, w - c0), d.A(t.k, t.k), d.tm(t.k), d.inv(t.k),
+            trsm_left<T, SP>(X.sub(0, c0), min(IB, w - c0), d.A(t.k, t.k), d.tm(t.k), d.inv(t.k),
                       t.kind == TK_BWD_TRSM, smem);
         break;
     }
@@ -157,16 +146,16 @@ __device__ void run_task(const Task &t, const ExecParams &p, const Dims &d, doub
         const int r0 = t.sub * SUBB;
         const int rows = min(SUBB, d.tm(t.m) - r0);
         const int w = d.wB(t.bn);
-        const View Bm = d.Bt(t.m, t.bn).sub(r0, 0);
-        const View Bk = d.Bt(t.k, t.bn);
-        const View L = (t.kind == TK_FWD_UPD) ? d.A(t.m, t.k).sub(r0, 0) : d.A(t.k, t.m).t().sub(r0, 0);
+        const VT Bm = d.Bt(t.m, t.bn).sub(r0, 0);
+        const VT Bk = d.Bt(t.k, t.bn);
+        const VT L = (t.kind == TK_FWD_UPD) ? d.A(t.m, t.k).sub(r0, 0) : d.A(t.k, t.m).t().sub(r0, 0);
         for (int c0 = 0; c0 < w; c0 += 64) {
             const int wc = min(64, w - c0);
-            Acc<Cfg12864> acc;
+            Acc<Cfg12864<T, SP>> acc;
             acc.zero();
             cta_gemm(acc, L, Bk.sub(0, c0).t(), rows, wc, d.tm(t.k), smem);
-            const View Bc = Bm.sub(0, c0);
-            acc.for_each([&](int r, int c, double v) {
+            const VT Bc = Bm.sub(0, c0);
+            acc.for_each([&](int r, int c, T v) {
                 if (r < rows && c < wc) *Bc.at(r, c) -= v;
             });
         }
@@ -189,12 +178,13 @@ __device__ int *task_counter(const Task &t, const ExecParams &p) {
     return nullptr;
 }
 
+template <class T, int SP>
 __global__ void __launch_bounds__(NT_CTA, 1) cholesky_dag_kernel(ExecParams p) {
-    extern __shared__ __align__(128) double smem[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    T *smem = reinterpret_cast<T *>(smem_raw);
     __shared__ int s_task;
     __shared__ int s_ok;
-    __shared__ int s_flag;
-    const Dims d{p};
+    const Dims<T> d{p};
     while (true) {
         if (threadIdx.x == 0) {
             int ti = -1;
@@ -212,7 +202,7 @@ __global__ void __launch_bounds__(NT_CTA, 1) cholesky_dag_kernel(ExecParams p) {
         const Task t = p.tasks[ti];
         uint64_t t0 = 0;
         if (p.trace && threadIdx.x == 0) t0 = globaltimer();
-        run_task(t, p, d, smem, &s_flag);
+        run_task<T, SP>(t, p, d, smem);
         __threadfence();
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -468,8 +458,19 @@ int ensure_ws(size_t ctr_bytes, size_t inv_bytes) {
 TraceRec *g_trace_buf = nullptr;   // set by the tracing entry point (host-owned device buffer)
 int g_trace_cap = 0;
 
+template <class T, int SP>
+static int set_dag_smem() {
+    static bool done = false;
+    if (!done) {
+        CHB_CUDA(cudaFuncSetAttribute(cholesky_dag_kernel<T, SP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)tile_smem_bytes<T, SP>()));
+        done = true;
+    }
+    return 0;
+}
+
 int run_cholesky_dag(int mode, cham_uplo_t uplo, CHAM_desc_t *A, CHAM_desc_t *B, cudaStream_t s,
-                     ExecResult *res) {
+                     ExecResult *res, int split) {
     Context &c = ctx();
     const int N = A->n;
     const int NB = A->nb;
@@ -477,21 +478,23 @@ int run_cholesky_dag(int mode, cham_uplo_t uplo, CHAM_desc_t *A, CHAM_desc_t *B,
     const int nrhs = (B && (mode & MODE_SOLVE)) ? B->n : 0;
     const int NBB = B ? B->nb : NB;
     const int NTB = nrhs ? B->nt : 0;
+    const bool f32 = (A->dtyp == ChamRealFloat);
     res->info = 0; res->error = 0; res->ms = 0.f;
     if (N == 0) return 0;
-    static int smem_set = 0;
-    if (!smem_set) {
-        CHB_CUDA(cudaFuncSetAttribute(cholesky_dag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)TILE_KERNEL_SMEM_BYTES));
-        smem_set = 1;
-    }
+    if (nrhs && B->dtyp != A->dtyp) return CHAMELEON_ERR_ILLEGAL_VALUE;
+    int rc = 0;
+    if (!f32) rc = set_dag_smem<double, SPLIT_BF16X3>();
+    else if (split == SPLIT_TF32X3) rc = set_dag_smem<float, SPLIT_TF32X3>();
+    else rc = set_dag_smem<float, SPLIT_BF16X3>();
+    if (rc) return rc;
     const int grid = c.num_sms;
     Shape sh{mode, N, NB, nrhs, NBB, grid};
     Schedule *sch = get_schedule(sh);
     if (!sch) return CHAMELEON_ERR_OUT_OF_RESOURCES;
     const int NIB = (NB + IB - 1) / IB;
     const size_t nctr = (size_t)2 * NT * NT + (size_t)4 * NT * std::max(NTB, 1);
-    int rc = ensure_ws(nctr * sizeof(int), (size_t)NT * NIB * IB * IB * sizeof(double));
+    const size_t esz = f32 ? sizeof(float) : sizeof(double);
+    rc = ensure_ws(nctr * sizeof(int), (size_t)NT * NIB * IB * IB * esz);
     if (rc) return rc;
     int rcA = desc_upload(A);
     if (rcA) return rcA;
@@ -505,11 +508,11 @@ int run_cholesky_dag(int mode, cham_uplo_t uplo, CHAM_desc_t *A, CHAM_desc_t *B,
     p.mode = mode;
     p.upper = (uplo == ChamUpper);
     p.NT = NT; p.N = N; p.NB = NB;
-    p.A = (double *)A->mat;
+    p.A = A->mat;
     p.a_off = priv(A)->dev.off;
     p.a_ld = priv(A)->dev.ld;
     p.NTB = NTB; p.nrhs = nrhs; p.NBB = NBB;
-    p.B = nrhs ? (double *)B->mat : nullptr;
+    p.B = nrhs ? B->mat : nullptr;
     p.b_off = nrhs ? priv(B)->dev.off : nullptr;
     p.b_ld = nrhs ? priv(B)->dev.ld : nullptr;
     int *ctr = (int *)g_ws.ctr;
@@ -531,8 +534,15 @@ int run_cholesky_dag(int mode, cham_uplo_t uplo, CHAM_desc_t *A, CHAM_desc_t *B,
     CHB_CUDA(cudaMemsetAsync(ctr, 0, nctr * sizeof(int), s));
     CHB_CUDA(cudaMemcpyAsync(g_ws.st, &init, sizeof(init), cudaMemcpyHostToDevice, s));
     CHB_CUDA(cudaEventRecord(g_ws.e0, s));
-    if (p.ntasks > 0)
-        cholesky_dag_kernel<<<grid, NT_CTA, TILE_KERNEL_SMEM_BYTES, s>>>(p);
+    if (p.ntasks > 0) {
+        CHB_LAUNCHED(1);
+        if (!f32)
+            cholesky_dag_kernel<double, SPLIT_BF16X3><<<grid, NT_CTA, tile_smem_bytes<double>(), s>>>(p);
+        else if (split == SPLIT_TF32X3)
+            cholesky_dag_kernel<float, SPLIT_TF32X3><<<grid, NT_CTA, tile_smem_bytes<float, SPLIT_TF32X3>(), s>>>(p);
+        else
+            cholesky_dag_kernel<float, SPLIT_BF16X3><<<grid, NT_CTA, tile_smem_bytes<float, SPLIT_BF16X3>(), s>>>(p);
+    }
     CHB_CUDA(cudaGetLastError());
     CHB_CUDA(cudaEventRecord(g_ws.e1, s));
     ExecState out{};

@@ -57,15 +57,15 @@ struct ExecParams {
     int mode;
     int upper;
     int NT, N, NB;          // A: NT x NT tiles, order N, tile size NB (square tiles)
-    double *A;
+    void *A;                // double or float tiles
     const int64_t *a_off;   // element offset of tile (m,n) at a_off[m + NT*n]
     const int *a_ld;        // leading dimension of tile row m
     int NTB, nrhs, NBB;     // B: NT x NTB tiles of NB x NBB
-    double *B;
+    void *B;
     const int64_t *b_off;   // b_off[m + NT*bn]
     const int *b_ld;
     int *updA, *panA, *fwdB, *fwdDone, *bwdB, *bwdDone;
-    double *invd;           // NT * NIB inverted IB x IB blocks
+    void *invd;             // NT * NIB inverted IB x IB blocks (element type of A)
     int NIB;
     ExecState *st;
     TraceRec *trace;        // optional per-task trace (nullptr: off)

@@ -32,6 +32,22 @@ struct Context {
 };
 Context &ctx();
 
+// Count of this library's kernel launches (reported by the benchmark).
+extern unsigned long long g_launch_count;
+#define CHB_LAUNCHED(n) (::chb::g_launch_count += (n))
+
+// Phase breakdown of the last mixed-precision solve (device times, ms).
+struct MixedStats {
+    float factor_ms = 0;        // FP32 factorization + first solve (one DAG launch)
+    float refine_solve_ms = 0;  // correction solves
+    float residual_ms = 0;      // FP64 residuals
+    float cast_ms = 0;          // casts + norm
+    float total_ms = 0;
+    int iterations = 0;
+    int fallback = 0;
+};
+extern MixedStats g_mixed_stats;
+
 #define CHB_CUDA(call)                                                                 \
     do {                                                                               \
         cudaError_t _e = (call);                                                       \
@@ -64,6 +80,7 @@ int desc_upload(CHAM_desc_t *d);
 // tile size nb: tile (m,n) at A + m*nb + n*nb*lda (control/descriptor.h:238-252).
 int desc_create_cm(CHAM_desc_t **desc, double *dA, int lda, int m, int n, int nb);
 int desc_sync_to_host(CHAM_desc_t *d);
+double *staging(int slot, size_t bytes);   // LAPACK-layout staging buffers (0: A, 1: B, 2: X)
 
 // Executor entry (executor.cu).
 struct ExecResult {
@@ -71,7 +88,9 @@ struct ExecResult {
     int error = 0;    // CHAMELEON_ERR_*
     float ms = 0.f;   // device time of the launch
 };
+// A, B: double descriptors (FP64 path) or float descriptors (split-precision
+// path, `split` = SPLIT_BF16X3 or SPLIT_TF32X3 from core.cuh).
 int run_cholesky_dag(int mode, cham_uplo_t uplo, CHAM_desc_t *A, CHAM_desc_t *B, cudaStream_t s,
-                     ExecResult *res);
+                     ExecResult *res, int split = 0);
 
 }  // namespace chb

@@ -1,0 +1,547 @@
+// mixed.cu -- mixed-precision Cholesky solve with FP64 iterative refinement.
+//
+// The reference has no working mixed solver: zcposv / zcgesv are commented out
+// of its build (compute/CMakeLists.txt:211-212, include/chameleon/chameleon_zc.h
+// :33-42); only the tile casts chameleon_pzlag2c / pclag2z exist
+// (compute/pzlag2c.c:33-104).  This file restates LAPACK's dsposv scheme (the
+// CPU comparator, LAPACKE_dsposv) on the B200 path:
+//
+//   A32 = float(A)                        (tile cast, overflow -> FP64 fallback)
+//   L32 = chol(A32)                       (tile-DAG executor, FP32 storage,
+//                                          BF16x3 or TF32x3 tensor-core GEMMs)
+//   X   = double(L32^-T L32^-1 float(B))
+//   repeat: R = B - A X (FP64, DMMA)      converged when, for every column,
+//           max|R| <= max|X| * ||A||_inf * eps * sqrt(N)   (dsposv's test)
+//           X += double(L32^-T L32^-1 float(R))
+//   after REFINE_MAXITER iterations without convergence: FP64 dposv on A.
+//
+// ITER follows LAPACK: >= 0 iterations used; -2 overflow in the cast; -3 the
+// low-precision factorization failed; -(maxiter+1) refinement did not
+// converge.  On fallback A holds the FP64 factor (as in dsposv).
+#include <cuda_runtime.h>
+#include <math.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "core.cuh"
+#include "internal.h"
+
+namespace chb {
+
+struct TileMapD {
+    void *base;
+    const int64_t *off;
+    const int *ld;
+    int mt, mb, nb;
+    template <class T>
+    __device__ T *at(int i, int j) const {
+        const int m = i / mb, n = j / nb;
+        return static_cast<T *>(base) + off[m + (int64_t)mt * n] + (i - m * mb) + (int64_t)(j - n * nb) * ld[m];
+    }
+};
+
+// Device tile map of a descriptor.  Its offset table must be on the device
+// already (desc_upload); every workspace descriptor is uploaded at creation.
+static TileMapD tmap(CHAM_desc_t *d) {
+    return TileMapD{d->mat, priv(d)->dev.off, priv(d)->dev.ld, d->mt, d->mb, d->nb};
+}
+static bool uploaded(const CHAM_desc_t *d) { return priv(d)->dev.off != nullptr && priv(d)->dev.ld != nullptr; }
+
+// Flat cast of tile storage with identical layout (CCRB -> CCRB, same tiling):
+// element offsets coincide, so the cast is one coalesced pass over the storage.
+__global__ void cast_d2s_flat(const double *__restrict__ src, float *__restrict__ dst, size_t n, int *overflow) {
+    size_t i = (blockIdx.x * (size_t)blockDim.x + threadIdx.x) * 4;
+    const size_t stride = (size_t)gridDim.x * blockDim.x * 4;
+    int ovf = 0;
+    for (; i + 3 < n; i += stride) {
+        const double2 a = *reinterpret_cast<const double2 *>(src + i);
+        const double2 b = *reinterpret_cast<const double2 *>(src + i + 2);
+        ovf |= (fabs(a.x) > 3.4028234663852886e38) | (fabs(a.y) > 3.4028234663852886e38) |
+               (fabs(b.x) > 3.4028234663852886e38) | (fabs(b.y) > 3.4028234663852886e38);
+        *reinterpret_cast<float4 *>(dst + i) =
+            make_float4(__double2float_rn(a.x), __double2float_rn(a.y), __double2float_rn(b.x), __double2float_rn(b.y));
+    }
+    for (; i < n; ++i) {   // tail (only the last thread range)
+        ovf |= fabs(src[i]) > 3.4028234663852886e38;
+        dst[i] = __double2float_rn(src[i]);
+    }
+    if (ovf && overflow) *overflow = 1;
+}
+
+// Generic element-wise cast through the two tile maps (any layouts).
+template <class S, class D>
+__global__ void cast_tiles(TileMapD s, TileMapD d, int M, int N, int *overflow) {
+    const int64_t total = (int64_t)M * N;
+    int ovf = 0;
+    for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
+         idx += (int64_t)gridDim.x * blockDim.x) {
+        const int i = (int)(idx % M), j = (int)(idx / M);
+        const double v = (double)*s.at<S>(i, j);
+        if (overflow) ovf |= fabs(v) > 3.4028234663852886e38;
+        *d.at<D>(i, j) = (D)v;
+    }
+    if (ovf && overflow) *overflow = 1;
+}
+
+// X += double(D) on N x nrhs tile-layout operands.
+__global__ void add_correction(TileMapD x, TileMapD d, int M, int N) {
+    const int64_t total = (int64_t)M * N;
+    for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
+         idx += (int64_t)gridDim.x * blockDim.x) {
+        const int i = (int)(idx % M), j = (int)(idx / M);
+        *x.at<double>(i, j) += (double)*d.at<float>(i, j);
+    }
+}
+
+// Logical lower tile (m,n), m >= n, of a symmetric matrix stored in `uplo`.
+struct SymTiles {
+    double *A;
+    const int64_t *off;
+    const int *ld;
+    int NT, N, NB, upper;
+    __device__ int tm(int m) const { return (m == NT - 1) ? N - m * NB : NB; }
+    __device__ View L(int m, int n) const {
+        if (!upper) return View{A + off[m + NT * n], 1, ld[m]};
+        return View{A + off[n + NT * m], ld[n], 1};
+    }
+};
+
+// R = B - A X for symmetric A (one triangle stored), FP64 on DMMA.  One CTA
+// per (tile row m, 128-row block, 64-column block of the right-hand sides);
+// it sweeps the whole block row of A.  Also records per-column max |R|.
+__global__ void __launch_bounds__(NT_CTA, 1) sym_residual_kernel(SymTiles a, TileMapD xb, TileMapD bb, TileMapD rb,
+                                                                 int nrhs, int nrb, int ncb,
+                                                                 unsigned long long *rmax) {
+    extern __shared__ __align__(128) double smem[];
+    const int task = blockIdx.x;
+    const int cb = task % ncb;            // 64-column block, aligned to the tile columns of X
+    const int mr = task / ncb;            // (m, row block) flattened
+    const int m = mr / nrb, rblk = mr % nrb;
+    const int r0 = rblk * 128;
+    if (m >= a.NT || r0 >= a.tm(m)) return;
+    const int rows = min(128, a.tm(m) - r0);
+    const int per_tile = (xb.nb + 63) / 64;
+    const int bn = cb / per_tile;
+    const int c0 = bn * xb.nb + (cb % per_tile) * 64;
+    const int w = min(min(64, (bn + 1) * xb.nb - c0), nrhs - c0);
+    if (w <= 0) return;
+    Acc<Cfg12864<double>> acc;
+    acc.zero();
+    for (int n = 0; n < a.NT; ++n) {
+        const View An = (n <= m) ? a.L(m, n).sub(r0, 0) : a.L(n, m).t().sub(r0, 0);
+        // X tile n, columns c0..c0+w: view of the N x nrhs operand in tile layout
+        double *xp = xb.at<double>(n * a.NB, c0);
+        const View Xn{xp, 1, xb.ld[n]};
+        cta_gemm(acc, An, Xn.t(), rows, w, a.tm(n), smem);
+    }
+    __shared__ unsigned long long cmax[64];
+    if (threadIdx.x < 64) cmax[threadIdx.x] = 0ull;
+    __syncthreads();
+    const int gi0 = m * a.NB + r0;
+    acc.for_each([&](int r, int c, double v) {
+        if (r < rows && c < w) {
+            const double res = *bb.at<double>(gi0 + r, c0 + c) - v;
+            *rb.at<double>(gi0 + r, c0 + c) = res;
+            atomicMax(&cmax[c], (unsigned long long)__double_as_longlong(fabs(res)));
+        }
+    });
+    __syncthreads();
+    if (threadIdx.x < w) atomicMax(&rmax[c0 + threadIdx.x], cmax[threadIdx.x]);
+}
+
+// Per-column max |X| of an N x nrhs operand.
+__global__ void colmax_kernel(TileMapD x, int M, int N, unsigned long long *out) {
+    const int64_t total = (int64_t)M * N;
+    for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
+         idx += (int64_t)gridDim.x * blockDim.x) {
+        const int i = (int)(idx % M), j = (int)(idx / M);
+        atomicMax(&out[j], (unsigned long long)__double_as_longlong(fabs(*x.at<double>(i, j))));
+    }
+}
+
+// Infinity norm of the symmetric matrix (= one norm): per lower tile, row sums
+// (thread per row, coalesced) feed the columns of the mirrored part and column
+// sums (thread per column) feed the tile's own columns.
+__global__ void sym_absnorm_kernel(SymTiles a, double *colsum) {
+    int t = blockIdx.x;
+    int m = 0;
+    while (t > m) { t -= m + 1; ++m; }   // t-th lower tile in row-major order
+    const int n = t;
+    const View L = a.L(m, n);
+    const int rm = a.tm(m), cn = a.tm(n);
+    const bool diag = (m == n);
+    for (int i = threadIdx.x; i < rm; i += blockDim.x) {
+        double s = 0.0;
+        const int jmax = diag ? i : cn;          // strictly lower part of the row
+        for (int j = 0; j < jmax; ++j) s += fabs(*L.at(i, j));
+        if (s != 0.0) atomicAdd(&colsum[m * a.NB + i], s);
+    }
+    for (int j = threadIdx.x; j < cn; j += blockDim.x) {
+        double s = 0.0;
+        for (int i = diag ? j : 0; i < rm; ++i) s += fabs(*L.at(i, j));
+        atomicAdd(&colsum[n * a.NB + j], s);
+    }
+}
+
+static int ew_grid(int64_t total) {
+    const int64_t b = (total + 255) / 256;
+    return (int)std::min<int64_t>(std::max<int64_t>(b, 1), (int64_t)ctx().num_sms * 16);
+}
+
+namespace {
+struct MixedWs {
+    CHAM_desc_t *A32 = nullptr, *B32 = nullptr, *R = nullptr;
+    int N = -1, NB = -1, nrhs = -1;
+    unsigned long long *rmax = nullptr, *xmax = nullptr;
+    double *colsum = nullptr;
+    int *flag = nullptr;
+    int cap_rhs = 0, cap_n = 0;
+};
+MixedWs g_mws;
+
+int mixed_reserve(int N, int NB, int nrhs) {
+    if (g_mws.N != N || g_mws.NB != NB) {
+        if (g_mws.A32) CHAMELEON_Desc_Destroy(&g_mws.A32);
+        int rc = CHAMELEON_Desc_Create(&g_mws.A32, CHAMELEON_MAT_ALLOC_TILE, ChamRealFloat, NB, NB, NB * NB, N, N, 0,
+                                       0, N, N, 1, 1);
+        if (rc) return rc;
+        if ((rc = desc_upload(g_mws.A32))) return rc;
+        g_mws.N = N;
+        g_mws.NB = NB;
+        g_mws.nrhs = -1;
+    }
+    if (g_mws.nrhs != nrhs) {
+        if (g_mws.B32) CHAMELEON_Desc_Destroy(&g_mws.B32);
+        if (g_mws.R) CHAMELEON_Desc_Destroy(&g_mws.R);
+        int rc = CHAMELEON_Desc_Create(&g_mws.B32, CHAMELEON_MAT_ALLOC_TILE, ChamRealFloat, NB, NB, NB * NB, N, nrhs,
+                                       0, 0, N, nrhs, 1, 1);
+        if (!rc)
+            rc = CHAMELEON_Desc_Create(&g_mws.R, CHAMELEON_MAT_ALLOC_TILE, ChamRealDouble, NB, NB, NB * NB, N, nrhs, 0,
+                                       0, N, nrhs, 1, 1);
+        if (rc) return rc;
+        if ((rc = desc_upload(g_mws.B32)) || (rc = desc_upload(g_mws.R))) return rc;
+        g_mws.nrhs = nrhs;
+    }
+    if (nrhs > g_mws.cap_rhs) {
+        if (g_mws.rmax) cudaFree(g_mws.rmax);
+        if (g_mws.xmax) cudaFree(g_mws.xmax);
+        CHB_CUDA(cudaMalloc(&g_mws.rmax, nrhs * sizeof(unsigned long long)));
+        CHB_CUDA(cudaMalloc(&g_mws.xmax, nrhs * sizeof(unsigned long long)));
+        g_mws.cap_rhs = nrhs;
+    }
+    if (N > g_mws.cap_n) {
+        if (g_mws.colsum) cudaFree(g_mws.colsum);
+        CHB_CUDA(cudaMalloc(&g_mws.colsum, N * sizeof(double)));
+        g_mws.cap_n = N;
+    }
+    if (!g_mws.flag) CHB_CUDA(cudaMalloc(&g_mws.flag, sizeof(int)));
+    return 0;
+}
+
+bool g_res_attr = false;
+}  // namespace
+
+static SymTiles symtiles(CHAM_desc_t *A, cham_uplo_t uplo) {
+    return SymTiles{(double *)A->mat, priv(A)->dev.off, priv(A)->dev.ld, A->nt, A->n, A->nb, uplo == ChamUpper};
+}
+
+double sym_norm_inf(CHAM_desc_t *A, cham_uplo_t uplo, cudaStream_t s) {
+    if (desc_upload(A) || mixed_reserve(A->n, A->nb, std::max(1, g_mws.nrhs))) return -1.0;
+    const int NT = A->nt;
+    cudaMemsetAsync(g_mws.colsum, 0, A->n * sizeof(double), s);
+    sym_absnorm_kernel<<<NT * (NT + 1) / 2, 256, 0, s>>>(symtiles(A, uplo), g_mws.colsum);
+    CHB_LAUNCHED(1);
+    std::vector<double> h(A->n);
+    cudaMemcpyAsync(h.data(), g_mws.colsum, A->n * sizeof(double), cudaMemcpyDeviceToHost, s);
+    cudaStreamSynchronize(s);
+    double r = 0;
+    for (double v : h) r = std::max(r, v);
+    return r;
+}
+
+// R = B - A X and the per-column max |R|, max |X| (host copies).
+static int residual(CHAM_desc_t *A, cham_uplo_t uplo, CHAM_desc_t *B, CHAM_desc_t *X, cudaStream_t s,
+                    std::vector<double> &rn, std::vector<double> &xn) {
+    if (!uploaded(A) || !uploaded(B) || !uploaded(X) || !uploaded(g_mws.R)) return CHAMELEON_ERR_UNEXPECTED;
+    if (!g_res_attr) {
+        CHB_CUDA(cudaFuncSetAttribute(sym_residual_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)Cfg12864<double>::SMEM_BYTES));
+        g_res_attr = true;
+    }
+    const int nrhs = B->n;
+    const int nrb = (A->nb + 127) / 128;
+    const int ncb = X->nt * ((X->nb + 63) / 64);
+    CHB_CUDA(cudaMemsetAsync(g_mws.rmax, 0, nrhs * sizeof(unsigned long long), s));
+    CHB_CUDA(cudaMemsetAsync(g_mws.xmax, 0, nrhs * sizeof(unsigned long long), s));
+    sym_residual_kernel<<<A->nt * nrb * ncb, NT_CTA, Cfg12864<double>::SMEM_BYTES, s>>>(
+        symtiles(A, uplo), tmap(X), tmap(B), tmap(g_mws.R), nrhs, nrb, ncb, g_mws.rmax);
+    colmax_kernel<<<ew_grid((int64_t)X->m * nrhs), 256, 0, s>>>(tmap(X), X->m, nrhs, g_mws.xmax);
+    CHB_LAUNCHED(2);
+    CHB_CUDA(cudaGetLastError());
+    std::vector<unsigned long long> hr(nrhs), hx(nrhs);
+    CHB_CUDA(cudaMemcpyAsync(hr.data(), g_mws.rmax, nrhs * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+    CHB_CUDA(cudaMemcpyAsync(hx.data(), g_mws.xmax, nrhs * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+    CHB_CUDA(cudaStreamSynchronize(s));
+    rn.resize(nrhs);
+    xn.resize(nrhs);
+    for (int j = 0; j < nrhs; ++j) {
+        memcpy(&rn[j], &hr[j], 8);
+        memcpy(&xn[j], &hx[j], 8);
+    }
+    return 0;
+}
+
+static bool converged(const std::vector<double> &rn, const std::vector<double> &xn, double cte, double *berr) {
+    bool ok = true;
+    double b = 0;
+    for (size_t j = 0; j < rn.size(); ++j) {
+        if (!(rn[j] <= xn[j] * cte)) ok = false;
+        if (xn[j] > 0) b = std::max(b, rn[j] / xn[j]);
+    }
+    if (berr) *berr = b;
+    return ok;
+}
+
+static int cast_desc(CHAM_desc_t *src, CHAM_desc_t *dst, cudaStream_t s, int *overflow_flag) {
+    if (desc_upload(src) || desc_upload(dst)) return CHAMELEON_ERR_UNEXPECTED;
+    const bool same_layout = !priv(src)->cm_view && !priv(dst)->cm_view && src->mb == dst->mb && src->nb == dst->nb &&
+                             src->lm == dst->lm && src->ln == dst->ln;
+    if (src->dtyp == ChamRealDouble && dst->dtyp == ChamRealFloat && same_layout) {
+        const size_t n = (size_t)src->lm * src->ln;
+        cast_d2s_flat<<<ctx().num_sms * 8, 256, 0, s>>>((const double *)src->mat, (float *)dst->mat, n,
+                                                      overflow_flag);
+    } else if (src->dtyp == ChamRealDouble && dst->dtyp == ChamRealFloat) {
+        cast_tiles<double, float><<<ew_grid((int64_t)src->m * src->n), 256, 0, s>>>(tmap(src), tmap(dst), src->m,
+                                                                                     src->n, overflow_flag);
+    } else if (src->dtyp == ChamRealFloat && dst->dtyp == ChamRealDouble) {
+        cast_tiles<float, double><<<ew_grid((int64_t)src->m * src->n), 256, 0, s>>>(tmap(src), tmap(dst), src->m,
+                                                                                     src->n, nullptr);
+    } else {
+        cast_tiles<double, double><<<ew_grid((int64_t)src->m * src->n), 256, 0, s>>>(tmap(src), tmap(dst), src->m,
+                                                                                      src->n, nullptr);
+    }
+    CHB_CUDA(cudaGetLastError());
+    CHB_LAUNCHED(1);
+    return 0;
+}
+
+// Accumulates the device time of host-delimited phases on one stream.
+struct PhaseClock {
+    cudaEvent_t a = nullptr, b = nullptr;
+    cudaStream_t s;
+    explicit PhaseClock(cudaStream_t st) : s(st) {
+        cudaEventCreate(&a);
+        cudaEventCreate(&b);
+    }
+    ~PhaseClock() {
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+    }
+    void tic() { cudaEventRecord(a, s); }
+    void toc(float &acc) {
+        cudaEventRecord(b, s);
+        cudaEventSynchronize(b);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, a, b);
+        acc += ms;
+    }
+};
+
+// The refinement driver.  A: FP64 (uplo triangle), B: N x nrhs FP64, X: output.
+int mixed_posv(cham_uplo_t uplo, int precision, CHAM_desc_t *A, CHAM_desc_t *B, CHAM_desc_t *X, int *iter_out,
+               CHAM_b200_refine_info_t *info) {
+    Context &c = ctx();
+    cudaStream_t s = c.stream;
+    const int N = A->n, nrhs = B->n, NB = A->nb;
+    int iter = 0;
+    CHAM_b200_refine_info_t inf{};
+    inf.precision = precision;
+    static cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (!e0) {
+        CHB_CUDA(cudaEventCreate(&e0));
+        CHB_CUDA(cudaEventCreate(&e1));
+    }
+    cudaEventRecord(e0, s);
+    int rc = 0;
+    ExecResult res;
+    bool fallback = (precision == CHAM_B200_PREC_FP64);
+    double berr = 0;
+    MixedStats st;
+    PhaseClock clk(s);
+    if (!fallback) {
+        if ((rc = mixed_reserve(N, NB, nrhs))) return rc;
+        if ((rc = desc_upload(A)) || (rc = desc_upload(B)) || (rc = desc_upload(X))) return rc;
+        clk.tic();
+        const double anrm = sym_norm_inf(A, uplo, s);
+        const double cte = anrm * 1.1102230246251565e-16 * sqrt((double)N);
+        const int split = (precision == CHAM_B200_PREC_FP32) ? SPLIT_TF32X3 : SPLIT_BF16X3;
+        CHB_CUDA(cudaMemsetAsync(g_mws.flag, 0, sizeof(int), s));
+        if ((rc = cast_desc(A, g_mws.A32, s, g_mws.flag))) return rc;
+        if ((rc = cast_desc(B, g_mws.B32, s, g_mws.flag))) return rc;
+        int ovf = 0;
+        CHB_CUDA(cudaMemcpyAsync(&ovf, g_mws.flag, sizeof(int), cudaMemcpyDeviceToHost, s));
+        clk.toc(st.cast_ms);
+        if (ovf) {
+            iter = -2;
+            fallback = true;
+        }
+        if (!fallback) {
+            if ((rc = run_cholesky_dag(MODE_FACT | MODE_SOLVE, uplo, g_mws.A32, g_mws.B32, s, &res, split))) return rc;
+            st.factor_ms += res.ms;
+            if (res.error) return res.error;
+            if (res.info) {
+                iter = -3;
+                fallback = true;
+            }
+        }
+        if (!fallback) {
+            if ((rc = cast_desc(g_mws.B32, X, s, nullptr))) return rc;
+            std::vector<double> rn, xn;
+            clk.tic();
+            if ((rc = residual(A, uplo, B, X, s, rn, xn))) return rc;
+            clk.toc(st.residual_ms);
+            bool ok = converged(rn, xn, cte, &berr);
+            int it = 0;
+            while (!ok && it < c.refine_maxiter) {
+                ++it;
+                if ((rc = cast_desc(g_mws.R, g_mws.B32, s, nullptr))) return rc;
+                if ((rc = run_cholesky_dag(MODE_SOLVE, uplo, g_mws.A32, g_mws.B32, s, &res, split))) return rc;
+                st.refine_solve_ms += res.ms;
+                if (res.error) return res.error;
+                if (!uploaded(X) || !uploaded(g_mws.B32)) return CHAMELEON_ERR_UNEXPECTED;
+                add_correction<<<ew_grid((int64_t)N * nrhs), 256, 0, s>>>(tmap(X), tmap(g_mws.B32), N, nrhs);
+                CHB_LAUNCHED(1);
+                CHB_CUDA(cudaGetLastError());
+                if ((rc = residual(A, uplo, B, X, s, rn, xn))) return rc;
+                ok = converged(rn, xn, cte, &berr);
+            }
+            if (ok) {
+                iter = it;
+            } else {
+                iter = -(c.refine_maxiter + 1);
+                fallback = true;
+            }
+        }
+    }
+    if (fallback) {
+        if ((rc = cast_desc(B, X, s, nullptr))) return rc;
+        if ((rc = run_cholesky_dag(MODE_FACT | MODE_SOLVE, uplo, A, X, s, &res))) return rc;
+        if (res.error) return res.error;
+        if (res.info) return res.info;
+        inf.fallback = (precision != CHAM_B200_PREC_FP64);
+        if (iter == 0 && precision == CHAM_B200_PREC_FP64) iter = 0;
+        berr = 0;
+    }
+    cudaEventRecord(e1, s);
+    cudaEventSynchronize(e1);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    st.total_ms = ms;
+    st.iterations = iter;
+    st.fallback = fallback ? 1 : 0;
+    g_mixed_stats = st;
+    inf.iterations = iter;
+    inf.backward_error = berr;
+    inf.seconds = ms * 1e-3;
+    if (iter_out) *iter_out = iter;
+    if (info) *info = inf;
+    if (fallback) desc_sync_to_host(A);
+    return desc_sync_to_host(X);
+}
+
+}  // namespace chb
+
+using namespace chb;
+
+extern "C" {
+
+static int check_mixed_args(CHAM_desc_t *A, CHAM_desc_t *B, CHAM_desc_t *X) {
+    if (!A || !B || !X) return CHAMELEON_ERR_ILLEGAL_VALUE;
+    if (A->dtyp != ChamRealDouble || B->dtyp != ChamRealDouble || X->dtyp != ChamRealDouble)
+        return CHAMELEON_ERR_ILLEGAL_VALUE;
+    if (A->m != A->n || A->mb != A->nb || B->m != A->n || X->m != A->n || B->n != X->n || B->mb != A->mb ||
+        X->mb != A->mb || X->nb != B->nb)
+        return CHAMELEON_ERR_ILLEGAL_VALUE;
+    return 0;
+}
+
+// Tile-layout dsposv (the reference's commented-out zcposv_Tile prototype,
+// include/chameleon/chameleon_zc.h:42, in d/s precision).
+int CHAMELEON_dsposv_Tile(cham_uplo_t uplo, CHAM_desc_t *A, CHAM_desc_t *B, CHAM_desc_t *X, int *ITER) {
+    int rc = ensure_init();
+    if (rc) return rc;
+    if (uplo != ChamUpper && uplo != ChamLower) return CHAMELEON_ERR_ILLEGAL_VALUE;
+    if ((rc = check_mixed_args(A, B, X))) return rc;
+    if (A->n == 0 || B->n == 0) return 0;
+    const int prec = ctx().precision == CHAM_B200_PREC_FP64 ? CHAM_B200_PREC_BF16X3 : ctx().precision;
+    return mixed_posv(uplo, prec, A, B, X, ITER, nullptr);
+}
+
+int CHAMELEON_B200_dposv_mixed_Tile(cham_uplo_t uplo, int precision, CHAM_desc_t *A, CHAM_desc_t *B,
+                                    CHAM_desc_t *X, CHAM_b200_refine_info_t *info) {
+    int rc = ensure_init();
+    if (rc) return rc;
+    if (uplo != ChamUpper && uplo != ChamLower) return CHAMELEON_ERR_ILLEGAL_VALUE;
+    if (precision < CHAM_B200_PREC_FP64 || precision > CHAM_B200_PREC_BF16X3) return CHAMELEON_ERR_ILLEGAL_VALUE;
+    if ((rc = check_mixed_args(A, B, X))) return rc;
+    if (A->n == 0 || B->n == 0) return 0;
+    return mixed_posv(uplo, precision, A, B, X, nullptr, info);
+}
+
+// LAPACK-layout dsposv (chameleon_zc.h:34 prototype, d/s precision): A, B, X
+// column-major host or device arrays.
+int CHAMELEON_dsposv(cham_uplo_t uplo, int N, int NRHS, double *A, int LDA, double *B, int LDB, double *X, int LDX,
+                     int *ITER) {
+    int rc = ensure_init();
+    if (rc) return rc;
+    if (uplo != ChamUpper && uplo != ChamLower) return -1;
+    if (N < 0) return -2;
+    if (NRHS < 0) return -3;
+    if (LDA < std::max(1, N)) return -5;
+    if (LDB < std::max(1, N)) return -7;
+    if (LDX < std::max(1, N)) return -9;
+    if (N == 0 || NRHS == 0) {
+        if (ITER) *ITER = 0;
+        return 0;
+    }
+    Context &c = ctx();
+    cudaStream_t s = c.stream;
+    cudaPointerAttributes at;
+    auto on_dev = [&](const void *p) {
+        if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
+    };
+    const bool ad = on_dev(A), bd = on_dev(B), xd = on_dev(X);
+    double *dA = A, *dB = B, *dX = X;
+    const size_t ab = (size_t)LDA * N * 8, bb = (size_t)LDB * NRHS * 8, xb = (size_t)LDX * NRHS * 8;
+    if (!ad) {
+        if (!(dA = staging(0, ab))) return CHAMELEON_ERR_OUT_OF_RESOURCES;
+        CHB_CUDA(cudaMemcpyAsync(dA, A, ab, cudaMemcpyHostToDevice, s));
+    }
+    if (!bd) {
+        if (!(dB = staging(1, bb))) return CHAMELEON_ERR_OUT_OF_RESOURCES;
+        CHB_CUDA(cudaMemcpyAsync(dB, B, bb, cudaMemcpyHostToDevice, s));
+    }
+    if (!xd && !(dX = staging(2, xb))) return CHAMELEON_ERR_OUT_OF_RESOURCES;
+    CHAM_desc_t *Ad, *Bd, *Xd;
+    desc_create_cm(&Ad, dA, LDA, N, N, c.tile_size);
+    desc_create_cm(&Bd, dB, LDB, N, NRHS, c.tile_size);
+    desc_create_cm(&Xd, dX, LDX, N, NRHS, c.tile_size);
+    const int prec = c.precision == CHAM_B200_PREC_FP64 ? CHAM_B200_PREC_BF16X3 : c.precision;
+    int iter = 0;
+    rc = mixed_posv(uplo, prec, Ad, Bd, Xd, &iter, nullptr);
+    if (ITER) *ITER = iter;
+    if (!xd) cudaMemcpyAsync(X, dX, xb, cudaMemcpyDeviceToHost, s);
+    if (!ad && iter < 0) cudaMemcpyAsync(A, dA, ab, cudaMemcpyDeviceToHost, s);
+    cudaStreamSynchronize(s);
+    CHAMELEON_Desc_Destroy(&Ad);
+    CHAMELEON_Desc_Destroy(&Bd);
+    CHAMELEON_Desc_Destroy(&Xd);
+    return rc;
+}
+
+}  // extern "C"

@@ -42,7 +42,7 @@ __global__ void __launch_bounds__(NT_CTA, 1) gemm_kernel(View A, View B, View C,
     if (tri == 2 && bi > bj) return;
     const int i0 = bi * 128, j0 = bj * 128;
     const int rows = min(128, M - i0), cols = min(128, N - j0);
-    Acc<Cfg128> acc;
+    Acc<Cfg128<double>> acc;
     acc.zero();
     cta_gemm(acc, A.sub(i0, 0), B.sub(j0, 0), rows, cols, K, smem);
     const View Cb = C.sub(i0, j0);
@@ -86,12 +86,12 @@ __global__ void __launch_bounds__(NT_CTA, 1) trsm_kernel(View L, int n, const do
                                                          int trans) {
     extern __shared__ __align__(128) double smem[];
     const int c0 = blockIdx.x * IB;
-    trsm_left(X.sub(0, c0), min(IB, w - c0), L, n, invd, trans != 0, smem);
+    trsm_left<double, SPLIT_BF16X3>(X.sub(0, c0), min(IB, w - c0), L, n, invd, trans != 0, smem);
 }
 
 __global__ void __launch_bounds__(NT_CTA, 1) potrf_kernel(View T, int n, double *invd, int *info) {
     extern __shared__ __align__(128) double smem[];
-    const int r = tile_potrf(T, n, invd, smem);
+    const int r = tile_potrf<double, SPLIT_BF16X3>(T, n, invd, smem);
     if (threadIdx.x == 0 && info) *info = r;
 }
 
@@ -155,8 +155,8 @@ static int ew_grid(int64_t total) {
 static bool smem_attr_done = false;
 static int set_smem_attrs() {
     if (smem_attr_done) return 0;
-    CHB_CUDA(cudaFuncSetAttribute(gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg128::SMEM_BYTES));
-    CHB_CUDA(cudaFuncSetAttribute(trsm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg64::SMEM_BYTES));
+    CHB_CUDA(cudaFuncSetAttribute(gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg128<double>::SMEM_BYTES));
+    CHB_CUDA(cudaFuncSetAttribute(trsm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg64<double>::SMEM_BYTES));
     CHB_CUDA(cudaFuncSetAttribute(potrf_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)TILE_KERNEL_SMEM_BYTES));
     CHB_CUDA(cudaFuncSetAttribute(inv_diag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -220,8 +220,9 @@ int CUDA_dgemm(cham_trans_t transa, cham_trans_t transb, int m, int n, int k, co
         scale_kernel<<<ew_grid((int64_t)m * n), 256, 0, handle->stream>>>(Cv, m, n, *beta);
     } else {
         dim3 grid((m + 127) / 128, (n + 127) / 128);
-        gemm_kernel<<<grid, NT_CTA, Cfg128::SMEM_BYTES, handle->stream>>>(Av, Bv, Cv, m, n, k, *alpha, *beta, 0);
+        gemm_kernel<<<grid, NT_CTA, Cfg128<double>::SMEM_BYTES, handle->stream>>>(Av, Bv, Cv, m, n, k, *alpha, *beta, 0);
     }
+    CHB_LAUNCHED(1);
     return cudaGetLastError() == cudaSuccess ? CHAMELEON_SUCCESS : CHAMELEON_ERR_UNEXPECTED;
 }
 
@@ -237,8 +238,9 @@ int CUDA_dsyrk(cham_uplo_t uplo, cham_trans_t trans, int n, int k, const double 
     const View Av = (trans == ChamNoTrans) ? View{const_cast<double *>(A), 1, lda} : View{const_cast<double *>(A), lda, 1};
     dim3 grid((n + 127) / 128, (n + 127) / 128);
     const View Cv{C, 1, ldc};
-    gemm_kernel<<<grid, NT_CTA, Cfg128::SMEM_BYTES, handle->stream>>>(Av, Av, Cv, n, n, k, (k == 0) ? 0.0 : *alpha,
+    gemm_kernel<<<grid, NT_CTA, Cfg128<double>::SMEM_BYTES, handle->stream>>>(Av, Av, Cv, n, n, k, (k == 0) ? 0.0 : *alpha,
                                                                      *beta, uplo == ChamLower ? 1 : 2);
+    CHB_LAUNCHED(1);
     return cudaGetLastError() == cudaSuccess ? CHAMELEON_SUCCESS : CHAMELEON_ERR_UNEXPECTED;
 }
 
@@ -264,8 +266,9 @@ int CUDA_dtrsm(cham_side_t side, cham_uplo_t uplo, cham_trans_t transa, cham_dia
     if (*alpha != 1.0) scale_kernel<<<ew_grid((int64_t)ns * w), 256, 0, handle->stream>>>(X, ns, w, *alpha);
     inv_diag_kernel<<<nblk, NT_CTA, 2 * IB * LDD * sizeof(double), handle->stream>>>(L, ns, handle->ws,
                                                                                      diag == ChamUnit);
-    trsm_kernel<<<(w + IB - 1) / IB, NT_CTA, Cfg64::SMEM_BYTES, handle->stream>>>(L, ns, handle->ws, X, w,
+    trsm_kernel<<<(w + IB - 1) / IB, NT_CTA, Cfg64<double>::SMEM_BYTES, handle->stream>>>(L, ns, handle->ws, X, w,
                                                                                  trans_eff);
+    CHB_LAUNCHED(3);
     return cudaGetLastError() == cudaSuccess ? CHAMELEON_SUCCESS : CHAMELEON_ERR_UNEXPECTED;
 }
 
@@ -286,6 +289,7 @@ int CUDA_dpotrf(cham_uplo_t uplo, int n, double *A, int lda, double *WORK, int l
     if (int rc = handle_ws(handle, (size_t)nblk * IB * IB * sizeof(double))) return rc;
     const View T = (uplo == ChamLower) ? View{A, 1, lda} : View{A, lda, 1};
     potrf_kernel<<<1, NT_CTA, TILE_KERNEL_SMEM_BYTES, handle->stream>>>(T, n, handle->ws, d_info);
+    CHB_LAUNCHED(1);
     return cudaGetLastError() == cudaSuccess ? CHAMELEON_SUCCESS : CHAMELEON_ERR_UNEXPECTED;
 }
 
@@ -294,6 +298,7 @@ int CUDA_dplgsy(const double *bump, int m, int n, double *A, int lda, int bigM, 
     if (!handle || !bump) return CHAMELEON_ERR_ILLEGAL_VALUE;
     if (m <= 0 || n <= 0) return 0;
     plgsy_tile_kernel<<<ew_grid((int64_t)m * n), 256, 0, handle->stream>>>(A, lda, m, n, *bump, bigM, m0, n0, seed);
+    CHB_LAUNCHED(1);
     return cudaGetLastError() == cudaSuccess ? CHAMELEON_SUCCESS : CHAMELEON_ERR_UNEXPECTED;
 }
 
@@ -302,6 +307,7 @@ int CUDA_dplrnt(int m, int n, double *A, int lda, int bigM, int m0, int n0, unsi
     if (!handle) return CHAMELEON_ERR_ILLEGAL_VALUE;
     if (m <= 0 || n <= 0) return 0;
     plrnt_tile_kernel<<<ew_grid((int64_t)m * n), 256, 0, handle->stream>>>(A, lda, m, n, bigM, m0, n0, seed);
+    CHB_LAUNCHED(1);
     return cudaGetLastError() == cudaSuccess ? CHAMELEON_SUCCESS : CHAMELEON_ERR_UNEXPECTED;
 }
 
@@ -313,6 +319,7 @@ int CUDA_dlag2s(int m, int n, const double *A, int lda, float *SA, int ldsa, cub
     if (ldsa < std::max(1, m)) return -6;
     if (m == 0 || n == 0) return 0;
     dlag2s_kernel<<<ew_grid((int64_t)m * n), 256, 0, handle->stream>>>(A, lda, SA, ldsa, m, n, handle->flag);
+    CHB_LAUNCHED(1);
     return cudaGetLastError() == cudaSuccess ? CHAMELEON_SUCCESS : CHAMELEON_ERR_UNEXPECTED;
 }
 
@@ -324,6 +331,7 @@ int CUDA_slag2d(int m, int n, const float *SA, int ldsa, double *A, int lda, cub
     if (lda < std::max(1, m)) return -6;
     if (m == 0 || n == 0) return 0;
     slag2d_kernel<<<ew_grid((int64_t)m * n), 256, 0, handle->stream>>>(SA, ldsa, A, lda, m, n);
+    CHB_LAUNCHED(1);
     return cudaGetLastError() == cudaSuccess ? CHAMELEON_SUCCESS : CHAMELEON_ERR_UNEXPECTED;
 }
 

@@ -201,6 +201,30 @@ double CHAMELEON_dlansy_Tile(cham_normtype_t norm, cham_uplo_t uplo, CHAM_desc_t
 double CHAMELEON_dlange_Tile(cham_normtype_t norm, CHAM_desc_t *A);
 
 /* ------------------------------------------------------------------------- */
+/* Mixed precision (new; in the spirit of the reference's commented-out      */
+/* zcposv, include/chameleon/chameleon_zc.h:33-42, and LAPACK dsposv)         */
+/* ------------------------------------------------------------------------- */
+typedef struct cham_b200_refine_info_s {
+    int    iterations;      /* refinement iterations taken (0: direct FP64) */
+    int    fallback;        /* 1 when refinement stalled and FP64 was used  */
+    int    precision;       /* CHAM_B200_PREC_* of the factorization used   */
+    double backward_error;  /* max_j ||b_j - A x_j||_inf / (||A||_inf ||x_j||_inf) */
+    double seconds;         /* device time of the whole solve               */
+} CHAM_b200_refine_info_t;
+
+/* A is FP64 and is not overwritten unless refinement fails (then, as in
+ * LAPACK dsposv, A holds the FP64 factor and ITER < 0); X receives the
+ * solution of A X = B.  ITER: iterations used (>= 0), -2 cast overflow, -3
+ * low-precision factorization failed, -(maxiter+1) no convergence. */
+int CHAMELEON_dsposv(cham_uplo_t uplo, int N, int NRHS, double *A, int LDA, double *B, int LDB, double *X,
+                     int LDX, int *ITER);
+int CHAMELEON_dsposv_Tile(cham_uplo_t uplo, CHAM_desc_t *A, CHAM_desc_t *B, CHAM_desc_t *X,
+                          int *iter);
+int CHAMELEON_B200_dposv_mixed_Tile(cham_uplo_t uplo, int precision, CHAM_desc_t *A,
+                                    CHAM_desc_t *B, CHAM_desc_t *X,
+                                    CHAM_b200_refine_info_t *info);
+
+/* ------------------------------------------------------------------------- */
 /* GPU tile-kernel ABI (gpucublas/include/gpucublas/gpucublas_z.h:36-61,      */
 /* gpucublas_zc.h:22-23 after z->d / zc->ds generation).  The cuBLAS and      */
 /* cuSOLVER handle types are opaque handles of this library carrying the      */

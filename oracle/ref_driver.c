@@ -141,10 +141,10 @@ int chamref_dposv_tile_seeded(int uplo, int N, int nrhs, int nb,
 }
 
 /*
- * CHAMELEON_dpotrf_batch_Tile (compute/zpotrf_batch.c:89) over `count`
- * contiguous n x n column-major matrices: descriptor of (count*n) x n with
- * mb = nb = n, whose tiles A(i,0) are the matrices (tile-major storage puts
- * tile i at offset i*n*n).
+ * CHAMELEON_dpotrf_batch_Tile (compute/zpotrf_batch.c:89) over `count` n x n
+ * matrices stacked in one column-major (count*n) x n array: a caller matrix
+ * is a column-major view (control/descriptor.c:183-199), and with mb = nb = n
+ * its tiles A(i,0) are the stacked matrices.
  */
 int chamref_dpotrf_batch(int uplo, int n, int count, double *mats, double *seconds)
 {
@@ -166,7 +166,9 @@ int chamref_dpotrf_batch(int uplo, int n, int count, double *mats, double *secon
     return rc;
 }
 
-/* CHAMELEON_dtrsm_batch_Tile (compute/ztrsm_batch.c:180): A tiles n x n, B tiles n x nrhs. */
+/* CHAMELEON_dtrsm_batch_Tile (compute/ztrsm_batch.c:180): stacked column-major
+ * A ((count*an) x an) and B ((count*bm) x bn); tile i of B is solved with
+ * tile i of A. */
 int chamref_dtrsm_batch(int side, int uplo, int trans, int diag, double alpha,
                         int n, int nrhs, int count, double *A, double *B)
 {

@@ -14,6 +14,8 @@ Fixtures (all small):
                      which the reference generated)
   * gen_37.npz    -- the reference's dplgsy (N=37, seed 51) and dplrnt
                      (37 x 3, seed 5673)
+  * batch_<uplo>.npz -- the reference's CHAMELEON_dpotrf_batch_Tile and
+                     CHAMELEON_dtrsm_batch_Tile on 6 matrices of order 40
   * posv_<uplo>_<N>_<NB>_<nrhs>.npz -- the reference's dposv on the
                      testing/input/posv.in-style odd sizes: A (full symmetric
                      input), B, factor F (uplo triangle) and solution X.
@@ -58,6 +60,22 @@ def main():
         tri = np.triu(F) if uplo == 121 else np.tril(F)
         np.savez_compressed(os.path.join(HERE, "posv_%d_%d_%d_%d.npz" % (uplo, N, NB, nrhs)),
                             A=A, B=B, F=tri, X=X, info=info)
+    import ctypes
+    L = O.reference()
+    n, count, nrhs = 40, 6, 3
+    for uplo in (121, 122):
+        # stacked column-major (count*n) x n array; tile i (mb = nb = n) is matrix i
+        A = np.asfortranarray(np.concatenate([O.ref_dplgsy(float(n), 123, n, 100 + i, n) for i in range(count)]))
+        Ain = A.copy()
+        t = ctypes.c_double()
+        assert L.chamref_dpotrf_batch(uplo, n, count, O._ptr(A), ctypes.byref(t)) == 0
+        B = np.asfortranarray(np.concatenate([O.ref_dplrnt(n, nrhs, 7 + i, n) for i in range(count)]))
+        Bin = B.copy()
+        # forward solve with the factors: op(T) lower-effective (L, or U^T)
+        trans = 112 if uplo == 121 else 111
+        assert L.chamref_dtrsm_batch(141, uplo, trans, 131, 1.0, n, nrhs, count, O._ptr(A), O._ptr(B)) == 0
+        np.savez_compressed(os.path.join(HERE, "batch_%d.npz" % uplo), A=Ain, F=A, B=Bin, Y=B, n=n, count=count,
+                            nrhs=nrhs, trans=trans)
     print("golden fixtures written to", HERE)
 
 

@@ -1,0 +1,106 @@
+"""GPU tests of the batch entry points.
+
+Uniform batches (CHAMELEON_dpotrf_batch_Tile / dtrsm_batch_Tile) are compared
+with the reference's own batch results (tests/golden/batch_*.npz, produced by
+the reference library); the uneven-size batch (no reference equivalent) is
+compared per matrix with the oracle and the reference's residual checks.
+"""
+import ctypes
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+
+pytestmark = pytest.mark.gpu
+EPS = 1.1102230246251565e-16
+
+
+@pytest.mark.parametrize("uplo", [121, 122])
+def test_potrf_trsm_batch_vs_reference_golden(cb, uplo):
+    import torch
+    g = np.load(os.path.join(GOLDEN, "batch_%d.npz" % uplo))
+    n, count, nrhs, trans = int(g["n"]), int(g["count"]), int(g["nrhs"]), int(g["trans"])
+    # caller matrices are column-major (count*n) x n / (count*n) x nrhs arrays on the device
+    tA = torch.from_numpy(g["A"].T.copy()).cuda()
+    tB = torch.from_numpy(g["B"].T.copy()).cuda()
+    dA = cb.Desc.create(count * n, n, n, mat=tA)
+    dB = cb.Desc.create(count * n, nrhs, n, nb=nrhs, mat=tB)
+    assert cb.lib().CHAMELEON_dpotrf_batch_Tile(uplo, dA.ptr) == 0
+    torch.cuda.synchronize()
+    F = tA.cpu().numpy().T
+    tri = np.triu if uplo == 121 else np.tril
+    for i in range(count):
+        blk = slice(i * n, (i + 1) * n)
+        assert np.abs(tri(F[blk]) - tri(g["F"][blk])).max() < 1e-12
+    assert cb.lib().CHAMELEON_dtrsm_batch_Tile(141, uplo, trans, 131, ctypes.c_double(1.0), dA.ptr, dB.ptr) == 0
+    torch.cuda.synchronize()
+    assert np.abs(tB.cpu().numpy().T - g["Y"]).max() < 1e-12
+
+
+@pytest.mark.parametrize("side", [141, 142])
+@pytest.mark.parametrize("uplo", [121, 122])
+@pytest.mark.parametrize("trans", [111, 112])
+def test_trsm_batch_all_variants(cb, side, uplo, trans):
+    import torch
+    n, w, count = 48, 20, 5
+    rng = np.random.default_rng(side + uplo + trans)
+    Ts = []
+    for i in range(count):
+        T = rng.standard_normal((n, n)) * 0.1 + 2 * np.eye(n)
+        Ts.append(np.triu(T) if uplo == 121 else np.tril(T))
+    A = np.asfortranarray(np.concatenate(Ts))
+    bm, bn = (n, w) if side == 141 else (w, n)
+    B = np.asfortranarray(rng.standard_normal((count * bm, bn)))
+    tA = torch.from_numpy(A.T.copy()).cuda()
+    tB = torch.from_numpy(B.T.copy()).cuda()
+    dA = cb.Desc.create(count * n, n, n, mat=tA)
+    dB = cb.Desc.create(count * bm, bn, bm, nb=bn, mat=tB)
+    assert cb.lib().CHAMELEON_dtrsm_batch_Tile(side, uplo, trans, 131, ctypes.c_double(2.0), dA.ptr, dB.ptr) == 0
+    torch.cuda.synchronize()
+    X = tB.cpu().numpy().T
+    for i in range(count):
+        op = Ts[i] if trans == 111 else Ts[i].T
+        Bi = B[i * bm:(i + 1) * bm]
+        ref = np.linalg.solve(op, 2 * Bi) if side == 141 else np.linalg.solve(op.T, 2 * Bi.T).T
+        assert np.abs(X[i * bm:(i + 1) * bm] - ref).max() < 1e-11
+
+
+def _uneven_batch(orc, count, nmin, nmax, rmax, seed):
+    rng = np.random.default_rng(seed)
+    ns = rng.integers(nmin, nmax + 1, count)
+    rs = rng.integers(1, rmax + 1, count)
+    As = [orc.dplgsy(float(n), int(n), 1000 + i) for i, n in enumerate(ns)]
+    Bs = [orc.dplrnt(int(n), int(r), 2000 + i) for i, (n, r) in enumerate(zip(ns, rs))]
+    return ns, rs, As, Bs
+
+
+@pytest.mark.parametrize("uplo", [121, 122])
+def test_uneven_batch_dposv(cb, orc, uplo):
+    import torch
+    ns, rs, As, Bs = _uneven_batch(orc, 300, 16, 512, 8, 2024)
+    a_off = np.cumsum([0] + [n * n for n in ns[:-1]]).astype(np.int64)
+    b_off = np.cumsum([0] + [n * r for n, r in zip(ns[:-1], rs[:-1])]).astype(np.int64)
+    A = np.concatenate([a.ravel(order="F") for a in As])
+    B = np.concatenate([b.ravel(order="F") for b in Bs])
+    As[17] = As[17].copy(); As[17][5, 5] = -1.0      # one matrix not SPD
+    A[a_off[17]:a_off[17] + ns[17] ** 2] = As[17].ravel(order="F")
+    dev = lambda x, dt=None: torch.from_numpy(np.ascontiguousarray(x)).cuda()
+    tA, tB = dev(A), dev(B)
+    tn, tr = dev(ns.astype(np.int32)), dev(rs.astype(np.int32))
+    ta, tb = dev(a_off), dev(b_off)
+    info = torch.zeros(len(ns), dtype=torch.int32, device="cuda")
+    p = lambda t: ctypes.c_void_p(t.data_ptr())
+    rc = cb.lib().CHAM_B200_dposv_batch(uplo, len(ns), p(tn), p(tr), p(tA), p(ta), p(tB), p(tb), p(info), None)
+    assert rc == 0
+    X = tB.cpu().numpy()
+    inf = info.cpu().numpy()
+    assert inf[17] == 6 and (np.delete(inf, 17) == 0).all()
+    for i, (n, r) in enumerate(zip(ns, rs)):
+        if i == 17:
+            continue
+        Xi = X[b_off[i]:b_off[i] + n * r].reshape((n, r), order="F")
+        R = Bs[i] - As[i] @ Xi
+        res = np.abs(R).sum(0).max() / (np.abs(As[i]).sum(0).max() * np.abs(Xi).sum(0).max() * n * EPS)
+        assert res < 60, (i, n, res)

@@ -1,0 +1,125 @@
+"""GPU tests of the mixed-precision solver (FP32 / BF16x3 factor + FP64 refinement).
+
+The reference has no mixed solver to compare with (zcposv is commented out of
+its build), so parity is pinned on the FP64 answer: the refined solution must
+pass the reference's solve check (threshold 60, testing/testing_zcheck_facto.c
+:430-438) and match the FP64 oracle solution to near machine precision (forward
+error), with LAPACK dsposv's ITER conventions for fallbacks.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+EPS = 1.1102230246251565e-16
+
+
+def np_check_solve(A0, X, B):
+    R = B - A0 @ X
+    return np.abs(R).sum(0).max() / (np.abs(A0).sum(0).max() * np.abs(X).sum(0).max() * A0.shape[0] * EPS)
+
+
+def spd_with_condition(N, cond, seed):
+    """Q diag(s) Q^T with s geometric from 1 down to 1/cond (seeded Gaussian QR)."""
+    rng = np.random.default_rng(seed)
+    Q, _ = np.linalg.qr(rng.standard_normal((N, N)))
+    s = np.geomspace(1.0, 1.0 / cond, N)
+    A = (Q * s) @ Q.T
+    return np.asfortranarray((A + A.T) / 2)
+
+
+def solve_mixed(cb, uplo, prec, A0, B0, NB):
+    N, nrhs = B0.shape
+    dA = cb.Desc.create(N, N, NB)
+    dB = cb.Desc.create(N, nrhs, NB)
+    dX = cb.Desc.create(N, nrhs, NB)
+    dA.from_numpy(A0)
+    dB.from_numpy(B0)
+    rc, info = cb.dposv_mixed_Tile(uplo, prec, dA, dB, dX)
+    return rc, info, dX.to_numpy(), dA.to_numpy()
+
+
+@pytest.mark.parametrize("prec", [2, 1])          # BF16x3, FP32 (TF32x3)
+@pytest.mark.parametrize("uplo", [121, 122])
+@pytest.mark.parametrize("N,NB,nrhs", [(1000, 256, 5), (2048, 320, 1), (3000, 512, 64), (37, 17, 3)])
+def test_mixed_refines_to_fp64_accuracy(cb, orc, prec, uplo, N, NB, nrhs):
+    A0 = orc.dplgsy(float(N), N, 51)
+    B0 = orc.dplrnt(N, nrhs, 5673)
+    rc, info, X, Aout = solve_mixed(cb, uplo, prec, A0, B0, NB)
+    assert rc == 0
+    assert 0 <= info.iterations <= 6 and info.fallback == 0
+    assert np_check_solve(A0, X, B0) < 60
+    Xr = np.linalg.solve(A0, B0)
+    assert np.abs(X - Xr).max() / np.abs(Xr).max() < 1e-14
+    assert np.array_equal(Aout, A0)          # A untouched when refinement succeeds
+
+
+@pytest.mark.parametrize("cond", [1e3, 1e6])
+def test_mixed_ill_conditioned_converges_or_falls_back(cb, cond):
+    N, NB, nrhs = 512, 128, 4
+    A0 = spd_with_condition(N, cond, 7)
+    rng = np.random.default_rng(3)
+    xt = rng.standard_normal((N, nrhs))
+    B0 = np.asfortranarray(A0 @ xt)
+    for prec in (2, 1):
+        rc, info, X, _ = solve_mixed(cb, 122, prec, A0, B0, NB)
+        assert rc == 0
+        assert np_check_solve(A0, X, B0) < 60
+        assert np.abs(X - xt).max() / np.abs(xt).max() < cond * 1e-13
+
+
+def test_mixed_fallback_when_refinement_stalls(cb):
+    N, NB = 400, 128
+    A0 = spd_with_condition(N, 1e12, 11)
+    B0 = np.asfortranarray(A0 @ np.ones((N, 2)))
+    cb.set_param(cb.CHAMELEON_B200_REFINE_MAXITER, 30)
+    rc, info, X, Aout = solve_mixed(cb, 122, 2, A0, B0, NB)
+    assert rc == 0
+    assert info.iterations < 0 and info.fallback == 1       # LAPACK dsposv: ITER < 0 on fallback
+    assert np_check_solve(A0, X, B0) < 60
+    L = np.tril(Aout)                                        # A holds the FP64 factor, as in dsposv
+    assert np.abs(L @ L.T - A0).max() < 1e-12 * np.abs(A0).max() * N
+
+
+def test_mixed_overflow_in_cast_falls_back(cb):
+    N, NB = 300, 128
+    A0 = np.asfortranarray(np.eye(N) * 1e39)
+    B0 = np.asfortranarray(np.ones((N, 1)) * 1e39)
+    rc, info, X, _ = solve_mixed(cb, 122, 2, A0, B0, NB)
+    assert rc == 0 and info.iterations == -2
+    assert np.allclose(X, 1.0)
+
+
+def test_mixed_not_spd_reports_info(cb, orc):
+    N, NB = 300, 128
+    A0 = orc.dplgsy(float(N), N, 2)
+    A0[150, 150] = -5.0
+    B0 = orc.dplrnt(N, 1, 3)
+    rc, info, X, _ = solve_mixed(cb, 122, 2, A0, B0, NB)
+    assert rc == 151
+
+
+@pytest.mark.parametrize("uplo", [121, 122])
+def test_dsposv_lapack_layout_host(cb, orc, uplo):
+    N, nrhs, LDA = 777, 6, 800
+    A0 = orc.dplgsy(float(N), N, 8)
+    B0 = orc.dplrnt(N, nrhs, 9)
+    A = np.zeros((LDA, N), order="F"); A[:N] = A0
+    B = np.zeros((LDA, nrhs), order="F"); B[:N] = B0
+    X = np.zeros((LDA, nrhs), order="F")
+    rc, it = cb.dsposv(uplo, N, nrhs, A, LDA, B, LDA, X, LDA)
+    assert rc == 0 and it >= 0
+    assert np_check_solve(A0, X[:N], B0) < 60
+    assert np.array_equal(A[:N], A0)
+
+
+def test_dsposv_tile_api(cb, orc):
+    N, NB, nrhs = 1500, 384, 3
+    dA = cb.Desc.create(N, N, NB)
+    dB = cb.Desc.create(N, nrhs, NB)
+    dX = cb.Desc.create(N, nrhs, NB)
+    cb.dplgsy_Tile(float(N), 122, dA, 51)
+    cb.dplrnt_Tile(dB, 5673)
+    rc, it = cb.dsposv_Tile(122, dA, dB, dX)
+    assert rc == 0 and it >= 0
+    A0 = orc.dplgsy(float(N), N, 51)
+    assert np_check_solve(A0, dX.to_numpy(), dB.to_numpy()) < 60
