@@ -30,6 +30,7 @@ CHAMELEON_B200_PRECISION = 101
 CHAMELEON_B200_REFINE_MAXITER = 102
 CHAMELEON_B200_WAIT_BUDGET_MS = 103
 CHAMELEON_B200_WAIT_BUDGET_US = 104
+CHAMELEON_B200_TCGEN05 = 105
 PREC_FP64, PREC_FP32, PREC_BF16X3 = 0, 1, 2
 CHAMELEON_SUCCESS = 0
 CHAMELEON_ERR_NOT_INITIALIZED = -101
@@ -145,6 +146,7 @@ EXTRAS = {
     "CHAM_B200_Launch_Count": (ctypes.c_ulonglong, []),
     "CHAM_B200_Device_Sync": (_i, []),
     "CHAM_B200_Mixed_Stats": (_i, [_dp]),
+    "CHAM_B200_Test_TC05": (_i, [_vp, _vp, _i, _vp]),
 }
 
 _lib = None

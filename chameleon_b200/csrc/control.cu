@@ -333,6 +333,9 @@ int CHAMELEON_Set(int param, int value) {
         if (value <= 0) return CHAMELEON_ERR_ILLEGAL_VALUE;
         c.wait_budget_us = value;
         return 0;
+    case CHAMELEON_B200_TCGEN05:
+        c.use_tcgen05 = (value != 0);
+        return 0;
     case CHAMELEON_TRANSLATION_MODE:
     case CHAMELEON_LOOKAHEAD:
     case CHAMELEON_CONCURRENCY:
@@ -351,6 +354,7 @@ int CHAMELEON_Get(int param, int *value) {
     case CHAMELEON_B200_REFINE_MAXITER: *value = c.refine_maxiter; return 0;
     case CHAMELEON_B200_WAIT_BUDGET_MS: *value = (int)(c.wait_budget_us / 1000); return 0;
     case CHAMELEON_B200_WAIT_BUDGET_US: *value = (int)std::min<long long>(c.wait_budget_us, INT_MAX); return 0;
+    case CHAMELEON_B200_TCGEN05: *value = c.use_tcgen05 ? 1 : 0; return 0;
     }
     return CHAMELEON_ERR_ILLEGAL_VALUE;
 }

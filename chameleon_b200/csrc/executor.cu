@@ -18,6 +18,7 @@
 
 #include "core.cuh"
 #include "internal.h"
+#include "tc05.cuh"
 
 namespace chb {
 
@@ -97,8 +98,15 @@ __device__ bool task_wait(const Task &t, const ExecParams &p, const Dims<T> &d, 
     return false;
 }
 
-template <class T, int SP>
-__device__ void run_task(const Task &t, const ExecParams &p, const Dims<T> &d, T *smem) {
+// Split chunks (hi/lo BF16, swizzled) of panel tile (m,k), m > k.
+__device__ __forceinline__ uint8_t *split_tile(const ExecParams &p, int m, int k) {
+    const size_t tile_bytes = (size_t)p.split_nrb * p.split_nkc * 2 * tc05::CHUNK_BYTES;
+    return p.split + ((size_t)m * (m - 1) / 2 + k) * tile_bytes;
+}
+
+template <class T, int SP, bool TC>
+__device__ void run_task(const Task &t, const ExecParams &p, const Dims<T> &d, T *smem, tc05::Smem *tsm,
+                         uint8_t *stage) {
     using VT = ViewT<T>;
     switch (t.kind) {
     case TK_POTRF: {
@@ -116,17 +124,43 @@ __device__ void run_task(const Task &t, const ExecParams &p, const Dims<T> &d, T
         const int r0 = t.sub * SUBB;
         const int rows = min(SUBB, d.tm(t.m) - r0);
         trsm_rows<T, SP>(d.A(t.m, t.k).sub(r0, 0), rows, d.A(t.k, t.k), d.tm(t.k), d.inv(t.k), smem);
+        if constexpr (TC) {
+            // emit the split-BF16 chunks of these 128 rows for the tcgen05 updates
+            const VT X = d.A(t.m, t.k).sub(r0, 0);
+            const int K = d.tm(t.k);
+            uint8_t *base = split_tile(p, t.m, t.k) + (size_t)t.sub * p.split_nkc * 2 * tc05::CHUNK_BYTES;
+            for (int idx = threadIdx.x; idx < 128 * K; idx += NT_CTA) {
+                const int r = idx % 128, c = idx / 128;
+                const float v = (r < rows) ? (float)*X.at(r, c) : 0.f;
+                tc05::split_store(base + (size_t)(c / tc05::BK) * 2 * tc05::CHUNK_BYTES, r, c % tc05::BK, v);
+            }
+            tc05::fence_proxy_async();
+            cta_sync_global();
+        }
         break;
     }
     case TK_UPD: {
         const int bi = t.sub & 0xff, bj = (t.sub >> 8) & 0xff;
         const int rows = min(SUBB, d.tm(t.m) - bi * SUBB), cols = min(SUBB, d.tm(t.n) - bj * SUBB);
         const VT C = d.A(t.m, t.n).sub(bi * SUBB, bj * SUBB);
+        const bool diag = (t.m == t.n) && (bi == bj);
+        if constexpr (TC) {
+            const size_t rbytes = (size_t)p.split_nkc * 2 * tc05::CHUNK_BYTES;
+            const uint8_t *a = split_tile(p, t.m, t.k) + bi * rbytes;
+            const uint8_t *b = split_tile(p, t.n, t.k) + bj * rbytes;
+            const bool ok = tc05::gemm_bf16x3(tsm, stage, a, b, p.split_nkc, [&](int r, int c, float v) {
+                if (r < rows && c < cols && (!diag || r >= c)) *C.at(r, c) -= v;
+            });
+            if (!ok && threadIdx.x == 0) {
+                atomicCAS(&p.st->error, 0, CHAMELEON_ERR_DEVICE_TIMEOUT);
+                atomicExch(&p.st->abort, 1);
+            }
+            break;
+        }
         Acc<Cfg128<T, SP>> acc;
         acc.zero();
         cta_gemm(acc, d.A(t.m, t.k).sub(bi * SUBB, 0), d.A(t.n, t.k).sub(bj * SUBB, 0), rows, cols,
                  d.tm(t.k), smem);
-        const bool diag = (t.m == t.n) && (bi == bj);
         acc.for_each([&](int r, int c, T v) {
             if (r < rows && c < cols && (!diag || r >= c)) *C.at(r, c) -= v;
         });
@@ -178,13 +212,17 @@ __device__ int *task_counter(const Task &t, const ExecParams &p) {
     return nullptr;
 }
 
-template <class T, int SP>
+template <class T, int SP, bool TC>
 __global__ void __launch_bounds__(NT_CTA, 1) cholesky_dag_kernel(ExecParams p) {
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    T *smem = reinterpret_cast<T *>(smem_raw);
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    // 1024-byte aligned base: the tcgen05 stages need it; other tasks share it
+    uint8_t *stage = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    T *smem = reinterpret_cast<T *>(stage);
     __shared__ int s_task;
     __shared__ int s_ok;
+    __shared__ tc05::Smem tsm;
     const Dims<T> d{p};
+    if constexpr (TC) tc05::init(&tsm);
     while (true) {
         if (threadIdx.x == 0) {
             int ti = -1;
@@ -202,7 +240,7 @@ __global__ void __launch_bounds__(NT_CTA, 1) cholesky_dag_kernel(ExecParams p) {
         const Task t = p.tasks[ti];
         uint64_t t0 = 0;
         if (p.trace && threadIdx.x == 0) t0 = globaltimer();
-        run_task<T, SP>(t, p, d, smem);
+        run_task<T, SP, TC>(t, p, d, smem, &tsm, stage);
         __threadfence();
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -215,6 +253,7 @@ __global__ void __launch_bounds__(NT_CTA, 1) cholesky_dag_kernel(ExecParams p) {
             }
         }
     }
+    if constexpr (TC) tc05::finish(&tsm);
 }
 
 // ---------------------------------------------------------------------------
@@ -424,6 +463,8 @@ Schedule *get_schedule(const Shape &s) {
 
 // Per-shape device workspace (counters, inverted blocks, state).
 struct Workspace {
+    uint8_t *split = nullptr;
+    size_t split_bytes = 0;
     size_t ctr_bytes = 0, inv_bytes = 0;
     void *ctr = nullptr;
     double *inv = nullptr;
@@ -458,12 +499,17 @@ int ensure_ws(size_t ctr_bytes, size_t inv_bytes) {
 TraceRec *g_trace_buf = nullptr;   // set by the tracing entry point (host-owned device buffer)
 int g_trace_cap = 0;
 
-template <class T, int SP>
+template <class T, int SP, bool TC>
+constexpr size_t dag_smem_bytes() {
+    return (TC && (size_t)tc05::SMEM_BYTES > tile_smem_bytes<T, SP>() + 1024) ? (size_t)tc05::SMEM_BYTES
+                                                                           : tile_smem_bytes<T, SP>() + 1024;
+}
+template <class T, int SP, bool TC>
 static int set_dag_smem() {
     static bool done = false;
     if (!done) {
-        CHB_CUDA(cudaFuncSetAttribute(cholesky_dag_kernel<T, SP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)tile_smem_bytes<T, SP>()));
+        CHB_CUDA(cudaFuncSetAttribute(cholesky_dag_kernel<T, SP, TC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)dag_smem_bytes<T, SP, TC>()));
         done = true;
     }
     return 0;
@@ -482,10 +528,15 @@ int run_cholesky_dag(int mode, cham_uplo_t uplo, CHAM_desc_t *A, CHAM_desc_t *B,
     res->info = 0; res->error = 0; res->ms = 0.f;
     if (N == 0) return 0;
     if (nrhs && B->dtyp != A->dtyp) return CHAMELEON_ERR_ILLEGAL_VALUE;
+    // tcgen05 trailing updates: FP32 factorization with BF16x3 products and
+    // 64-aligned tiles (the split chunks are 64 wide in k).
+    const bool tc = f32 && split == SPLIT_BF16X3 && (mode & MODE_FACT) && (NB % tc05::BK == 0) && NT > 1 &&
+                    c.use_tcgen05;
     int rc = 0;
-    if (!f32) rc = set_dag_smem<double, SPLIT_BF16X3>();
-    else if (split == SPLIT_TF32X3) rc = set_dag_smem<float, SPLIT_TF32X3>();
-    else rc = set_dag_smem<float, SPLIT_BF16X3>();
+    if (!f32) rc = set_dag_smem<double, SPLIT_BF16X3, false>();
+    else if (split == SPLIT_TF32X3) rc = set_dag_smem<float, SPLIT_TF32X3, false>();
+    else if (tc) rc = set_dag_smem<float, SPLIT_BF16X3, true>();
+    else rc = set_dag_smem<float, SPLIT_BF16X3, false>();
     if (rc) return rc;
     const int grid = c.num_sms;
     Shape sh{mode, N, NB, nrhs, NBB, grid};
@@ -528,6 +579,20 @@ int run_cholesky_dag(int mode, cham_uplo_t uplo, CHAM_desc_t *A, CHAM_desc_t *B,
     p.st = g_ws.st;
     p.trace = (g_trace_buf && g_trace_cap >= p.ntasks) ? g_trace_buf : nullptr;
     p.wait_budget_ns = (unsigned long long)c.wait_budget_us * 1000ull;
+    if (tc) {
+        p.split_nrb = (NB + SUBB - 1) / SUBB;
+        p.split_nkc = NB / tc05::BK;
+        const size_t tile_bytes = (size_t)p.split_nrb * p.split_nkc * 2 * tc05::CHUNK_BYTES;
+        const size_t bytes = (size_t)NT * (NT - 1) / 2 * tile_bytes;
+        if (bytes > g_ws.split_bytes) {
+            if (g_ws.split) cudaFree(g_ws.split);
+            g_ws.split = nullptr;
+            g_ws.split_bytes = 0;
+            CHB_CUDA(cudaMalloc(&g_ws.split, bytes));
+            g_ws.split_bytes = bytes;
+        }
+        p.split = g_ws.split;
+    }
     ExecState init{};
     init.info = INT_MAX;
     init.stuck_task = -1;
@@ -537,11 +602,17 @@ int run_cholesky_dag(int mode, cham_uplo_t uplo, CHAM_desc_t *A, CHAM_desc_t *B,
     if (p.ntasks > 0) {
         CHB_LAUNCHED(1);
         if (!f32)
-            cholesky_dag_kernel<double, SPLIT_BF16X3><<<grid, NT_CTA, tile_smem_bytes<double>(), s>>>(p);
+            cholesky_dag_kernel<double, SPLIT_BF16X3, false>
+                <<<grid, NT_CTA, dag_smem_bytes<double, SPLIT_BF16X3, false>(), s>>>(p);
         else if (split == SPLIT_TF32X3)
-            cholesky_dag_kernel<float, SPLIT_TF32X3><<<grid, NT_CTA, tile_smem_bytes<float, SPLIT_TF32X3>(), s>>>(p);
+            cholesky_dag_kernel<float, SPLIT_TF32X3, false>
+                <<<grid, NT_CTA, dag_smem_bytes<float, SPLIT_TF32X3, false>(), s>>>(p);
+        else if (tc)
+            cholesky_dag_kernel<float, SPLIT_BF16X3, true>
+                <<<grid, NT_CTA, dag_smem_bytes<float, SPLIT_BF16X3, true>(), s>>>(p);
         else
-            cholesky_dag_kernel<float, SPLIT_BF16X3><<<grid, NT_CTA, tile_smem_bytes<float, SPLIT_BF16X3>(), s>>>(p);
+            cholesky_dag_kernel<float, SPLIT_BF16X3, false>
+                <<<grid, NT_CTA, dag_smem_bytes<float, SPLIT_BF16X3, false>(), s>>>(p);
     }
     CHB_CUDA(cudaGetLastError());
     CHB_CUDA(cudaEventRecord(g_ws.e1, s));

@@ -69,6 +69,10 @@ struct ExecParams {
     int NIB;
     ExecState *st;
     TraceRec *trace;        // optional per-task trace (nullptr: off)
+    // tcgen05 trailing update of the FP32 factorization (split-BF16 operands):
+    // split chunks of panel tile (m,k), m > k, at split + (m(m-1)/2 + k) * tile_split_bytes
+    uint8_t *split;
+    int split_nrb, split_nkc;   // 128-row blocks and 64-wide k chunks per panel tile
     unsigned long long wait_budget_ns;
 };
 

@@ -27,6 +27,7 @@ struct Context {
     int precision = CHAM_B200_PREC_BF16X3;
     int refine_maxiter = 30;
     long long wait_budget_us = 20000000;
+    bool use_tcgen05 = true;      // tcgen05 trailing updates in the BF16x3 factorization
     int desc_ids = 0;
     std::mutex mu;
 };

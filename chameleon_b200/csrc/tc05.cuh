@@ -1,0 +1,271 @@
+// tc05.cuh -- 5th-generation tensor-core (tcgen05 / TMEM) building blocks for
+// the FP32 trailing update of the split-precision factorization.
+//
+//   C(128 x 128, FP32) -= A(128 x K) * B(128 x K)^T,  A, B = hi + lo in BF16
+//
+// computed as hi*hi + hi*lo + lo*hi on tcgen05.mma kind::f16 (BF16 inputs,
+// FP32 accumulation in tensor memory).  Operands are stored once, by the panel
+// solve that produces them, as "split chunks": for each 128-row block and each
+// 64-wide k chunk, 16 KB of hi followed by 16 KB of lo, every row 128 bytes,
+// already in the K-major 128-byte-swizzled canonical layout of the tensor core
+// (16-byte column group g of row r stored at group g ^ (r & 7)).  A chunk is
+// therefore one contiguous bulk copy (cp.async.bulk, TMA engine) into a
+// 1024-byte aligned shared-memory stage, and the MMA reads it through a shared
+// memory descriptor (SWIZZLE_128B, SBO = 1024 B).
+//
+// Roles inside the 256-thread CTA: thread 0 issues the bulk copies, thread 32
+// issues the MMAs, all 8 warps run the epilogue (TMEM lanes 32*(warp%4)..+31,
+// warps 0-3 columns 0-63, warps 4-7 columns 64-127).  Every mbarrier wait is
+// bounded; on expiry the task records an error and returns.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace chb {
+namespace tc05 {
+
+constexpr int BM = 128, BN = 128, BK = 64;   // output block, k chunk
+constexpr int CHUNK_BYTES = 128 * BK * 2;     // one operand half (hi or lo): 16 KB
+constexpr int STAGES = 3;
+constexpr int STAGE_BYTES = 4 * CHUNK_BYTES;  // A hi, A lo, B hi, B lo
+constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 /*alignment*/ + 256 /*barriers*/;
+constexpr int TMEM_COLS = 128;
+constexpr unsigned long long WAIT_NS = 2000000000ull;   // bound of one mbarrier wait (2 s)
+
+// Byte offset of element (r, c) (r < 128, c < 64) inside one swizzled chunk half.
+__host__ __device__ __forceinline__ int swz_off(int r, int c) {
+    return r * 128 + ((((c >> 3) ^ (r & 7)) & 7) << 4) + ((c & 7) << 1);
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count));
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ unsigned long long now_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;\n" : "=l"(t));
+    return t;
+}
+// Bounded wait for phase `parity` to complete; false when WAIT_NS ran out.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+    const uint32_t a = smem_u32(bar);
+    unsigned long long t0 = 0;
+    for (unsigned i = 0;; ++i) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (done) return true;
+        if ((i & 255) == 0) {
+            const unsigned long long t = now_ns();
+            if (i == 0) t0 = t;
+            else if (t - t0 > WAIT_NS) return false;
+        }
+    }
+}
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async;\n" ::: "memory"); }
+__device__ __forceinline__ void fence_mbar_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+
+// Shared-memory matrix descriptor: K-major, SWIZZLE_128B, SBO = 1024 B
+// (8-row groups), LBO unused (1), version 1.
+__device__ __forceinline__ uint64_t sdesc(const void *smem_tile) {
+    const uint64_t a = (smem_u32(smem_tile) >> 4) & 0x3FFFull;
+    return a | (1ull << 16) | (64ull << 32) | (1ull << 46) | (2ull << 61);
+}
+// Instruction descriptor, kind::f16: D = F32, A = B = BF16, both K-major,
+// N = 128, M = 128.
+constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
+                           ((uint32_t)(BM >> 4) << 24);
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+        "l"(da), "l"(db), "r"(IDESC), "r"(accumulate));
+}
+__device__ __forceinline__ void mma_commit(uint64_t *bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                     smem_u32(bar))
+                 : "memory");
+}
+__device__ __forceinline__ void fence_after_sync() {
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+}
+__device__ __forceinline__ void fence_before_sync() {
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+}
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
+        "[%16];\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// One warp allocates TMEM_COLS columns; the address lands in *slot.
+__device__ __forceinline__ void tmem_alloc(uint32_t *slot) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(slot)),
+                 "r"((uint32_t)TMEM_COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+}
+__device__ __forceinline__ void tmem_free(uint32_t taddr) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(taddr), "r"((uint32_t)TMEM_COLS)
+                 : "memory");
+}
+
+// Per-CTA state kept in shared memory across tasks.  Barriers are initialized
+// once per CTA (init()); the phase of each use follows from the running count
+// of k chunks (`chunks`) and of finished GEMMs (`gemms`), so no barrier is ever
+// re-initialized while an arrival could still be in flight.
+struct Smem {
+    uint64_t full[STAGES];
+    uint64_t empty[STAGES];
+    uint64_t accdone;
+    uint32_t tmem;
+    uint32_t chunks;
+    uint32_t gemms;
+    int err;
+};
+
+// Kernel prologue (all threads): barriers + TMEM allocation by warp 0.
+__device__ inline void init(Smem *sm) {
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; ++s) {
+            mbar_init(&sm->full[s], 1);
+            mbar_init(&sm->empty[s], 1);
+        }
+        mbar_init(&sm->accdone, 1);
+        sm->chunks = 0;
+        sm->gemms = 0;
+        sm->err = 0;
+        fence_mbar_init();
+        fence_proxy_async();
+    }
+    if ((threadIdx.x >> 5) == 0) tmem_alloc(&sm->tmem);
+    fence_before_sync();
+    __syncthreads();
+    fence_after_sync();
+}
+
+// Kernel epilogue (all threads): release TMEM (warp 0).
+__device__ inline void finish(Smem *sm) {
+    fence_before_sync();
+    __syncthreads();
+    fence_after_sync();
+    if ((threadIdx.x >> 5) == 0) tmem_free(sm->tmem);
+}
+
+// Writes the split (hi, lo) of v at (r, c) of one chunk pair.
+__device__ __forceinline__ void split_store(uint8_t *chunk, int r, int c, float v) {
+    const __nv_bfloat16 h = __float2bfloat16_rn(v);
+    const __nv_bfloat16 l = __float2bfloat16_rn(v - __bfloat162float(h));
+    const int off = swz_off(r, c);
+    *reinterpret_cast<__nv_bfloat16 *>(chunk + off) = h;
+    *reinterpret_cast<__nv_bfloat16 *>(chunk + CHUNK_BYTES + off) = l;
+}
+
+// acc = A * B^T over nkc chunks, A chunks at a_chunks[kc], B at b_chunks[kc]
+// (each chunk = hi 16 KB + lo 16 KB, consecutive chunks 32 KB apart), then
+// f(row, col, value) on every accumulator element (row, col < 128) by the
+// owning thread.  Call with all 256 threads.  Returns false on a wait timeout.
+template <class F>
+__device__ bool gemm_bf16x3(Smem *sm, uint8_t *stage_base, const uint8_t *a_chunks, const uint8_t *b_chunks,
+                            int nkc, F &&epilogue) {
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint32_t base = sm->chunks;      // k chunks issued by this CTA before this GEMM
+    const uint32_t gnum = sm->gemms;       // GEMMs finished by this CTA before this one
+    __syncthreads();
+    if (tid == 0) {
+        // producer: bulk copies of the four chunk halves of each k chunk
+        fence_proxy_async();   // generic-proxy writes of the operands (other SMs) -> async-proxy reads
+        for (int kc = 0; kc < nkc; ++kc) {
+            const uint32_t g = base + kc;
+            const int s = g % STAGES;
+            if (g >= STAGES && !mbar_wait(&sm->empty[s], ((g / STAGES) - 1) & 1)) {
+                sm->err = 1;
+                break;
+            }
+            uint8_t *st = stage_base + s * STAGE_BYTES;
+            mbar_expect_tx(&sm->full[s], STAGE_BYTES);
+            bulk_g2s(st, a_chunks + (size_t)kc * 2 * CHUNK_BYTES, 2 * CHUNK_BYTES, &sm->full[s]);
+            bulk_g2s(st + 2 * CHUNK_BYTES, b_chunks + (size_t)kc * 2 * CHUNK_BYTES, 2 * CHUNK_BYTES, &sm->full[s]);
+        }
+    } else if (tid == 32) {
+        // MMA issuer
+        for (int kc = 0; kc < nkc; ++kc) {
+            const uint32_t g = base + kc;
+            const int s = g % STAGES;
+            if (!mbar_wait(&sm->full[s], (g / STAGES) & 1)) {
+                sm->err = 1;
+                break;
+            }
+            fence_after_sync();
+            uint8_t *st = stage_base + s * STAGE_BYTES;
+            const uint64_t ahi = sdesc(st), alo = sdesc(st + CHUNK_BYTES);
+            const uint64_t bhi = sdesc(st + 2 * CHUNK_BYTES), blo = sdesc(st + 3 * CHUNK_BYTES);
+#pragma unroll
+            for (int k16 = 0; k16 < BK / 16; ++k16) {
+                const uint64_t dk = (uint64_t)(k16 * 32) >> 4;   // +32 bytes inside the swizzle atom
+                const uint32_t acc0 = (kc > 0 || k16 > 0) ? 1u : 0u;
+                mma_bf16(sm->tmem, alo + dk, bhi + dk, acc0);
+                mma_bf16(sm->tmem, ahi + dk, blo + dk, 1u);
+                mma_bf16(sm->tmem, ahi + dk, bhi + dk, 1u);
+            }
+            mma_commit(&sm->empty[s]);   // stage free once these MMAs have read it
+        }
+        mma_commit(&sm->accdone);
+    }
+    // epilogue: everyone waits for the accumulator
+    bool ok = mbar_wait(&sm->accdone, gnum & 1);
+    __syncthreads();
+    if (sm->err) ok = false;
+    if (ok) {
+        fence_after_sync();
+        const int q = warp & 3;                 // TMEM lane quarter of this warp
+        const int cbase = (warp >> 2) * 64;     // column half
+        const int row = q * 32 + lane;
+#pragma unroll
+        for (int cc = 0; cc < 64; cc += 16) {
+            float v[16];
+            tmem_ld16(sm->tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(cbase + cc), v);
+#pragma unroll
+            for (int i = 0; i < 16; ++i) epilogue(row, cbase + cc + i, v[i]);
+        }
+    }
+    fence_before_sync();
+    __syncthreads();
+    if (tid == 0) {
+        sm->chunks = base + nkc;
+        sm->gemms = gnum + 1;
+    }
+    __syncthreads();
+    return ok;
+}
+
+}  // namespace tc05
+}  // namespace chb

@@ -62,6 +62,7 @@ typedef enum {
 #define CHAMELEON_B200_REFINE_MAXITER 102 /* iterative-refinement iteration cap           */
 #define CHAMELEON_B200_WAIT_BUDGET_MS 103 /* bound on any device-side dependency wait     */
 #define CHAMELEON_B200_WAIT_BUDGET_US 104 /* the same bound in microseconds              */
+#define CHAMELEON_B200_TCGEN05        105 /* 1: tcgen05 trailing updates in BF16x3 (default) */
 
 /* Factorization precisions for CHAMELEON_B200_PRECISION */
 #define CHAM_B200_PREC_FP64   0
