@@ -147,6 +147,7 @@ EXTRAS = {
     "CHAM_B200_Device_Sync": (_i, []),
     "CHAM_B200_Mixed_Stats": (_i, [_dp]),
     "CHAM_B200_Test_TC05": (_i, [_vp, _vp, _i, _vp]),
+    "CHAM_B200_Mixed_Factor_Only": (_i, [_i, _i, _D, _D, ctypes.POINTER(ctypes.c_float)]),
 }
 
 _lib = None

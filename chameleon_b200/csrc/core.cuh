@@ -230,9 +230,10 @@ using Cfg12864 = GemmCfg<T, 128, 64, 4, 2, SP>;  // panel rows x one inner block
 template <class T, int SP = SPLIT_BF16X3>
 using Cfg64 = GemmCfg<T, 64, 64, 2, 4, SP>;      // inner block x inner block
 
-template <class C>
+template <class C_>
 struct Acc {
-    using T = typename C::T;
+    using C = C_;
+    using T = typename C_::T;
     T v[C::FM][C::FN][C::NACC];
     __device__ __forceinline__ void zero() {
 #pragma unroll
@@ -241,6 +242,59 @@ struct Acc {
             for (int b = 0; b < C::FN; ++b)
 #pragma unroll
                 for (int e = 0; e < C::NACC; ++e) v[a][b][e] = T(0);
+    }
+    // C(r, c) -= acc for r < rows, c < cols (and r >= c when lower_only): per
+    // MMA row tile, all loads are issued before any store, so they overlap
+    // instead of serializing behind possible aliasing.
+    __device__ __forceinline__ void sub_from(const ViewT<T> &C, int rows, int cols, bool lower_only) const {
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        const int wm = warp / C_::WN, wn = warp % C_::WN;
+        const int g = lane >> 2, t = lane & 3;
+#pragma unroll
+        for (int a = 0; a < C_::FM; ++a) {
+            T old[C_::FN][C_::NACC];
+            bool ok[C_::FN][C_::NACC];
+#pragma unroll
+            for (int b = 0; b < C_::FN; ++b)
+#pragma unroll
+                for (int e = 0; e < C_::NACC; ++e) {
+                    const int r = wm * C_::WTM + a * C_::MT + g + ((e >= 2) ? 8 : 0);
+                    const int c = wn * C_::WTN + b * 8 + 2 * t + (e & 1);
+                    ok[b][e] = r < rows && c < cols && (!lower_only || r >= c);
+                    old[b][e] = ok[b][e] ? __ldcg(C.at(r, c)) : T(0);
+                }
+#pragma unroll
+            for (int b = 0; b < C_::FN; ++b)
+#pragma unroll
+                for (int e = 0; e < C_::NACC; ++e) {
+                    const int r = wm * C_::WTM + a * C_::MT + g + ((e >= 2) ? 8 : 0);
+                    const int c = wn * C_::WTN + b * 8 + 2 * t + (e & 1);
+                    if (ok[b][e]) *C.at(r, c) = old[b][e] - v[a][b][e];
+                }
+        }
+    }
+    // C(r, c) = acc for r < rows, c < cols.
+    __device__ __forceinline__ void store_to(const ViewT<T> &C, int rows, int cols) const {
+        for_each([&](int r, int c, T x) {
+            if (r < rows && c < cols) *C.at(r, c) = x;
+        });
+    }
+    // f(a, b, e, row, col, value): for_each with the register coordinates.
+    template <class F>
+    __device__ __forceinline__ void for_each_idx(F &&f) const {
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        const int wm = warp / C::WN, wn = warp % C::WN;
+        const int g = lane >> 2, t = lane & 3;
+#pragma unroll
+        for (int a = 0; a < C::FM; ++a)
+#pragma unroll
+            for (int b = 0; b < C::FN; ++b)
+#pragma unroll
+                for (int e = 0; e < C::NACC; ++e) {
+                    const int r = wm * C::WTM + a * C::MT + g + ((e >= 2) ? 8 : 0);
+                    const int c = wn * C::WTN + b * 8 + 2 * t + (e & 1);
+                    f(a, b, e, r, c, v[a][b][e]);
+                }
     }
     // f(row, col, value) for every accumulator element owned by this thread.
     template <class F>
@@ -397,6 +451,7 @@ __device__ void cta_gemm(Acc<C> &acc, const ViewT<typename C::T> &A, const ViewT
 template <class T>
 __device__ inline int blk_chol(T *sD, int n) {
     const int tid = threadIdx.x;
+    const int ri = tid & 63, cg = tid >> 6;   // 64 rows x 4 column classes
     for (int j = 0; j < n; ++j) {
         const T d = sD[j + j * LDD];
         if (!(d > T(0))) {      // also catches NaN; uniform across the CTA
@@ -405,13 +460,13 @@ __device__ inline int blk_chol(T *sD, int n) {
         }
         const T ljj = sqrt(d);
         const T inv = T(1) / ljj;
-        for (int i = j + 1 + tid; i < n; i += NT_CTA) sD[i + j * LDD] *= inv;
+        if (tid > j && tid < n) sD[tid + j * LDD] *= inv;
         __syncthreads();
         if (tid == 0) sD[j + j * LDD] = ljj;
-        const int w = n - j - 1;
-        for (int idx = tid; idx < w * w; idx += NT_CTA) {
-            const int i = j + 1 + idx % w, c = j + 1 + idx / w;
-            if (c <= i) sD[i + c * LDD] -= sD[i + j * LDD] * sD[c + j * LDD];
+        // trailing update: row i = ri, columns c = j+1+cg, +4, ..., c <= i
+        if (ri > j && ri < n) {
+            const T lij = sD[ri + j * LDD];
+            for (int c = j + 1 + cg; c <= ri; c += 4) sD[ri + c * LDD] -= lij * sD[c + j * LDD];
         }
         __syncthreads();
     }
@@ -422,21 +477,33 @@ __device__ inline int blk_chol(T *sD, int n) {
 // rows < i; 4 threads per column split the dot product (shuffle combine).
 template <class T>
 __device__ inline void blk_inv(const T *sD, T *sInv, int n, bool unit = false) {
+    // sInv has room for IB x LDD elements: the sweep works at stride LDD
+    // (conflict-free column reads), then compacts to stride IB in place.
     const int tid = threadIdx.x;
-    for (int idx = tid; idx < IB * IB; idx += NT_CTA) sInv[idx] = T(0);
+    for (int idx = tid; idx < IB * LDD; idx += NT_CTA) sInv[idx] = T(0);
     __syncthreads();
     const int c = tid >> 2, part = tid & 3;   // 64 columns x 4 parts
     for (int i = 0; i < n; ++i) {
         T s = T(0);
         if (c < i) {
-            for (int k = c + part; k < i; k += 4) s += sD[i + k * LDD] * sInv[k + c * IB];
+            for (int k = c + part; k < i; k += 4) s += sD[i + k * LDD] * sInv[k + c * LDD];
         }
         s += __shfl_down_sync(0xffffffffu, s, 2, 4);
         s += __shfl_down_sync(0xffffffffu, s, 1, 4);
         if (part == 0 && c <= i) {
             const T rhs = (c == i) ? T(1) : T(0);
-            sInv[i + c * IB] = unit ? (rhs - s) : (rhs - s) / sD[i + i * LDD];
+            sInv[i + c * LDD] = unit ? (rhs - s) : (rhs - s) / sD[i + i * LDD];
         }
+        __syncthreads();
+    }
+    // compact columns 1..63 from stride LDD to stride IB (ascending: each
+    // destination range starts before its source range, ranges of one column
+    // do not overlap earlier compacted columns)
+    for (int col = 1; col < IB; ++col) {
+        T v = T(0);
+        if (tid < IB) v = sInv[tid + col * LDD];
+        __syncthreads();
+        if (tid < IB) sInv[tid + col * IB] = v;
         __syncthreads();
     }
 }
@@ -463,19 +530,13 @@ __device__ inline void trsm_rows(const ViewT<T> &X, int rows, const ViewT<T> &L,
         if (jb > 0) {
             acc.zero();
             cta_gemm(acc, X, L.sub(jb, 0), rows, nbk, jb, smem);
-            const ViewT<T> Xj = X.sub(0, jb);
-            acc.for_each([&](int r, int c, T v) {
-                if (r < rows && c < nbk) *Xj.at(r, c) -= v;
-            });
+            acc.sub_from(X.sub(0, jb), rows, nbk, false);
             cta_sync_global();
         }
         acc.zero();
         const ViewT<T> Inv{const_cast<T *>(invd) + (int64_t)(jb / IB) * IB * IB, 1, IB};
         cta_gemm(acc, X.sub(0, jb), Inv, rows, nbk, nbk, smem);
-        const ViewT<T> Xj = X.sub(0, jb);
-        acc.for_each([&](int r, int c, T v) {
-            if (r < rows && c < nbk) *Xj.at(r, c) = v;
-        });
+        acc.store_to(X.sub(0, jb), rows, nbk);
         cta_sync_global();
     }
 }
@@ -506,9 +567,7 @@ __device__ inline void trsm_left(const ViewT<T> &X, int w, const ViewT<T> &L, in
         }
         const ViewT<T> Xj = X.sub(jb, 0);
         if (had) {
-            acc.for_each([&](int r, int c, T v) {
-                if (r < nbk && c < w) *Xj.at(r, c) -= v;
-            });
+            acc.sub_from(Xj, nbk, w, false);
             cta_sync_global();
         }
         acc.zero();
@@ -516,9 +575,7 @@ __device__ inline void trsm_left(const ViewT<T> &X, int w, const ViewT<T> &L, in
         if (trans) Inv = Inv.t();
         // acc(i,c) = sum_k op(Inv)(i,k) Xj(k,c)
         cta_gemm(acc, Inv, Xj.t(), nbk, w, nbk, smem);
-        acc.for_each([&](int r, int c, T v) {
-            if (r < nbk && c < w) *Xj.at(r, c) = v;
-        });
+        acc.store_to(Xj, nbk, w);
         cta_sync_global();
     }
 }
@@ -565,19 +622,13 @@ __device__ inline int tile_potrf(const ViewT<T> &Tv, int n, T *invd, T *smem) {
             if (jb > 0) {
                 pa.zero();
                 cta_gemm(pa, Tv.sub(r0, 0), Tv.sub(jb, 0), mr, nbk, jb, smem);
-                const ViewT<T> P = Tv.sub(r0, jb);
-                pa.for_each([&](int r, int c, T v) {
-                    if (r < mr && c < nbk) *P.at(r, c) -= v;
-                });
+                pa.sub_from(Tv.sub(r0, jb), mr, nbk, false);
                 cta_sync_global();
             }
             pa.zero();
             const ViewT<T> Inv{invd + (int64_t)(jb / IB) * IB * IB, 1, IB};
             cta_gemm(pa, Tv.sub(r0, jb), Inv, mr, nbk, nbk, smem);
-            const ViewT<T> P = Tv.sub(r0, jb);
-            pa.for_each([&](int r, int c, T v) {
-                if (r < mr && c < nbk) *P.at(r, c) = v;
-            });
+            pa.store_to(Tv.sub(r0, jb), mr, nbk);
             cta_sync_global();
         }
     }

@@ -148,8 +148,20 @@ __device__ void run_task(const Task &t, const ExecParams &p, const Dims<T> &d, T
             const size_t rbytes = (size_t)p.split_nkc * 2 * tc05::CHUNK_BYTES;
             const uint8_t *a = split_tile(p, t.m, t.k) + bi * rbytes;
             const uint8_t *b = split_tile(p, t.n, t.k) + bj * rbytes;
-            const bool ok = tc05::gemm_bf16x3(tsm, stage, a, b, p.split_nkc, [&](int r, int c, float v) {
-                if (r < rows && c < cols && (!diag || r >= c)) *C.at(r, c) -= v;
+            // epilogue per 16 consecutive columns of one row: all loads first
+            const bool ok = tc05::gemm_bf16x3(tsm, stage, a, b, p.split_nkc, [&](int r, int c0, const float *v) {
+                if (r >= rows) return;
+                float old[16];
+#pragma unroll
+                for (int i = 0; i < 16; ++i) {
+                    const int c = c0 + i;
+                    old[i] = (c < cols && (!diag || r >= c)) ? __ldcg(C.at(r, c)) : 0.f;
+                }
+#pragma unroll
+                for (int i = 0; i < 16; ++i) {
+                    const int c = c0 + i;
+                    if (c < cols && (!diag || r >= c)) *C.at(r, c) = old[i] - v[i];
+                }
             });
             if (!ok && threadIdx.x == 0) {
                 atomicCAS(&p.st->error, 0, CHAMELEON_ERR_DEVICE_TIMEOUT);
@@ -161,9 +173,7 @@ __device__ void run_task(const Task &t, const ExecParams &p, const Dims<T> &d, T
         acc.zero();
         cta_gemm(acc, d.A(t.m, t.k).sub(bi * SUBB, 0), d.A(t.n, t.k).sub(bj * SUBB, 0), rows, cols,
                  d.tm(t.k), smem);
-        acc.for_each([&](int r, int c, T v) {
-            if (r < rows && c < cols && (!diag || r >= c)) *C.at(r, c) -= v;
-        });
+        acc.sub_from(C, rows, cols, diag);
         break;
     }
     case TK_FWD_TRSM:
@@ -188,10 +198,7 @@ __device__ void run_task(const Task &t, const ExecParams &p, const Dims<T> &d, T
             Acc<Cfg12864<T, SP>> acc;
             acc.zero();
             cta_gemm(acc, L, Bk.sub(0, c0).t(), rows, wc, d.tm(t.k), smem);
-            const VT Bc = Bm.sub(0, c0);
-            acc.for_each([&](int r, int c, T v) {
-                if (r < rows && c < wc) *Bc.at(r, c) -= v;
-            });
+            acc.sub_from(Bm.sub(0, c0), rows, wc, false);
         }
         break;
     }

@@ -139,9 +139,14 @@ __global__ void __launch_bounds__(NT_CTA, 1) sym_residual_kernel(SymTiles a, Til
     if (threadIdx.x < 64) cmax[threadIdx.x] = 0ull;
     __syncthreads();
     const int gi0 = m * a.NB + r0;
-    acc.for_each([&](int r, int c, double v) {
+    // R = B - acc: B and R are different arrays; all B loads go first
+    Acc<Cfg12864<double>> bv;
+    acc.for_each_idx([&](int a2, int b2, int e, int r, int c, double) {
+        bv.v[a2][b2][e] = (r < rows && c < w) ? __ldcg(bb.at<double>(gi0 + r, c0 + c)) : 0.0;
+    });
+    acc.for_each_idx([&](int a2, int b2, int e, int r, int c, double v) {
         if (r < rows && c < w) {
-            const double res = *bb.at<double>(gi0 + r, c0 + c) - v;
+            const double res = bv.v[a2][b2][e] - v;
             *rb.at<double>(gi0 + r, c0 + c) = res;
             atomicMax(&cmax[c], (unsigned long long)__double_as_longlong(fabs(res)));
         }
@@ -542,6 +547,23 @@ int CHAMELEON_dsposv(cham_uplo_t uplo, int N, int NRHS, double *A, int LDA, doub
     CHAMELEON_Desc_Destroy(&Bd);
     CHAMELEON_Desc_Destroy(&Xd);
     return rc;
+}
+
+// Diagnostics: only the first phase of the mixed solve (casts + the FP32
+// factor-and-solve DAG launch), returning that launch's device time.
+int CHAM_B200_Mixed_Factor_Only(cham_uplo_t uplo, int precision, CHAM_desc_t *A, CHAM_desc_t *B, float *ms) {
+    int rc = ensure_init();
+    if (rc) return rc;
+    if (!A || !B || precision == CHAM_B200_PREC_FP64) return CHAMELEON_ERR_ILLEGAL_VALUE;
+    cudaStream_t s = ctx().stream;
+    if ((rc = mixed_reserve(A->n, A->nb, B->n))) return rc;
+    CHB_CUDA(cudaMemsetAsync(g_mws.flag, 0, sizeof(int), s));
+    if ((rc = cast_desc(A, g_mws.A32, s, g_mws.flag)) || (rc = cast_desc(B, g_mws.B32, s, g_mws.flag))) return rc;
+    ExecResult res;
+    const int split = (precision == CHAM_B200_PREC_FP32) ? SPLIT_TF32X3 : SPLIT_BF16X3;
+    rc = run_cholesky_dag(MODE_FACT | MODE_SOLVE, uplo, g_mws.A32, g_mws.B32, s, &res, split);
+    if (ms) *ms = res.ms;
+    return rc ? rc : (res.error ? res.error : res.info);
 }
 
 }  // extern "C"

@@ -191,7 +191,7 @@ __device__ __forceinline__ void split_store(uint8_t *chunk, int r, int c, float 
 
 // acc = A * B^T over nkc chunks, A chunks at a_chunks[kc], B at b_chunks[kc]
 // (each chunk = hi 16 KB + lo 16 KB, consecutive chunks 32 KB apart), then
-// f(row, col, value) on every accumulator element (row, col < 128) by the
+// f(row, col0, v[16]) for accumulator row `row`, columns col0..col0+15, by the
 // owning thread.  Call with all 256 threads.  Returns false on a wait timeout.
 template <class F>
 __device__ bool gemm_bf16x3(Smem *sm, uint8_t *stage_base, const uint8_t *a_chunks, const uint8_t *b_chunks,
@@ -253,8 +253,7 @@ __device__ bool gemm_bf16x3(Smem *sm, uint8_t *stage_base, const uint8_t *a_chun
         for (int cc = 0; cc < 64; cc += 16) {
             float v[16];
             tmem_ld16(sm->tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(cbase + cc), v);
-#pragma unroll
-            for (int i = 0; i < 16; ++i) epilogue(row, cbase + cc + i, v[i]);
+            epilogue(row, cbase + cc, (const float *)v);
         }
     }
     fence_before_sync();
