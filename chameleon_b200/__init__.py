@@ -127,6 +127,7 @@ PROTOS = {
     "CUDA_dsyrk": (_i, [_i, _i, _i, _i, _dp, _vp, _i, _dp, _vp, _i, _vp]),
     "CUDA_dtrsm": (_i, [_i, _i, _i, _i, _i, _i, _dp, _vp, _i, _vp, _i, _vp]),
     "CUDA_dpotrf": (_i, [_i, _i, _vp, _i, _vp, _i, _vp, _vp]),
+    "CUDA_dpotrf_noalloc": (_i, [_i, _i, _vp, _i, _vp, _vp]),
     "CUDA_dplgsy": (_i, [_dp, _i, _i, _vp, _i, _i, _i, _i, _ull, _vp]),
     "CUDA_dplrnt": (_i, [_i, _i, _vp, _i, _i, _i, _i, _ull, _vp]),
     "CUDA_dlag2s": (_i, [_i, _i, _vp, _i, _vp, _i, _vp]),

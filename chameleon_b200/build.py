@@ -14,7 +14,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libchameleon_b200.so")
 
-SOURCES = ["control.cu", "executor.cu", "tile_abi.cu", "mixed.cu", "batch.cu", "tc05.cu"]
+SOURCES = ["control.cu", "executor.cu", "tile_abi.cu", "mixed.cu", "batch.cu", "tc05.cu", "noalloc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -248,6 +248,16 @@ int CUDA_dtrsm(cham_side_t side, cham_uplo_t uplo, cham_trans_t transa, cham_dia
 /* d_info: device int receiving LAPACK's info; WORK/lwork are accepted and unused */
 int CUDA_dpotrf(cham_uplo_t uplo, int n, double *A, int lda, double *WORK, int lwork,
                 int *d_info, cusolverDnHandle_t handle);
+/* No counterpart in the reference.  CUDA_dpotrf without any device
+ * allocation, for callers that cannot allocate: a task runtime that owns the
+ * device memory and forbids allocation inside its worker callbacks (StarPU
+ * codelets, for instance), or latency-critical code that must not wait on
+ * cudaMalloc.  Its scratch is one fixed 512 KiB array in the library's device
+ * memory, so n <= 1024 (larger n returns CHAMELEON_ERR_INTERNAL_LIMIT); all
+ * calls on a device share that array, so calls that could overlap on the GPU
+ * must not be issued.  The first call on a device does a one-time set-up and
+ * should come before any stream capture.  Same result and `info` as CUDA_dpotrf. */
+int CUDA_dpotrf_noalloc(cham_uplo_t uplo, int n, double *A, int lda, int *d_info, void *cuda_stream);
 int CUDA_dplgsy(const double *bump, int m, int n, double *A, int lda, int bigM, int m0, int n0,
                 unsigned long long int seed, cublasHandle_t handle);
 int CUDA_dplrnt(int m, int n, double *A, int lda, int bigM, int m0, int n0,
