@@ -214,6 +214,260 @@ def cpu_baseline_sample():
 
 
 # ---------------------------------------------------------------------------
+# Uneven batch: 8192 systems, n ~ U{16..512}, nrhs ~ U{1..8}
+# ---------------------------------------------------------------------------
+BATCH_COUNT, BATCH_SEED, BATCH_NMIN, BATCH_NMAX = 8192, 2024, 16, 512
+
+
+def batch_workload(count=BATCH_COUNT, seed=BATCH_SEED):
+    rng = np.random.default_rng(seed)
+    n = rng.integers(BATCH_NMIN, BATCH_NMAX + 1, size=count).astype(np.int32)
+    k = rng.integers(1, 9, size=count).astype(np.int32)
+    a_off = np.zeros(count, np.int64)
+    b_off = np.zeros(count, np.int64)
+    a_off[1:] = np.cumsum(n.astype(np.int64) ** 2)[:-1]
+    b_off[1:] = np.cumsum(n.astype(np.int64) * k)[:-1]
+    return n, k, a_off, b_off
+
+
+def batch_section(args, cb, world, rank):
+    """C4: one uneven batch per step through CHAM_B200_dposv_batch vs one
+    CHAMELEON_dposv call per matrix (the plain per-matrix launch path)."""
+    import torch
+    L = cb.lib()
+    n, k, a_off, b_off = batch_workload(args.batch_count)
+    count = len(n)
+    na = int(a_off[-1] + int(n[-1]) ** 2)
+    nb_ = int(b_off[-1] + int(n[-1]) * int(k[-1]))
+    A0 = torch.empty(na, dtype=torch.float64, device="cuda")
+    B0 = torch.empty(nb_, dtype=torch.float64, device="cuda")
+    h = ctypes.c_void_p()
+    assert L.CHAM_B200_Handle_Create(ctypes.byref(h), None) == 0
+    for i in range(count):
+        ni, ki = int(n[i]), int(k[i])
+        bump = ctypes.c_double(float(ni))
+        pa = ctypes.c_void_p(A0.data_ptr() + 8 * int(a_off[i]))
+        pb = ctypes.c_void_p(B0.data_ptr() + 8 * int(b_off[i]))
+        assert L.CUDA_dplgsy(ctypes.byref(bump), ni, ni, pa, ni, ni, 0, 0, BATCH_SEED + i, h) == 0
+        assert L.CUDA_dplrnt(ni, ki, pb, ni, ni, 0, 0, BATCH_SEED + 7 * count + i, h) == 0
+    torch.cuda.synchronize()
+    L.CHAM_B200_Handle_Destroy(h)
+    A, B = A0.clone(), B0.clone()
+    dn = torch.from_numpy(n).cuda()
+    dk = torch.from_numpy(k).cuda()
+    da = torch.from_numpy(a_off).cuda()
+    db = torch.from_numpy(b_off).cuda()
+    info = torch.zeros(count, dtype=torch.int32, device="cuda")
+    flops = sum(dposv_flops(int(a), int(b)) for a, b in zip(n, k))
+    ptr = lambda t: ctypes.c_void_p(t.data_ptr())
+
+    def step():
+        rc = L.CHAM_B200_dposv_batch(cb.ChamLower, count, ptr(dn), ptr(dk), ptr(A), ptr(da), ptr(B), ptr(db),
+                                     ptr(info), None)
+        assert rc == 0, rc
+
+    times = []
+    for it in range(args.warmup + args.steps):
+        A.copy_(A0)
+        B.copy_(B0)
+        torch.cuda.synchronize()
+        L.CHAM_B200_Event_Record(6)
+        step()
+        L.CHAM_B200_Event_Record(7)
+        if it >= args.warmup:
+            times.append(L.CHAM_B200_Event_Elapsed(6, 7))
+    assert int(info.abs().sum()) == 0
+    # accuracy on a sample: FP64 backward error against the generated inputs
+    Ah, Bh, Xh = A0.cpu().numpy(), B0.cpu().numpy(), B.cpu().numpy()
+    worst = 0.0
+    for i in list(range(0, count, max(1, count // 24))):
+        ni, ki = int(n[i]), int(k[i])
+        Ai = Ah[a_off[i]:a_off[i] + ni * ni].reshape(ni, ni).T
+        Ai = np.tril(Ai) + np.tril(Ai, -1).T
+        Bi = Bh[b_off[i]:b_off[i] + ni * ki].reshape(ki, ni).T
+        Xi = Xh[b_off[i]:b_off[i] + ni * ki].reshape(ki, ni).T
+        r = np.abs(Bi - Ai @ Xi).max() / (np.abs(Ai).sum(1).max() * np.abs(Xi).max() * ni * 1.1102230246251565e-16)
+        worst = max(worst, float(r))
+    ms = statistics.median(times)
+    ms_max = allreduce_max(ms, world)
+    # plain path: one CHAMELEON_dposv (FP64 tile DAG) launch per matrix, device arrays
+    plain_ms = None
+    if rank == 0 and args.batch_plain:
+        A.copy_(A0)
+        B.copy_(B0)
+        torch.cuda.synchronize()
+        m = min(count, args.batch_plain)
+        t0 = time.perf_counter()
+        for i in range(m):
+            ni, ki = int(n[i]), int(k[i])
+            rc = L.CHAMELEON_dposv(cb.ChamLower, ni, ki, ctypes.c_void_p(A.data_ptr() + 8 * int(a_off[i])), ni,
+                                   ctypes.c_void_p(B.data_ptr() + 8 * int(b_off[i])), ni)
+            assert rc == 0, rc
+        torch.cuda.synchronize()
+        plain_ms = (time.perf_counter() - t0) * 1e3 * count / m
+    del A0, B0, A, B
+    sps = count * world / (ms_max * 1e-3)
+    return {
+        "workload": "%d SPD systems, n~U{%d..%d}, nrhs~U{1..8} (seed %d), dplgsy(bump=n, seed=%d+i, bigM=n), "
+                    "FP64, Lower, one CHAM_B200_dposv_batch call per step" % (count, BATCH_NMIN, BATCH_NMAX,
+                                                                              BATCH_SEED, BATCH_SEED),
+        "solves_per_s": sps, "ms_per_step": ms_max, "tflops": flops * world / (ms_max * 1e-3) / 1e12,
+        "backward_error_max_sampled": worst,
+        "plain_per_matrix": ({"solves_per_s": count / (plain_ms * 1e-3), "ms": plain_ms,
+                              "sampled_matrices": min(count, args.batch_plain),
+                              "api": "CHAMELEON_dposv per matrix (device arrays)"} if plain_ms else None),
+        "speedup_vs_plain": (plain_ms / ms_max) if plain_ms else None,
+        "roofline": {"bound": "fp64", "achieved": flops / (ms_max * 1e-3) / 1e12, "peak": 40.0,
+                     "unit": "TFLOP/s", "frac": flops / (ms_max * 1e-3) / 1e12 / 40.0,
+                     "peak_source": "FP64 spec 40 TFLOP/s (fallback: no FP64 entry in the measured peaks)"},
+    }
+
+
+# ---------------------------------------------------------------------------
+# Serving: Poisson arrivals, N = floor(exp(U(ln 64, ln 8192))), nrhs ~ U{1..32},
+# 30% of requests reuse a kept factor with new right-hand sides
+# ---------------------------------------------------------------------------
+SERVE_NMIN, SERVE_NMAX, SERVE_SEED = 64, 8192, 77
+
+
+class ServeLoad:
+    """Host inputs of the serving workload: every request's matrix is the
+    leading N x N block of one dplgsy(bump = 8192) matrix in pinned memory."""
+
+    def __init__(self, cb):
+        import torch
+        self.cb = cb
+        N = SERVE_NMAX
+        self.A = torch.empty((N, N), dtype=torch.float64, pin_memory=True)   # column-major view: A[j, i] = a_ij
+        self.B = torch.empty((32, N), dtype=torch.float64, pin_memory=True)
+        dA = cb.Desc.create(N, N, 512)
+        dB = cb.Desc.create(N, 32, 512)
+        assert cb.dplgsy_Tile(float(N), cb.ChamUpperLower, dA, SEED_A) == 0
+        assert cb.dplrnt_Tile(dB, SEED_B) == 0
+        L = cb.lib()
+        assert L.CHAMELEON_Desc2Lap(cb.ChamUpperLower, dA.ptr, ctypes.c_void_p(self.A.data_ptr()), N) == 0
+        assert L.CHAMELEON_Desc2Lap(cb.ChamUpperLower, dB.ptr, ctypes.c_void_p(self.B.data_ptr()), N) == 0
+        dA.destroy()
+        dB.destroy()
+        self.An = self.A.numpy()
+        self.Bn = self.B.numpy()
+
+    def draw(self, rng, count, reuse_frac=0.3):
+        lo, hi = np.log(SERVE_NMIN), np.log(SERVE_NMAX)
+        out = []
+        for _ in range(count):
+            Nr = int(np.floor(np.exp(rng.uniform(lo, hi))))
+            Nr = min(max(Nr, SERVE_NMIN), SERVE_NMAX)
+            out.append((Nr, int(rng.integers(1, 33)), bool(rng.random() < reuse_frac)))
+        return out
+
+
+def serve_run(cb, load, reqs, arrivals, slots, key_pool=32):
+    """Submit `reqs` at `arrivals` (seconds from start; None: all at once).
+    Returns per-request (N, latency s, status, reuse, X) and the elapsed time."""
+    sv = cb.Server(slots=slots)
+    N0 = SERVE_NMAX
+    kept = {}      # key -> (N, Request) of the request that made it
+    next_key = 0
+    done = []
+    t0 = cb.Server.now()
+    pending = []
+    for i, (Nr, kr, reuse) in enumerate(reqs):
+        if arrivals is not None:
+            while cb.Server.now() - t0 < arrivals[i]:
+                time.sleep(min(0.0005, max(0.0, arrivals[i] - (cb.Server.now() - t0))))
+        X = np.empty((kr, Nr))   # column-major N x nrhs
+        ready = [key for key, (nk, r) in kept.items() if r.status == 0]
+        if reuse and ready:
+            key = ready[int(i * 2654435761) % len(ready)]
+            Nk = kept[key][0]
+            X = np.empty((kr, Nk))
+            r = sv.submit(None, load.Bn, X, N=Nk, nrhs=kr, factor_key=key, ldb=N0, ldx=Nk)
+            pending.append((Nk, kr, True, r, X, t0 + (arrivals[i] if arrivals is not None else 0.0)))
+            continue
+        key = -1
+        if Nr > 512 and reuse is False and (i % 3 == 0):
+            key = next_key % key_pool
+            next_key += 1
+        r = sv.submit(load.An, load.Bn, X, N=Nr, nrhs=kr, factor_key=key, lda=N0, ldb=N0, ldx=Nr)
+        if key >= 0:
+            kept[key] = (Nr, r)
+        pending.append((Nr, kr, False, r, X, t0 + (arrivals[i] if arrivals is not None else 0.0)))
+    sv.drain()
+    t1 = cb.Server.now()
+    st = sv.stats()
+    sv.close()
+    for (Nr, kr, reuse, r, X, tarr) in pending:
+        done.append((Nr, kr, reuse, r.t_done - tarr, r.status, X, r.iterations))
+    return done, t1 - t0, st
+
+
+def serve_section(args, cb, rank):
+    if rank != 0:
+        return None
+    load = ServeLoad(cb)
+    rng = np.random.default_rng(SERVE_SEED)
+    slots = args.serve_slots
+    # capacity: closed loop, everything submitted at once
+    cap_reqs = load.draw(rng, args.serve_cap_requests)
+    serve_run(cb, load, cap_reqs[:16], None, slots)   # warm-up (schedules, workspaces)
+    done, el, st = serve_run(cb, load, cap_reqs, None, slots)
+    capacity = len(done) / el
+    bad = [d for d in done if d[4] != 0]
+    assert not bad, bad[:3]
+    # accuracy on a sample of the capacity run
+    worst = 0.0
+    for (Nr, kr, reuse, lat, status, X, it) in done[::max(1, len(done) // 12)]:
+        Ai = load.An[:Nr, :Nr].T
+        Ai = np.tril(Ai) + np.tril(Ai, -1).T
+        Bi = load.Bn[:kr, :Nr].T
+        Xi = X.T
+        r = np.abs(Bi - Ai @ Xi).max() / (np.abs(Ai).sum(1).max() * np.abs(Xi).max() * Nr * 1.1102230246251565e-16)
+        worst = max(worst, float(r))
+    # plain path: one CHAMELEON_dsposv call per request, one after another
+    L = cb.lib()
+    plain_rate = None
+    if args.serve_plain:
+        m = min(len(cap_reqs), args.serve_plain)
+        it = ctypes.c_int()
+        cb.set_param(cb.CHAMELEON_TILE_SIZE, 512)
+        t0 = time.perf_counter()
+        for (Nr, kr, reuse) in cap_reqs[:m]:
+            X = np.empty((kr, Nr))
+            rc = L.CHAMELEON_dsposv(cb.ChamLower, Nr, kr, ctypes.c_void_p(load.A.data_ptr()), SERVE_NMAX,
+                                    ctypes.c_void_p(load.B.data_ptr()), SERVE_NMAX, X.ctypes.data_as(ctypes.c_void_p),
+                                    Nr, ctypes.byref(it))
+            assert rc == 0, rc
+        plain_rate = m / (time.perf_counter() - t0)
+    loads = []
+    for frac in args.serve_loads:
+        rate = frac * capacity
+        n_req = max(20, int(rate * args.serve_window))
+        reqs = load.draw(rng, n_req)
+        gaps = rng.exponential(1.0 / rate, size=n_req)
+        arr = np.cumsum(gaps) - gaps[0]
+        done, el, st = serve_run(cb, load, reqs, arr, slots)
+        warm = int(0.1 * len(done))
+        lat = np.array([d[3] for d in done[warm:]]) * 1e3
+        assert all(d[4] == 0 for d in done)
+        loads.append({"load_frac": frac, "offered_per_s": rate, "requests": len(done),
+                      "solves_per_s": len(done) / el, "p50_ms": float(np.percentile(lat, 50)),
+                      "p99_ms": float(np.percentile(lat, 99)), "batches": st["batches"],
+                      "batched_requests": st["batched_requests"], "max_batch": st["max_batch"],
+                      "reused_factors": st["reused_factors"]})
+    return {
+        "workload": "serving: N=floor(exp(U(ln 64, ln 8192))), nrhs~U{1..32}, 30%% reuse of a kept factor, "
+                    "Poisson arrivals; mixed BF16x3 + FP64 refinement for N>512, batched FP64 for N<=512; host "
+                    "pinned inputs, latency = arrival -> result in host memory; %d slots" % slots,
+        "capacity_solves_per_s": capacity, "capacity_requests": len(cap_reqs),
+        "backward_error_max_sampled": worst,
+        "plain_per_request_solves_per_s": plain_rate,
+        "speedup_vs_plain": (capacity / plain_rate) if plain_rate else None,
+        "window_s": args.serve_window, "loads": loads,
+    }
+
+
+# ---------------------------------------------------------------------------
 # B200 arm
 # ---------------------------------------------------------------------------
 def b200_arm(args, world, rank, local):
@@ -326,6 +580,8 @@ def b200_arm(args, world, rank, local):
                "api": "CHAMELEON_dsposv (LAPACK layout, pinned host A/B/X)"}
         del hA
 
+    batch = batch_section(args, cb, world, rank) if args.batch else None
+    serving = serve_section(args, cb, rank) if args.serve else None
     cpu = cpu_baseline_sample() if (rank == 0 and not args.no_cpu) else None
     line = {
         "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,
@@ -347,6 +603,8 @@ def b200_arm(args, world, rank, local):
         "e2e": e2e,
         "clocks": clk,
         "gpu_launches": launches,
+        "batch": batch,
+        "serving": serving,
     }
     if rank == 0:
         print(json.dumps(line))
@@ -367,6 +625,16 @@ def main():
     ap.add_argument("--no-e2e", dest="e2e", action="store_false")
     ap.add_argument("--no-fp64", dest="compare_fp64", action="store_false")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-batch", dest="batch", action="store_false")
+    ap.add_argument("--batch-count", type=int, default=BATCH_COUNT)
+    ap.add_argument("--batch-plain", type=int, default=BATCH_COUNT,
+                    help="matrices timed through the plain per-matrix path (0: skip)")
+    ap.add_argument("--no-serve", dest="serve", action="store_false")
+    ap.add_argument("--serve-slots", type=int, default=2)
+    ap.add_argument("--serve-window", type=float, default=10.0, help="seconds of arrivals per load level")
+    ap.add_argument("--serve-loads", type=float, nargs="+", default=[0.5, 0.8, 0.95])
+    ap.add_argument("--serve-cap-requests", type=int, default=300)
+    ap.add_argument("--serve-plain", type=int, default=100, help="requests timed through CHAMELEON_dsposv")
     args = ap.parse_args()
     world, rank, local = dist_setup(args.gpus)
     try:

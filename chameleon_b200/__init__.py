@@ -36,6 +36,7 @@ CHAMELEON_SUCCESS = 0
 CHAMELEON_ERR_NOT_INITIALIZED = -101
 CHAMELEON_ERR_ILLEGAL_VALUE = -104
 CHAMELEON_ERR_NOT_SUPPORTED = -103
+CHAMELEON_ERR_NOT_FOUND = -105
 CHAMELEON_ERR_OUT_OF_RESOURCES = -106
 CHAMELEON_ERR_UNEXPECTED = -110
 CHAMELEON_ERR_DEVICE_TIMEOUT = -120
@@ -74,6 +75,26 @@ class Task(ctypes.Structure):
     _fields_ = [("kind", ctypes.c_int16), ("sub", ctypes.c_int16), ("m", ctypes.c_int16),
                 ("n", ctypes.c_int16), ("k", ctypes.c_int16), ("bn", ctypes.c_int16), ("pad", ctypes.c_int32)]
 
+
+class Request(ctypes.Structure):
+    """CHAM_b200_request_t (serving loop)."""
+    _fields_ = [("N", ctypes.c_int), ("nrhs", ctypes.c_int), ("uplo", ctypes.c_int),
+                ("A", ctypes.c_void_p), ("lda", ctypes.c_int),
+                ("B", ctypes.c_void_p), ("ldb", ctypes.c_int),
+                ("X", ctypes.c_void_p), ("ldx", ctypes.c_int),
+                ("factor_key", ctypes.c_longlong),
+                ("status", ctypes.c_int), ("iterations", ctypes.c_int),
+                ("t_submit", ctypes.c_double), ("t_start", ctypes.c_double), ("t_done", ctypes.c_double)]
+
+
+class ServeStats(ctypes.Structure):
+    _fields_ = [("completed", ctypes.c_longlong), ("batches", ctypes.c_longlong),
+                ("batched_requests", ctypes.c_longlong), ("max_batch", ctypes.c_longlong),
+                ("reused_factors", ctypes.c_longlong), ("kept_factors", ctypes.c_longlong),
+                ("bytes_in_use", ctypes.c_double), ("budget_bytes", ctypes.c_double)]
+
+
+REQ_PENDING = 1 << 30
 
 _D = ctypes.POINTER(CHAM_desc_t)
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -133,14 +154,20 @@ PROTOS = {
     "CUDA_dlag2s": (_i, [_i, _i, _vp, _i, _vp, _i, _vp]),
     "CUDA_slag2d": (_i, [_i, _i, _vp, _i, _vp, _i, _vp]),
     "CHAM_B200_dposv_batch": (_i, [_i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "CHAM_B200_Serve_Create": (_i, [ctypes.POINTER(_vp), _i, ctypes.c_double, _i]),
+    "CHAM_B200_Serve_Submit": (_i, [_vp, ctypes.POINTER(Request)]),
+    "CHAM_B200_Serve_Drain": (_i, [_vp]),
+    "CHAM_B200_Serve_Stats": (_i, [_vp, ctypes.POINTER(ServeStats)]),
+    "CHAM_B200_Serve_Destroy": (_i, [_vp]),
+    "CHAM_B200_Serve_Now": (ctypes.c_double, []),
 }
 # library extras (not in the public header): tracing, schedule inspection, timing
 EXTRAS = {
     "CHAM_B200_Handle_Overflow": (_i, [_vp]),
     "CHAM_B200_Trace_Enable": (_i, [_i]),
     "CHAM_B200_Trace_Read": (_i, [_vp, _i]),
-    "CHAM_B200_Schedule_Size": (_i, [_i, _i, _i, _i, _i, _i]),
-    "CHAM_B200_Schedule_Build": (_i, [_i, _i, _i, _i, _i, _i, ctypes.POINTER(Task), _i]),
+    "CHAM_B200_Schedule_Size": (_i, [_i, _i, _i, _i, _i, _i, _i]),
+    "CHAM_B200_Schedule_Build": (_i, [_i, _i, _i, _i, _i, _i, _i, ctypes.POINTER(Task), _i]),
     "CHAM_B200_dposv_timed": (_i, [_i, _i, _i, _vp, _i, _vp, _i, ctypes.POINTER(ctypes.c_float)]),
     "CHAM_B200_Event_Record": (_i, [_i]),
     "CHAM_B200_Event_Elapsed": (ctypes.c_float, [_i, _i]),
@@ -340,14 +367,76 @@ def dsposv(uplo, N, NRHS, A, LDA, B, LDB, X, LDX):
     return rc, it.value
 
 
-def schedule(mode, N, NB, nrhs=0, NBB=None, workers=148):
-    """The executor's task list for a shape (host-only; no GPU needed)."""
+PROF_FP64, PROF_F32_MMA, PROF_F32_TC05 = 0, 1, 2
+
+
+def schedule(mode, N, NB, nrhs=0, NBB=None, workers=148, prof=PROF_FP64):
+    """The executor's task list for a shape and cost profile (host-only; no GPU needed)."""
     L = lib()
     NBB = NB if NBB is None else NBB
-    n = L.CHAM_B200_Schedule_Size(mode, N, NB, nrhs, NBB, workers)
+    n = L.CHAM_B200_Schedule_Size(mode, N, NB, nrhs, NBB, workers, prof)
     buf = (Task * max(n, 1))()
-    got = L.CHAM_B200_Schedule_Build(mode, N, NB, nrhs, NBB, workers, buf, n)
+    got = L.CHAM_B200_Schedule_Build(mode, N, NB, nrhs, NBB, workers, prof, buf, n)
     if got != n:
         raise ChameleonError("schedule build returned %d of %d" % (got, n))
     arr = np.frombuffer(buf, dtype=np.int16).reshape(-1, 8)[:n]
     return arr[:, :6].copy()   # kind, sub, m, n, k, bn
+
+
+class Server:
+    """Serving loop (CHAM_B200_Serve_*): submit solve requests, read results.
+
+    Arrays are host arrays (numpy or pinned torch CPU tensors), column-major:
+    A is N x N (lower triangle read for ChamLower), B and X are N x nrhs.  The
+    caller keeps them alive until the request completes (`drain()`).
+    """
+
+    def __init__(self, slots=2, hbm_budget_bytes=0.0, small_n=512):
+        init()
+        h = ctypes.c_void_p()
+        check(lib().CHAM_B200_Serve_Create(ctypes.byref(h), slots, float(hbm_budget_bytes), small_n),
+              "CHAM_B200_Serve_Create")
+        self.h = h
+        self._keep = {}
+
+    @staticmethod
+    def now():
+        return lib().CHAM_B200_Serve_Now()
+
+    def submit(self, A, B, X, nrhs=None, N=None, uplo=ChamLower, factor_key=-1, lda=None, ldb=None, ldx=None):
+        """Queue one solve; returns the Request (status == REQ_PENDING until done)."""
+        r = Request()
+        r.N = N if N is not None else B.shape[0]
+        r.nrhs = nrhs if nrhs is not None else (B.shape[1] if B.ndim > 1 else 1)
+        r.uplo = uplo
+        r.A = _addr(A).value if A is not None else None
+        r.lda = lda if lda is not None else r.N
+        r.B = _addr(B).value
+        r.ldb = ldb if ldb is not None else r.N
+        r.X = _addr(X).value
+        r.ldx = ldx if ldx is not None else r.N
+        r.factor_key = factor_key
+        check(lib().CHAM_B200_Serve_Submit(self.h, ctypes.byref(r)), "CHAM_B200_Serve_Submit")
+        self._keep[id(r)] = (r, A, B, X)
+        return r
+
+    def drain(self):
+        check(lib().CHAM_B200_Serve_Drain(self.h), "CHAM_B200_Serve_Drain")
+        self._keep.clear()
+
+    def stats(self):
+        st = ServeStats()
+        check(lib().CHAM_B200_Serve_Stats(self.h, ctypes.byref(st)), "CHAM_B200_Serve_Stats")
+        return {k: getattr(st, k) for k, _ in ServeStats._fields_}
+
+    def close(self):
+        if self.h:
+            lib().CHAM_B200_Serve_Destroy(self.h)
+            self.h = None
+            self._keep.clear()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()

@@ -8,13 +8,14 @@ import os
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libchameleon_b200.so")
 
-SOURCES = ["control.cu", "executor.cu", "tile_abi.cu", "mixed.cu", "batch.cu", "tc05.cu", "noalloc.cu"]
+SOURCES = ["control.cu", "executor.cu", "tile_abi.cu", "mixed.cu", "batch.cu", "tc05.cu", "noalloc.cu", "serve.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -40,12 +41,16 @@ def build(verbose=False, extra=()):
     nvcc = nvcc_path()
     common = [nvcc, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
               "-I", os.path.join(ROOT, "include"), "--expt-relaxed-constexpr", *extra]
-    for s in srcs:
+    def compile_one(s):
         o = os.path.join(objdir, os.path.basename(s) + ".o")
         cmd = common + ["-c", s, "-o", o]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")
-        r = subprocess.run(cmd, capture_output=True, text=True)
+        return s, o, subprocess.run(cmd, capture_output=True, text=True)
+
+    with ThreadPoolExecutor(max_workers=min(len(srcs), os.cpu_count() or 1)) as ex:
+        results = list(ex.map(compile_one, srcs))
+    for s, o, r in results:
         if r.returncode != 0:
             sys.stderr.write(r.stdout + r.stderr)
             raise RuntimeError("nvcc failed on %s" % s)

@@ -23,12 +23,6 @@
 
 namespace chb {
 
-struct BatchItem {
-    int64_t a_off, b_off;
-    int n, nrhs, lda, ldb;   // nrhs == 0: factor only
-    int info_idx;
-    int pad;
-};
 
 __global__ void __launch_bounds__(NT_CTA, 1) dposv_batch_kernel(const BatchItem *items, int count, double *A,
                                                                 double *B, int upper, int *info, int *cursor,
@@ -108,41 +102,32 @@ __global__ void __launch_bounds__(NT_CTA, 1) trsm_batch_kernel(const TrsmItem *i
     }
 }
 
-namespace {
-struct BatchWs {
-    void *items = nullptr;
-    size_t items_bytes = 0;
-    double *scratch = nullptr;
-    size_t scratch_bytes = 0;
-    int *cursor = nullptr;
-    int *info = nullptr;
-    size_t info_n = 0;
-};
 BatchWs g_bws;
 
-int bws_reserve(size_t item_bytes, size_t scratch_bytes, size_t ninfo) {
-    if (!g_bws.cursor) CHB_CUDA(cudaMalloc(&g_bws.cursor, sizeof(int)));
-    if (item_bytes > g_bws.items_bytes) {
-        if (g_bws.items) cudaFree(g_bws.items);
-        g_bws.items = nullptr;
-        CHB_CUDA(cudaMalloc(&g_bws.items, item_bytes));
-        g_bws.items_bytes = item_bytes;
+int bws_reserve(BatchWs &ws, size_t item_bytes, size_t scratch_bytes, size_t ninfo) {
+    if (!ws.cursor) CHB_CUDA(cudaMalloc(&ws.cursor, sizeof(int)));
+    if (item_bytes > ws.items_bytes) {
+        if (ws.items) cudaFree(ws.items);
+        ws.items = nullptr;
+        CHB_CUDA(cudaMalloc(&ws.items, item_bytes));
+        ws.items_bytes = item_bytes;
     }
-    if (scratch_bytes > g_bws.scratch_bytes) {
-        if (g_bws.scratch) cudaFree(g_bws.scratch);
-        g_bws.scratch = nullptr;
-        CHB_CUDA(cudaMalloc(&g_bws.scratch, scratch_bytes));
-        g_bws.scratch_bytes = scratch_bytes;
+    if (scratch_bytes > ws.scratch_bytes) {
+        if (ws.scratch) cudaFree(ws.scratch);
+        ws.scratch = nullptr;
+        CHB_CUDA(cudaMalloc(&ws.scratch, scratch_bytes));
+        ws.scratch_bytes = scratch_bytes;
     }
-    if (ninfo > g_bws.info_n) {
-        if (g_bws.info) cudaFree(g_bws.info);
-        g_bws.info = nullptr;
-        CHB_CUDA(cudaMalloc(&g_bws.info, ninfo * sizeof(int)));
-        g_bws.info_n = ninfo;
+    if (ninfo > ws.info_n) {
+        if (ws.info) cudaFree(ws.info);
+        ws.info = nullptr;
+        CHB_CUDA(cudaMalloc(&ws.info, ninfo * sizeof(int)));
+        ws.info_n = ninfo;
     }
     return 0;
 }
 
+namespace {
 bool g_attr = false;
 int set_attrs() {
     if (g_attr) return 0;
@@ -157,7 +142,8 @@ int set_attrs() {
 
 // Launch the factor(+solve) batch over host-described items (sorted here,
 // largest first).  `info` is a device array indexed by item.info_idx (or null).
-int launch_posv_batch(std::vector<BatchItem> &items, double *A, double *B, int upper, int *info, cudaStream_t s) {
+int launch_posv_batch(std::vector<BatchItem> &items, double *A, double *B, int upper, int *info, cudaStream_t s,
+                      BatchWs &ws) {
     if (items.empty()) return 0;
     if (int rc = set_attrs()) return rc;
     std::stable_sort(items.begin(), items.end(),
@@ -165,13 +151,13 @@ int launch_posv_batch(std::vector<BatchItem> &items, double *A, double *B, int u
     const int nmax = items.front().n;
     const int nib = std::max(1, (nmax + IB - 1) / IB);
     const int grid = std::min<int>(ctx().num_sms, (int)items.size());
-    if (int rc = bws_reserve(items.size() * sizeof(BatchItem), (size_t)grid * nib * IB * IB * sizeof(double), 1))
+    if (int rc = bws_reserve(ws, items.size() * sizeof(BatchItem), (size_t)grid * nib * IB * IB * sizeof(double), 1))
         return rc;
-    CHB_CUDA(cudaMemcpyAsync(g_bws.items, items.data(), items.size() * sizeof(BatchItem), cudaMemcpyHostToDevice, s));
-    CHB_CUDA(cudaMemsetAsync(g_bws.cursor, 0, sizeof(int), s));
+    CHB_CUDA(cudaMemcpyAsync(ws.items, items.data(), items.size() * sizeof(BatchItem), cudaMemcpyHostToDevice, s));
+    CHB_CUDA(cudaMemsetAsync(ws.cursor, 0, sizeof(int), s));
     CHB_LAUNCHED(1);
-    dposv_batch_kernel<<<grid, NT_CTA, TILE_KERNEL_SMEM_BYTES, s>>>((const BatchItem *)g_bws.items, (int)items.size(),
-                                                                    A, B, upper, info, g_bws.cursor, g_bws.scratch,
+    dposv_batch_kernel<<<grid, NT_CTA, TILE_KERNEL_SMEM_BYTES, s>>>((const BatchItem *)ws.items, (int)items.size(),
+                                                                    A, B, upper, info, ws.cursor, ws.scratch,
                                                                     nib);
     CHB_CUDA(cudaGetLastError());
     return 0;
@@ -203,9 +189,9 @@ int CHAMELEON_dpotrf_batch_Tile(cham_uplo_t uplo, CHAM_desc_t *A) {
             items.push_back(it);
         }
     cudaStream_t s = ctx().stream;
-    if ((rc = bws_reserve(0, 0, items.size()))) return rc;
+    if ((rc = bws_reserve(g_bws, 0, 0, items.size()))) return rc;
     int *dinfo = g_bws.info;
-    if ((rc = launch_posv_batch(items, (double *)A->mat, nullptr, uplo == ChamUpper, dinfo, s))) return rc;
+    if ((rc = launch_posv_batch(items, (double *)A->mat, nullptr, uplo == ChamUpper, dinfo, s, g_bws))) return rc;
     std::vector<int> hinfo(items.size());
     CHB_CUDA(cudaMemcpyAsync(hinfo.data(), dinfo, hinfo.size() * sizeof(int), cudaMemcpyDeviceToHost, s));
     CHB_CUDA(cudaStreamSynchronize(s));
@@ -248,7 +234,7 @@ int CHAMELEON_dtrsm_batch_Tile(cham_side_t side, cham_uplo_t uplo, cham_trans_t 
     const int nib = (nmax + IB - 1) / IB;
     const int grid = std::min<int>(ctx().num_sms, (int)items.size());
     cudaStream_t s = ctx().stream;
-    if ((rc = bws_reserve(items.size() * sizeof(TrsmItem), (size_t)grid * nib * IB * IB * sizeof(double), 1)))
+    if ((rc = bws_reserve(g_bws, items.size() * sizeof(TrsmItem), (size_t)grid * nib * IB * IB * sizeof(double), 1)))
         return rc;
     CHB_CUDA(cudaMemcpyAsync(g_bws.items, items.data(), items.size() * sizeof(TrsmItem), cudaMemcpyHostToDevice, s));
     CHB_CUDA(cudaMemsetAsync(g_bws.cursor, 0, sizeof(int), s));
@@ -287,7 +273,7 @@ int CHAM_B200_dposv_batch(cham_uplo_t uplo, int count, const int *n, const int *
     items.erase(std::remove_if(items.begin(), items.end(), [](const BatchItem &b) { return b.n == 0; }),
                 items.end());
     if (info) CHB_CUDA(cudaMemsetAsync(info, 0, count * sizeof(int), s));
-    if ((rc = launch_posv_batch(items, A, B, uplo == ChamUpper, info, s))) return rc;
+    if ((rc = launch_posv_batch(items, A, B, uplo == ChamUpper, info, s, g_bws))) return rc;
     CHB_CUDA(cudaStreamSynchronize(s));
     return 0;
 }

@@ -20,7 +20,7 @@ Context &ctx() {
     return c;
 }
 
-unsigned long long g_launch_count = 0;
+std::atomic<unsigned long long> g_launch_count{0};
 MixedStats g_mixed_stats;
 
 void report_cuda_error(const char *what, cudaError_t e, const char *file, int line) {
@@ -108,6 +108,13 @@ static void layout_init(CHAM_desc_t *d, cham_flttype_t dtyp, int mb, int nb, int
     d->get_blkldd = host_getldd;
 }
 
+cudaStream_t meta_stream() {
+    static std::once_flag once;
+    static cudaStream_t ms = nullptr;
+    std::call_once(once, [] { cudaStreamCreateWithFlags(&ms, cudaStreamNonBlocking); });
+    return ms;
+}
+
 int desc_upload(CHAM_desc_t *d) {
     DescPriv *pv = priv(d);
     if (pv->dev.off) return 0;
@@ -117,10 +124,15 @@ int desc_upload(CHAM_desc_t *d) {
     for (int n = 0; n < d->nt; ++n)
         for (int m = 0; m < d->mt; ++m) off[m + (size_t)d->mt * n] = desc_tile_off(d, m, n);
     for (int m = 0; m < d->mt; ++m) ld[m] = desc_tile_ld(d, m);
-    CHB_CUDA(cudaMalloc(&pv->dev.off, nt * sizeof(int64_t)));
-    CHB_CUDA(cudaMalloc(&pv->dev.ld, d->mt * sizeof(int)));
-    CHB_CUDA(cudaMemcpy(pv->dev.off, off.data(), nt * sizeof(int64_t), cudaMemcpyHostToDevice));
-    CHB_CUDA(cudaMemcpy(pv->dev.ld, ld.data(), d->mt * sizeof(int), cudaMemcpyHostToDevice));
+    // Stream-ordered allocation on a private stream: creating and destroying
+    // descriptors does not synchronize the device (cudaFree would), so
+    // concurrent solvers on other streams keep running.
+    cudaStream_t ms = meta_stream();
+    CHB_CUDA(cudaMallocAsync(&pv->dev.off, nt * sizeof(int64_t), ms));
+    CHB_CUDA(cudaMallocAsync(&pv->dev.ld, d->mt * sizeof(int), ms));
+    CHB_CUDA(cudaMemcpyAsync(pv->dev.off, off.data(), nt * sizeof(int64_t), cudaMemcpyHostToDevice, ms));
+    CHB_CUDA(cudaMemcpyAsync(pv->dev.ld, ld.data(), d->mt * sizeof(int), cudaMemcpyHostToDevice, ms));
+    CHB_CUDA(cudaStreamSynchronize(ms));
     return 0;
 }
 
@@ -446,8 +458,9 @@ int CHAMELEON_Desc_Destroy(CHAM_desc_t **descptr) {
     if (d->alloc_mat && d->mat) cudaFree(d->mat);
     DescPriv *pv = priv(d);
     if (pv) {
-        if (pv->dev.off) cudaFree(pv->dev.off);
-        if (pv->dev.ld) cudaFree(pv->dev.ld);
+        // the caller has synchronized the work that used the tables
+        if (pv->dev.off) cudaFreeAsync(pv->dev.off, meta_stream());
+        if (pv->dev.ld) cudaFreeAsync(pv->dev.ld, meta_stream());
         delete pv;
     }
     free(d->tiles);
@@ -737,6 +750,24 @@ double *staging(int slot, size_t bytes) {
     return g_stage[slot];
 }
 bool is_device_ptr_pub(const void *p) { return is_device_ptr(p); }
+
+double *stage_in(int slot, const double *host, int ld, int rows, int cols, cudaStream_t s) {
+    double *d = staging(slot, std::max<size_t>((size_t)rows * cols * sizeof(double), 16));
+    if (!d) return nullptr;
+    if (rows > 0 && cols > 0 &&
+        cudaMemcpy2DAsync(d, (size_t)rows * 8, host, (size_t)ld * 8, (size_t)rows * 8, cols, cudaMemcpyHostToDevice,
+                          s) != cudaSuccess)
+        return nullptr;
+    return d;
+}
+
+int stage_out(double *host, int ld, const double *dev, int rows, int cols, cudaStream_t s) {
+    if (rows <= 0 || cols <= 0) return 0;
+    CHB_CUDA(cudaMemcpy2DAsync(host, (size_t)ld * 8, dev, (size_t)rows * 8, (size_t)rows * 8, cols,
+                               cudaMemcpyDeviceToHost, s));
+    return 0;
+}
+
 }  // namespace chb
 
 extern "C" {
@@ -748,24 +779,24 @@ static int lapack_call(int mode, cham_uplo_t uplo, int N, int NRHS, double *A, i
     const bool a_dev = is_device_ptr(A);
     const bool b_dev = (NRHS > 0 && B) ? is_device_ptr(B) : true;
     double *dA = A, *dB = B;
-    const size_t abytes = (size_t)LDA * N * sizeof(double);
-    const size_t bbytes = (NRHS > 0) ? (size_t)LDB * NRHS * sizeof(double) : 0;
+    // host arrays are staged densely (ld = N): only the N x cols block moves
+    int lda = LDA, ldb = LDB;
     if (!a_dev) {
-        if (!(dA = staging(0, std::max<size_t>(abytes, 16)))) return CHAMELEON_ERR_OUT_OF_RESOURCES;
-        CHB_CUDA(cudaMemcpyAsync(dA, A, abytes, cudaMemcpyHostToDevice, s));
+        if (!(dA = stage_in(0, A, LDA, N, N, s))) return CHAMELEON_ERR_OUT_OF_RESOURCES;
+        lda = N;
     }
     if (!b_dev) {
-        if (!(dB = staging(1, std::max<size_t>(bbytes, 16)))) return CHAMELEON_ERR_OUT_OF_RESOURCES;
-        CHB_CUDA(cudaMemcpyAsync(dB, B, bbytes, cudaMemcpyHostToDevice, s));
+        if (!(dB = stage_in(1, B, LDB, N, NRHS, s))) return CHAMELEON_ERR_OUT_OF_RESOURCES;
+        ldb = N;
     }
     CHAM_desc_t *dAd = nullptr, *dBd = nullptr;
-    desc_create_cm(&dAd, dA, LDA, N, N, c.tile_size);
-    if (NRHS > 0 && (mode & MODE_SOLVE)) desc_create_cm(&dBd, dB, LDB, N, NRHS, c.tile_size);
+    desc_create_cm(&dAd, dA, lda, N, N, c.tile_size);
+    if (NRHS > 0 && (mode & MODE_SOLVE)) desc_create_cm(&dBd, dB, ldb, N, NRHS, c.tile_size);
     ExecResult res;
     int rc = run_cholesky_dag(mode, uplo, dAd, dBd, s, &res);
     if (ms_out) *ms_out = res.ms;
-    if (!a_dev && (mode & MODE_FACT)) cudaMemcpyAsync(A, dA, abytes, cudaMemcpyDeviceToHost, s);
-    if (!b_dev && (mode & MODE_SOLVE)) cudaMemcpyAsync(B, dB, bbytes, cudaMemcpyDeviceToHost, s);
+    if (!a_dev && (mode & MODE_FACT)) stage_out(A, LDA, dA, N, N, s);
+    if (!b_dev && (mode & MODE_SOLVE)) stage_out(B, LDB, dB, N, NRHS, s);
     cudaStreamSynchronize(s);
     CHAMELEON_Desc_Destroy(&dAd);
     if (dBd) CHAMELEON_Desc_Destroy(&dBd);
@@ -832,7 +863,7 @@ float CHAM_B200_Event_Elapsed(int a, int b) {
     cudaEventElapsedTime(&ms, g_ev[a], g_ev[b]);
     return ms;
 }
-unsigned long long CHAM_B200_Launch_Count(void) { return g_launch_count; }
+unsigned long long CHAM_B200_Launch_Count(void) { return g_launch_count.load(); }
 int CHAM_B200_Device_Sync(void) {
     return cudaStreamSynchronize(ctx().stream) == cudaSuccess ? 0 : CHAMELEON_ERR_UNEXPECTED;
 }

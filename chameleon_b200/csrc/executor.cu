@@ -268,16 +268,32 @@ __global__ void __launch_bounds__(NT_CTA, 1) cholesky_dag_kernel(ExecParams p) {
 // ---------------------------------------------------------------------------
 namespace {
 
+// Cost profile of the task kinds, per execution path: list-scheduling order
+// depends on the relative durations, which differ a lot between the FP64 DMMA
+// path and the tcgen05 path (where updates are ~6x cheaper relative to the
+// panel tasks).  Multipliers of the flop model, calibrated from per-task
+// device traces at NB = 512 (POTRF, TRSM, UPD, FWD/BWD TRSM, FWD/BWD UPD).
+enum CostProfile : int { PROF_FP64 = 0, PROF_F32_MMA = 1, PROF_F32_TC05 = 2 };
+struct Calib {
+    double potrf, trsm, upd, strsm, supd;
+};
+static const Calib kCalib[3] = {
+    {4.9, 4.7, 5.8, 3.9, 7.1},   // FP64 DMMA
+    {4.0, 4.7, 2.1, 2.4, 3.3},   // FP32, split products on mma.sync
+    {4.0, 4.7, 0.92, 2.4, 3.3},  // FP32, tcgen05 updates
+};
+
 struct Shape {
-    int mode, N, NB, nrhs, NBB, P;
+    int mode, N, NB, nrhs, NBB, P, prof;
     bool operator==(const Shape &o) const {
-        return mode == o.mode && N == o.N && NB == o.NB && nrhs == o.nrhs && NBB == o.NBB && P == o.P;
+        return mode == o.mode && N == o.N && NB == o.NB && nrhs == o.nrhs && NBB == o.NBB && P == o.P &&
+               prof == o.prof;
     }
 };
 struct ShapeHash {
     size_t operator()(const Shape &s) const {
         size_t h = 1469598103934665603ull;
-        for (int v : {s.mode, s.N, s.NB, s.nrhs, s.NBB, s.P}) h = (h ^ (size_t)v) * 1099511628211ull;
+        for (int v : {s.mode, s.N, s.NB, s.nrhs, s.NBB, s.P, s.prof}) h = (h ^ (size_t)v) * 1099511628211ull;
         return h;
     }
 };
@@ -320,13 +336,14 @@ std::vector<Task> build_order(const Shape &s) {
     // ids: potrf[k], trsm[m,k], upd[m,n,k] (last update of tile (m,n) so far)
     std::vector<int> P(NT, -1), Tr((size_t)NT * NT, -1), lastU((size_t)NT * NT, -1);
     const double nb = s.NB;
+    const Calib &cal = kCalib[(s.prof >= 0 && s.prof < 3) ? s.prof : 0];
     if (fact) {
         for (int k = 0; k < NT; ++k) {
             const double tk = tm(k);
-            P[k] = add(TK_POTRF, k, k, k, 0, 1, 6.0 * tk * tk * tk / 3.0);
+            P[k] = add(TK_POTRF, k, k, k, 0, 1, cal.potrf * 6.0 * tk * tk * tk / 3.0);
             edge(lastU[k + (size_t)NT * k], P[k]);
             for (int m = k + 1; m < NT; ++m) {
-                const int id = add(TK_TRSM, m, k, k, 0, nbi(m), 2.0 * SUBB * nb * nb);
+                const int id = add(TK_TRSM, m, k, k, 0, nbi(m), cal.trsm * 2.0 * SUBB * nb * nb);
                 edge(P[k], id);
                 edge(lastU[m + (size_t)NT * k], id);
                 Tr[m + (size_t)NT * k] = id;
@@ -334,7 +351,7 @@ std::vector<Task> build_order(const Shape &s) {
             for (int n = k + 1; n < NT; ++n) {
                 for (int m = n; m < NT; ++m) {
                     const int sub = (m == n) ? nbi(m) * (nbi(m) + 1) / 2 : nbi(m) * nbi(n);
-                    const int id = add(TK_UPD, m, n, k, 0, sub, 1.0 * SUBB * SUBB * nb * 2.0);
+                    const int id = add(TK_UPD, m, n, k, 0, sub, cal.upd * 1.0 * SUBB * SUBB * nb * 2.0);
                     edge(Tr[m + (size_t)NT * k], id);
                     if (m != n) edge(Tr[n + (size_t)NT * k], id);
                     edge(lastU[m + (size_t)NT * n], id);
@@ -351,12 +368,12 @@ std::vector<Task> build_order(const Shape &s) {
         for (int bn = 0; bn < NTB; ++bn) {
             const double w = wB(bn);
             for (int k = 0; k < NT; ++k) {
-                const int f = add(TK_FWD_TRSM, k, k, k, bn, 1, 3.0 * tm(k) * tm(k) * w);
+                const int f = add(TK_FWD_TRSM, k, k, k, bn, 1, cal.strsm * 3.0 * tm(k) * tm(k) * w);
                 edge(P[k], f);
                 edge(lastFU[k + (size_t)NT * bn], f);
                 F[k + (size_t)NT * bn] = f;
                 for (int m = k + 1; m < NT; ++m) {
-                    const int u = add(TK_FWD_UPD, m, k, k, bn, nbi(m), 2.0 * SUBB * tm(k) * w);
+                    const int u = add(TK_FWD_UPD, m, k, k, bn, nbi(m), cal.supd * 2.0 * SUBB * tm(k) * w);
                     edge(f, u);
                     if (fact) edge(Tr[m + (size_t)NT * k], u);
                     edge(lastFU[m + (size_t)NT * bn], u);
@@ -364,12 +381,12 @@ std::vector<Task> build_order(const Shape &s) {
                 }
             }
             for (int k = NT - 1; k >= 0; --k) {
-                const int b = add(TK_BWD_TRSM, k, k, k, bn, 1, 3.0 * tm(k) * tm(k) * w);
+                const int b = add(TK_BWD_TRSM, k, k, k, bn, 1, cal.strsm * 3.0 * tm(k) * tm(k) * w);
                 edge(F[k + (size_t)NT * bn], b);
                 edge(lastBU[k + (size_t)NT * bn], b);
                 Bk[k + (size_t)NT * bn] = b;
                 for (int m = k - 1; m >= 0; --m) {
-                    const int u = add(TK_BWD_UPD, m, k, k, bn, nbi(m), 2.0 * SUBB * tm(k) * w);
+                    const int u = add(TK_BWD_UPD, m, k, k, bn, nbi(m), cal.supd * 2.0 * SUBB * tm(k) * w);
                     edge(b, u);
                     edge(lastBU[m + (size_t)NT * bn], u);
                     lastBU[m + (size_t)NT * bn] = u;
@@ -468,35 +485,25 @@ Schedule *get_schedule(const Shape &s) {
     return raw;
 }
 
-// Per-shape device workspace (counters, inverted blocks, state).
-struct Workspace {
-    uint8_t *split = nullptr;
-    size_t split_bytes = 0;
-    size_t ctr_bytes = 0, inv_bytes = 0;
-    void *ctr = nullptr;
-    double *inv = nullptr;
-    ExecState *st = nullptr;
-    cudaEvent_t e0 = nullptr, e1 = nullptr;
-};
-Workspace g_ws;
+ExecWs g_ws;   // workspace of the synchronous API entry points
 
-int ensure_ws(size_t ctr_bytes, size_t inv_bytes) {
-    if (!g_ws.st) {
-        CHB_CUDA(cudaMalloc(&g_ws.st, sizeof(ExecState)));
-        CHB_CUDA(cudaEventCreate(&g_ws.e0));
-        CHB_CUDA(cudaEventCreate(&g_ws.e1));
+int ensure_ws(ExecWs &w, size_t ctr_bytes, size_t inv_bytes) {
+    if (!w.st) {
+        CHB_CUDA(cudaMalloc(&w.st, sizeof(ExecState)));
+        CHB_CUDA(cudaEventCreate(&w.e0));
+        CHB_CUDA(cudaEventCreate(&w.e1));
     }
-    if (ctr_bytes > g_ws.ctr_bytes) {
-        if (g_ws.ctr) cudaFree(g_ws.ctr);
-        g_ws.ctr = nullptr;
-        CHB_CUDA(cudaMalloc(&g_ws.ctr, ctr_bytes));
-        g_ws.ctr_bytes = ctr_bytes;
+    if (ctr_bytes > w.ctr_bytes) {
+        if (w.ctr) cudaFree(w.ctr);
+        w.ctr = nullptr;
+        CHB_CUDA(cudaMalloc(&w.ctr, ctr_bytes));
+        w.ctr_bytes = ctr_bytes;
     }
-    if (inv_bytes > g_ws.inv_bytes) {
-        if (g_ws.inv) cudaFree(g_ws.inv);
-        g_ws.inv = nullptr;
-        CHB_CUDA(cudaMalloc(&g_ws.inv, inv_bytes));
-        g_ws.inv_bytes = inv_bytes;
+    if (inv_bytes > w.inv_bytes) {
+        if (w.inv) cudaFree(w.inv);
+        w.inv = nullptr;
+        CHB_CUDA(cudaMalloc(&w.inv, inv_bytes));
+        w.inv_bytes = inv_bytes;
     }
     return 0;
 }
@@ -523,8 +530,9 @@ static int set_dag_smem() {
 }
 
 int run_cholesky_dag(int mode, cham_uplo_t uplo, CHAM_desc_t *A, CHAM_desc_t *B, cudaStream_t s,
-                     ExecResult *res, int split) {
+                     ExecResult *res, int split, ExecWs *wsp, int grid_req) {
     Context &c = ctx();
+    ExecWs &w = wsp ? *wsp : g_ws;
     const int N = A->n;
     const int NB = A->nb;
     const int NT = A->nt;
@@ -545,14 +553,21 @@ int run_cholesky_dag(int mode, cham_uplo_t uplo, CHAM_desc_t *A, CHAM_desc_t *B,
     else if (tc) rc = set_dag_smem<float, SPLIT_BF16X3, true>();
     else rc = set_dag_smem<float, SPLIT_BF16X3, false>();
     if (rc) return rc;
-    const int grid = c.num_sms;
-    Shape sh{mode, N, NB, nrhs, NBB, grid};
+    const int grid = (grid_req > 0) ? std::min(grid_req, c.num_sms) : c.num_sms;
+    const int prof = !f32 ? PROF_FP64 : (tc ? PROF_F32_TC05 : PROF_F32_MMA);
+    // The task list depends on N only through NT and the number of SUBB-row
+    // blocks of the last tile row, and on nrhs only through NTB (the kernel
+    // takes the exact sizes from the parameters): key the cache on that
+    // canonical shape so that callers with many distinct N share schedules.
+    const int last_sub = ((N - (NT - 1) * NB) + SUBB - 1) / SUBB;
+    const int canonN = (NT - 1) * NB + std::min(NB, last_sub * SUBB);
+    Shape sh{mode, canonN, NB, nrhs ? NTB * NBB : 0, NBB, grid, prof};
     Schedule *sch = get_schedule(sh);
     if (!sch) return CHAMELEON_ERR_OUT_OF_RESOURCES;
     const int NIB = (NB + IB - 1) / IB;
     const size_t nctr = (size_t)2 * NT * NT + (size_t)4 * NT * std::max(NTB, 1);
     const size_t esz = f32 ? sizeof(float) : sizeof(double);
-    rc = ensure_ws(nctr * sizeof(int), (size_t)NT * NIB * IB * IB * esz);
+    rc = ensure_ws(w, nctr * sizeof(int), (size_t)NT * NIB * IB * IB * esz);
     if (rc) return rc;
     int rcA = desc_upload(A);
     if (rcA) return rcA;
@@ -573,7 +588,7 @@ int run_cholesky_dag(int mode, cham_uplo_t uplo, CHAM_desc_t *A, CHAM_desc_t *B,
     p.B = nrhs ? B->mat : nullptr;
     p.b_off = nrhs ? priv(B)->dev.off : nullptr;
     p.b_ld = nrhs ? priv(B)->dev.ld : nullptr;
-    int *ctr = (int *)g_ws.ctr;
+    int *ctr = (int *)w.ctr;
     p.updA = ctr;
     p.panA = ctr + (size_t)NT * NT;
     const size_t nb4 = (size_t)NT * std::max(NTB, 1);
@@ -581,9 +596,9 @@ int run_cholesky_dag(int mode, cham_uplo_t uplo, CHAM_desc_t *A, CHAM_desc_t *B,
     p.fwdDone = p.fwdB + nb4;
     p.bwdB = p.fwdDone + nb4;
     p.bwdDone = p.bwdB + nb4;
-    p.invd = g_ws.inv;
+    p.invd = w.inv;
     p.NIB = NIB;
-    p.st = g_ws.st;
+    p.st = w.st;
     p.trace = (g_trace_buf && g_trace_cap >= p.ntasks) ? g_trace_buf : nullptr;
     p.wait_budget_ns = (unsigned long long)c.wait_budget_us * 1000ull;
     if (tc) {
@@ -591,21 +606,21 @@ int run_cholesky_dag(int mode, cham_uplo_t uplo, CHAM_desc_t *A, CHAM_desc_t *B,
         p.split_nkc = NB / tc05::BK;
         const size_t tile_bytes = (size_t)p.split_nrb * p.split_nkc * 2 * tc05::CHUNK_BYTES;
         const size_t bytes = (size_t)NT * (NT - 1) / 2 * tile_bytes;
-        if (bytes > g_ws.split_bytes) {
-            if (g_ws.split) cudaFree(g_ws.split);
-            g_ws.split = nullptr;
-            g_ws.split_bytes = 0;
-            CHB_CUDA(cudaMalloc(&g_ws.split, bytes));
-            g_ws.split_bytes = bytes;
+        if (bytes > w.split_bytes) {
+            if (w.split) cudaFree(w.split);
+            w.split = nullptr;
+            w.split_bytes = 0;
+            CHB_CUDA(cudaMalloc(&w.split, bytes));
+            w.split_bytes = bytes;
         }
-        p.split = g_ws.split;
+        p.split = w.split;
     }
     ExecState init{};
     init.info = INT_MAX;
     init.stuck_task = -1;
     CHB_CUDA(cudaMemsetAsync(ctr, 0, nctr * sizeof(int), s));
-    CHB_CUDA(cudaMemcpyAsync(g_ws.st, &init, sizeof(init), cudaMemcpyHostToDevice, s));
-    CHB_CUDA(cudaEventRecord(g_ws.e0, s));
+    CHB_CUDA(cudaMemcpyAsync(w.st, &init, sizeof(init), cudaMemcpyHostToDevice, s));
+    CHB_CUDA(cudaEventRecord(w.e0, s));
     if (p.ntasks > 0) {
         CHB_LAUNCHED(1);
         if (!f32)
@@ -622,11 +637,11 @@ int run_cholesky_dag(int mode, cham_uplo_t uplo, CHAM_desc_t *A, CHAM_desc_t *B,
                 <<<grid, NT_CTA, dag_smem_bytes<float, SPLIT_BF16X3, false>(), s>>>(p);
     }
     CHB_CUDA(cudaGetLastError());
-    CHB_CUDA(cudaEventRecord(g_ws.e1, s));
+    CHB_CUDA(cudaEventRecord(w.e1, s));
     ExecState out{};
-    CHB_CUDA(cudaMemcpyAsync(&out, g_ws.st, sizeof(out), cudaMemcpyDeviceToHost, s));
+    CHB_CUDA(cudaMemcpyAsync(&out, w.st, sizeof(out), cudaMemcpyDeviceToHost, s));
     CHB_CUDA(cudaStreamSynchronize(s));
-    CHB_CUDA(cudaEventElapsedTime(&res->ms, g_ws.e0, g_ws.e1));
+    CHB_CUDA(cudaEventElapsedTime(&res->ms, w.e0, w.e1));
     res->info = (out.info == INT_MAX) ? 0 : out.info;
     res->error = out.error;
     if (out.error) {
@@ -663,16 +678,16 @@ extern "C" int CHAM_B200_Trace_Read(void *host_out, int count) {
 }
 // Copy the schedule of a shape into `out` (host only; used by the CPU tests of
 // the DAG logic and by the trace tooling).  Returns the task count written.
-extern "C" int CHAM_B200_Schedule_Build(int mode, int N, int NB, int nrhs, int NBB, int workers, void *out,
-                                        int cap) {
+extern "C" int CHAM_B200_Schedule_Build(int mode, int N, int NB, int nrhs, int NBB, int workers, int prof,
+                                        void *out, int cap) {
     using namespace chb;
-    const std::vector<Task> t = build_order(Shape{mode, N, NB, nrhs, NBB, workers});
+    const std::vector<Task> t = build_order(Shape{mode, N, NB, nrhs, NBB, workers, prof});
     const int n = std::min<int>((int)t.size(), cap);
     memcpy(out, t.data(), sizeof(Task) * (size_t)n);
     return n;
 }
 // Number of tasks of the schedule of a given shape (for tests and tracing).
-extern "C" int CHAM_B200_Schedule_Size(int mode, int N, int NB, int nrhs, int NBB, int workers) {
+extern "C" int CHAM_B200_Schedule_Size(int mode, int N, int NB, int nrhs, int NBB, int workers, int prof) {
     using namespace chb;
-    return (int)build_order(Shape{mode, N, NB, nrhs, NBB, workers}).size();
+    return (int)build_order(Shape{mode, N, NB, nrhs, NBB, workers, prof}).size();
 }

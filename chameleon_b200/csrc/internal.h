@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <stdio.h>
+#include <atomic>
 #include <map>
 #include <mutex>
 #include <string>
@@ -34,7 +35,7 @@ struct Context {
 Context &ctx();
 
 // Count of this library's kernel launches (reported by the benchmark).
-extern unsigned long long g_launch_count;
+extern std::atomic<unsigned long long> g_launch_count;
 #define CHB_LAUNCHED(n) (::chb::g_launch_count += (n))
 
 // Phase breakdown of the last mixed-precision solve (device times, ms).
@@ -77,11 +78,64 @@ int desc_tile_cols(const CHAM_desc_t *d, int n);
 int64_t desc_tile_off(const CHAM_desc_t *d, int m, int n);
 int desc_tile_ld(const CHAM_desc_t *d, int m);
 int desc_upload(CHAM_desc_t *d);
+cudaStream_t meta_stream();   // private stream of descriptor metadata uploads
 // Create a descriptor viewing a device column-major array (ld = lda) with
 // tile size nb: tile (m,n) at A + m*nb + n*nb*lda (control/descriptor.h:238-252).
 int desc_create_cm(CHAM_desc_t **desc, double *dA, int lda, int m, int n, int nb);
 int desc_sync_to_host(CHAM_desc_t *d);
 double *staging(int slot, size_t bytes);   // LAPACK-layout staging buffers (0: A, 1: B, 2: X)
+// Copy the rows x cols block of a host array (leading dimension ld) into
+// staging slot `slot` with leading dimension rows; and back.
+double *stage_in(int slot, const double *host, int ld, int rows, int cols, cudaStream_t s);
+int stage_out(double *host, int ld, const double *dev, int rows, int cols, cudaStream_t s);
+
+// Device workspace of one executor stream: dependency counters, inverted
+// diagonal blocks, split-BF16 panel chunks (tcgen05 path), state, events.
+// Grow-only; one per concurrent caller (the synchronous API uses a global one).
+struct ExecWs {
+    uint8_t *split = nullptr;
+    size_t split_bytes = 0;
+    size_t ctr_bytes = 0, inv_bytes = 0;
+    void *ctr = nullptr;
+    void *inv = nullptr;
+    ExecState *st = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+};
+
+// Workspace of one mixed-precision solve stream (mixed.cu).
+struct MixedWs {
+    CHAM_desc_t *A32 = nullptr, *B32 = nullptr, *R = nullptr;
+    int N = -1, NB = -1, nrhs = -1;
+    unsigned long long *rmax = nullptr, *xmax = nullptr;
+    double *colsum = nullptr;
+    int *flag = nullptr;
+    int cap_rhs = 0, cap_n = 0;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+};
+
+// Batched dposv (batch.cu): one item per independent system; offsets in
+// elements into the batch's A / B arrays.
+struct BatchItem {
+    int64_t a_off, b_off;
+    int n, nrhs, lda, ldb;   // nrhs == 0: factor only
+    int info_idx;
+    int pad;
+};
+// Device workspace of one batch stream (grow-only).
+struct BatchWs {
+    void *items = nullptr;
+    size_t items_bytes = 0;
+    double *scratch = nullptr;
+    size_t scratch_bytes = 0;
+    int *cursor = nullptr;
+    int *info = nullptr;
+    size_t info_n = 0;
+};
+extern BatchWs g_bws;   // the synchronous API's
+int bws_reserve(BatchWs &ws, size_t item_bytes, size_t scratch_bytes, size_t ninfo);
+// One persistent launch over `items` (sorted in place, largest first).
+int launch_posv_batch(std::vector<BatchItem> &items, double *A, double *B, int upper, int *info, cudaStream_t s,
+                      BatchWs &ws);
 
 // Executor entry (executor.cu).
 struct ExecResult {
@@ -91,7 +145,15 @@ struct ExecResult {
 };
 // A, B: double descriptors (FP64 path) or float descriptors (split-precision
 // path, `split` = SPLIT_BF16X3 or SPLIT_TF32X3 from core.cuh).
+// ws: workspace (nullptr: the global one of the synchronous API); grid:
+// number of persistent CTAs (0: one per SM).
 int run_cholesky_dag(int mode, cham_uplo_t uplo, CHAM_desc_t *A, CHAM_desc_t *B, cudaStream_t s,
-                     ExecResult *res, int split = 0);
+                     ExecResult *res, int split = 0, ExecWs *ws = nullptr, int grid = 0);
+
+// Mixed-precision solve on an explicit stream and workspaces (mixed.cu).
+// factored = true: m.A32 already holds the low-precision factor of A (resident
+// factor re-use); only the solve and refinement run.
+int mixed_posv_ws(cham_uplo_t uplo, int precision, CHAM_desc_t *A, CHAM_desc_t *B, CHAM_desc_t *X, int *iter_out,
+                  CHAM_b200_refine_info_t *info, cudaStream_t s, MixedWs &m, ExecWs *ews, int grid, bool factored);
 
 }  // namespace chb

@@ -195,52 +195,48 @@ static int ew_grid(int64_t total) {
 }
 
 namespace {
-struct MixedWs {
-    CHAM_desc_t *A32 = nullptr, *B32 = nullptr, *R = nullptr;
-    int N = -1, NB = -1, nrhs = -1;
-    unsigned long long *rmax = nullptr, *xmax = nullptr;
-    double *colsum = nullptr;
-    int *flag = nullptr;
-    int cap_rhs = 0, cap_n = 0;
-};
-MixedWs g_mws;
+MixedWs g_mws;   // workspace of the synchronous API entry points
 
-int mixed_reserve(int N, int NB, int nrhs) {
-    if (g_mws.N != N || g_mws.NB != NB) {
-        if (g_mws.A32) CHAMELEON_Desc_Destroy(&g_mws.A32);
-        int rc = CHAMELEON_Desc_Create(&g_mws.A32, CHAMELEON_MAT_ALLOC_TILE, ChamRealFloat, NB, NB, NB * NB, N, N, 0,
+int mixed_reserve(MixedWs &m, int N, int NB, int nrhs) {
+    if (m.N != N || m.NB != NB) {
+        if (m.A32) CHAMELEON_Desc_Destroy(&m.A32);
+        int rc = CHAMELEON_Desc_Create(&m.A32, CHAMELEON_MAT_ALLOC_TILE, ChamRealFloat, NB, NB, NB * NB, N, N, 0,
                                        0, N, N, 1, 1);
         if (rc) return rc;
-        if ((rc = desc_upload(g_mws.A32))) return rc;
-        g_mws.N = N;
-        g_mws.NB = NB;
-        g_mws.nrhs = -1;
+        if ((rc = desc_upload(m.A32))) return rc;
+        m.N = N;
+        m.NB = NB;
+        m.nrhs = -1;
     }
-    if (g_mws.nrhs != nrhs) {
-        if (g_mws.B32) CHAMELEON_Desc_Destroy(&g_mws.B32);
-        if (g_mws.R) CHAMELEON_Desc_Destroy(&g_mws.R);
-        int rc = CHAMELEON_Desc_Create(&g_mws.B32, CHAMELEON_MAT_ALLOC_TILE, ChamRealFloat, NB, NB, NB * NB, N, nrhs,
+    if (m.nrhs != nrhs) {
+        if (m.B32) CHAMELEON_Desc_Destroy(&m.B32);
+        if (m.R) CHAMELEON_Desc_Destroy(&m.R);
+        int rc = CHAMELEON_Desc_Create(&m.B32, CHAMELEON_MAT_ALLOC_TILE, ChamRealFloat, NB, NB, NB * NB, N, nrhs,
                                        0, 0, N, nrhs, 1, 1);
         if (!rc)
-            rc = CHAMELEON_Desc_Create(&g_mws.R, CHAMELEON_MAT_ALLOC_TILE, ChamRealDouble, NB, NB, NB * NB, N, nrhs, 0,
+            rc = CHAMELEON_Desc_Create(&m.R, CHAMELEON_MAT_ALLOC_TILE, ChamRealDouble, NB, NB, NB * NB, N, nrhs, 0,
                                        0, N, nrhs, 1, 1);
         if (rc) return rc;
-        if ((rc = desc_upload(g_mws.B32)) || (rc = desc_upload(g_mws.R))) return rc;
-        g_mws.nrhs = nrhs;
+        if ((rc = desc_upload(m.B32)) || (rc = desc_upload(m.R))) return rc;
+        m.nrhs = nrhs;
     }
-    if (nrhs > g_mws.cap_rhs) {
-        if (g_mws.rmax) cudaFree(g_mws.rmax);
-        if (g_mws.xmax) cudaFree(g_mws.xmax);
-        CHB_CUDA(cudaMalloc(&g_mws.rmax, nrhs * sizeof(unsigned long long)));
-        CHB_CUDA(cudaMalloc(&g_mws.xmax, nrhs * sizeof(unsigned long long)));
-        g_mws.cap_rhs = nrhs;
+    if (nrhs > m.cap_rhs) {
+        if (m.rmax) cudaFree(m.rmax);
+        if (m.xmax) cudaFree(m.xmax);
+        CHB_CUDA(cudaMalloc(&m.rmax, nrhs * sizeof(unsigned long long)));
+        CHB_CUDA(cudaMalloc(&m.xmax, nrhs * sizeof(unsigned long long)));
+        m.cap_rhs = nrhs;
     }
-    if (N > g_mws.cap_n) {
-        if (g_mws.colsum) cudaFree(g_mws.colsum);
-        CHB_CUDA(cudaMalloc(&g_mws.colsum, N * sizeof(double)));
-        g_mws.cap_n = N;
+    if (N > m.cap_n) {
+        if (m.colsum) cudaFree(m.colsum);
+        CHB_CUDA(cudaMalloc(&m.colsum, N * sizeof(double)));
+        m.cap_n = N;
     }
-    if (!g_mws.flag) CHB_CUDA(cudaMalloc(&g_mws.flag, sizeof(int)));
+    if (!m.flag) CHB_CUDA(cudaMalloc(&m.flag, sizeof(int)));
+    if (!m.e0) {
+        CHB_CUDA(cudaEventCreate(&m.e0));
+        CHB_CUDA(cudaEventCreate(&m.e1));
+    }
     return 0;
 }
 
@@ -251,14 +247,14 @@ static SymTiles symtiles(CHAM_desc_t *A, cham_uplo_t uplo) {
     return SymTiles{(double *)A->mat, priv(A)->dev.off, priv(A)->dev.ld, A->nt, A->n, A->nb, uplo == ChamUpper};
 }
 
-double sym_norm_inf(CHAM_desc_t *A, cham_uplo_t uplo, cudaStream_t s) {
-    if (desc_upload(A) || mixed_reserve(A->n, A->nb, std::max(1, g_mws.nrhs))) return -1.0;
+double sym_norm_inf(CHAM_desc_t *A, cham_uplo_t uplo, cudaStream_t s, MixedWs &m) {
+    if (desc_upload(A) || mixed_reserve(m, A->n, A->nb, std::max(1, m.nrhs))) return -1.0;
     const int NT = A->nt;
-    cudaMemsetAsync(g_mws.colsum, 0, A->n * sizeof(double), s);
-    sym_absnorm_kernel<<<NT * (NT + 1) / 2, 256, 0, s>>>(symtiles(A, uplo), g_mws.colsum);
+    cudaMemsetAsync(m.colsum, 0, A->n * sizeof(double), s);
+    sym_absnorm_kernel<<<NT * (NT + 1) / 2, 256, 0, s>>>(symtiles(A, uplo), m.colsum);
     CHB_LAUNCHED(1);
     std::vector<double> h(A->n);
-    cudaMemcpyAsync(h.data(), g_mws.colsum, A->n * sizeof(double), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(h.data(), m.colsum, A->n * sizeof(double), cudaMemcpyDeviceToHost, s);
     cudaStreamSynchronize(s);
     double r = 0;
     for (double v : h) r = std::max(r, v);
@@ -267,8 +263,8 @@ double sym_norm_inf(CHAM_desc_t *A, cham_uplo_t uplo, cudaStream_t s) {
 
 // R = B - A X and the per-column max |R|, max |X| (host copies).
 static int residual(CHAM_desc_t *A, cham_uplo_t uplo, CHAM_desc_t *B, CHAM_desc_t *X, cudaStream_t s,
-                    std::vector<double> &rn, std::vector<double> &xn) {
-    if (!uploaded(A) || !uploaded(B) || !uploaded(X) || !uploaded(g_mws.R)) return CHAMELEON_ERR_UNEXPECTED;
+                    std::vector<double> &rn, std::vector<double> &xn, MixedWs &m) {
+    if (!uploaded(A) || !uploaded(B) || !uploaded(X) || !uploaded(m.R)) return CHAMELEON_ERR_UNEXPECTED;
     if (!g_res_attr) {
         CHB_CUDA(cudaFuncSetAttribute(sym_residual_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)Cfg12864<double>::SMEM_BYTES));
@@ -277,16 +273,16 @@ static int residual(CHAM_desc_t *A, cham_uplo_t uplo, CHAM_desc_t *B, CHAM_desc_
     const int nrhs = B->n;
     const int nrb = (A->nb + 127) / 128;
     const int ncb = X->nt * ((X->nb + 63) / 64);
-    CHB_CUDA(cudaMemsetAsync(g_mws.rmax, 0, nrhs * sizeof(unsigned long long), s));
-    CHB_CUDA(cudaMemsetAsync(g_mws.xmax, 0, nrhs * sizeof(unsigned long long), s));
+    CHB_CUDA(cudaMemsetAsync(m.rmax, 0, nrhs * sizeof(unsigned long long), s));
+    CHB_CUDA(cudaMemsetAsync(m.xmax, 0, nrhs * sizeof(unsigned long long), s));
     sym_residual_kernel<<<A->nt * nrb * ncb, NT_CTA, Cfg12864<double>::SMEM_BYTES, s>>>(
-        symtiles(A, uplo), tmap(X), tmap(B), tmap(g_mws.R), nrhs, nrb, ncb, g_mws.rmax);
-    colmax_kernel<<<ew_grid((int64_t)X->m * nrhs), 256, 0, s>>>(tmap(X), X->m, nrhs, g_mws.xmax);
+        symtiles(A, uplo), tmap(X), tmap(B), tmap(m.R), nrhs, nrb, ncb, m.rmax);
+    colmax_kernel<<<ew_grid((int64_t)X->m * nrhs), 256, 0, s>>>(tmap(X), X->m, nrhs, m.xmax);
     CHB_LAUNCHED(2);
     CHB_CUDA(cudaGetLastError());
     std::vector<unsigned long long> hr(nrhs), hx(nrhs);
-    CHB_CUDA(cudaMemcpyAsync(hr.data(), g_mws.rmax, nrhs * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
-    CHB_CUDA(cudaMemcpyAsync(hx.data(), g_mws.xmax, nrhs * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+    CHB_CUDA(cudaMemcpyAsync(hr.data(), m.rmax, nrhs * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+    CHB_CUDA(cudaMemcpyAsync(hx.data(), m.xmax, nrhs * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
     CHB_CUDA(cudaStreamSynchronize(s));
     rn.resize(nrhs);
     xn.resize(nrhs);
@@ -354,19 +350,15 @@ struct PhaseClock {
 };
 
 // The refinement driver.  A: FP64 (uplo triangle), B: N x nrhs FP64, X: output.
-int mixed_posv(cham_uplo_t uplo, int precision, CHAM_desc_t *A, CHAM_desc_t *B, CHAM_desc_t *X, int *iter_out,
-               CHAM_b200_refine_info_t *info) {
+int mixed_posv_ws(cham_uplo_t uplo, int precision, CHAM_desc_t *A, CHAM_desc_t *B, CHAM_desc_t *X, int *iter_out,
+                  CHAM_b200_refine_info_t *info, cudaStream_t s, MixedWs &m, ExecWs *ews, int grid, bool factored) {
     Context &c = ctx();
-    cudaStream_t s = c.stream;
     const int N = A->n, nrhs = B->n, NB = A->nb;
     int iter = 0;
     CHAM_b200_refine_info_t inf{};
     inf.precision = precision;
-    static cudaEvent_t e0 = nullptr, e1 = nullptr;
-    if (!e0) {
-        CHB_CUDA(cudaEventCreate(&e0));
-        CHB_CUDA(cudaEventCreate(&e1));
-    }
+    if (int rc0 = mixed_reserve(m, N, NB, nrhs)) return rc0;
+    cudaEvent_t e0 = m.e0, e1 = m.e1;
     cudaEventRecord(e0, s);
     int rc = 0;
     ExecResult res;
@@ -375,24 +367,23 @@ int mixed_posv(cham_uplo_t uplo, int precision, CHAM_desc_t *A, CHAM_desc_t *B, 
     MixedStats st;
     PhaseClock clk(s);
     if (!fallback) {
-        if ((rc = mixed_reserve(N, NB, nrhs))) return rc;
         if ((rc = desc_upload(A)) || (rc = desc_upload(B)) || (rc = desc_upload(X))) return rc;
         clk.tic();
-        const double anrm = sym_norm_inf(A, uplo, s);
+        const double anrm = sym_norm_inf(A, uplo, s, m);
         const double cte = anrm * 1.1102230246251565e-16 * sqrt((double)N);
         const int split = (precision == CHAM_B200_PREC_FP32) ? SPLIT_TF32X3 : SPLIT_BF16X3;
-        CHB_CUDA(cudaMemsetAsync(g_mws.flag, 0, sizeof(int), s));
-        if ((rc = cast_desc(A, g_mws.A32, s, g_mws.flag))) return rc;
-        if ((rc = cast_desc(B, g_mws.B32, s, g_mws.flag))) return rc;
+        CHB_CUDA(cudaMemsetAsync(m.flag, 0, sizeof(int), s));
+        if (!factored && (rc = cast_desc(A, m.A32, s, m.flag))) return rc;
+        if ((rc = cast_desc(B, m.B32, s, m.flag))) return rc;
         int ovf = 0;
-        CHB_CUDA(cudaMemcpyAsync(&ovf, g_mws.flag, sizeof(int), cudaMemcpyDeviceToHost, s));
+        CHB_CUDA(cudaMemcpyAsync(&ovf, m.flag, sizeof(int), cudaMemcpyDeviceToHost, s));
         clk.toc(st.cast_ms);
         if (ovf) {
             iter = -2;
             fallback = true;
         }
         if (!fallback) {
-            if ((rc = run_cholesky_dag(MODE_FACT | MODE_SOLVE, uplo, g_mws.A32, g_mws.B32, s, &res, split))) return rc;
+            if ((rc = run_cholesky_dag(factored ? MODE_SOLVE : (MODE_FACT | MODE_SOLVE), uplo, m.A32, m.B32, s, &res, split, ews, grid))) return rc;
             st.factor_ms += res.ms;
             if (res.error) return res.error;
             if (res.info) {
@@ -401,24 +392,24 @@ int mixed_posv(cham_uplo_t uplo, int precision, CHAM_desc_t *A, CHAM_desc_t *B, 
             }
         }
         if (!fallback) {
-            if ((rc = cast_desc(g_mws.B32, X, s, nullptr))) return rc;
+            if ((rc = cast_desc(m.B32, X, s, nullptr))) return rc;
             std::vector<double> rn, xn;
             clk.tic();
-            if ((rc = residual(A, uplo, B, X, s, rn, xn))) return rc;
+            if ((rc = residual(A, uplo, B, X, s, rn, xn, m))) return rc;
             clk.toc(st.residual_ms);
             bool ok = converged(rn, xn, cte, &berr);
             int it = 0;
             while (!ok && it < c.refine_maxiter) {
                 ++it;
-                if ((rc = cast_desc(g_mws.R, g_mws.B32, s, nullptr))) return rc;
-                if ((rc = run_cholesky_dag(MODE_SOLVE, uplo, g_mws.A32, g_mws.B32, s, &res, split))) return rc;
+                if ((rc = cast_desc(m.R, m.B32, s, nullptr))) return rc;
+                if ((rc = run_cholesky_dag(MODE_SOLVE, uplo, m.A32, m.B32, s, &res, split, ews, grid))) return rc;
                 st.refine_solve_ms += res.ms;
                 if (res.error) return res.error;
-                if (!uploaded(X) || !uploaded(g_mws.B32)) return CHAMELEON_ERR_UNEXPECTED;
-                add_correction<<<ew_grid((int64_t)N * nrhs), 256, 0, s>>>(tmap(X), tmap(g_mws.B32), N, nrhs);
+                if (!uploaded(X) || !uploaded(m.B32)) return CHAMELEON_ERR_UNEXPECTED;
+                add_correction<<<ew_grid((int64_t)N * nrhs), 256, 0, s>>>(tmap(X), tmap(m.B32), N, nrhs);
                 CHB_LAUNCHED(1);
                 CHB_CUDA(cudaGetLastError());
-                if ((rc = residual(A, uplo, B, X, s, rn, xn))) return rc;
+                if ((rc = residual(A, uplo, B, X, s, rn, xn, m))) return rc;
                 ok = converged(rn, xn, cte, &berr);
             }
             if (ok) {
@@ -431,7 +422,7 @@ int mixed_posv(cham_uplo_t uplo, int precision, CHAM_desc_t *A, CHAM_desc_t *B, 
     }
     if (fallback) {
         if ((rc = cast_desc(B, X, s, nullptr))) return rc;
-        if ((rc = run_cholesky_dag(MODE_FACT | MODE_SOLVE, uplo, A, X, s, &res))) return rc;
+        if ((rc = run_cholesky_dag(MODE_FACT | MODE_SOLVE, uplo, A, X, s, &res, 0, ews, grid))) return rc;
         if (res.error) return res.error;
         if (res.info) return res.info;
         inf.fallback = (precision != CHAM_B200_PREC_FP64);
@@ -445,7 +436,7 @@ int mixed_posv(cham_uplo_t uplo, int precision, CHAM_desc_t *A, CHAM_desc_t *B, 
     st.total_ms = ms;
     st.iterations = iter;
     st.fallback = fallback ? 1 : 0;
-    g_mixed_stats = st;
+    if (&m == &g_mws) g_mixed_stats = st;
     inf.iterations = iter;
     inf.backward_error = berr;
     inf.seconds = ms * 1e-3;
@@ -453,6 +444,11 @@ int mixed_posv(cham_uplo_t uplo, int precision, CHAM_desc_t *A, CHAM_desc_t *B, 
     if (info) *info = inf;
     if (fallback) desc_sync_to_host(A);
     return desc_sync_to_host(X);
+}
+
+int mixed_posv(cham_uplo_t uplo, int precision, CHAM_desc_t *A, CHAM_desc_t *B, CHAM_desc_t *X, int *iter_out,
+               CHAM_b200_refine_info_t *info) {
+    return mixed_posv_ws(uplo, precision, A, B, X, iter_out, info, ctx().stream, g_mws, nullptr, 0, false);
 }
 
 }  // namespace chb
@@ -521,27 +517,31 @@ int CHAMELEON_dsposv(cham_uplo_t uplo, int N, int NRHS, double *A, int LDA, doub
         return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
     };
     const bool ad = on_dev(A), bd = on_dev(B), xd = on_dev(X);
+    // host arrays are staged densely (ld = N): only the N x cols block moves
     double *dA = A, *dB = B, *dX = X;
-    const size_t ab = (size_t)LDA * N * 8, bb = (size_t)LDB * NRHS * 8, xb = (size_t)LDX * NRHS * 8;
+    int lda = LDA, ldb = LDB, ldx = LDX;
     if (!ad) {
-        if (!(dA = staging(0, ab))) return CHAMELEON_ERR_OUT_OF_RESOURCES;
-        CHB_CUDA(cudaMemcpyAsync(dA, A, ab, cudaMemcpyHostToDevice, s));
+        if (!(dA = stage_in(0, A, LDA, N, N, s))) return CHAMELEON_ERR_OUT_OF_RESOURCES;
+        lda = N;
     }
     if (!bd) {
-        if (!(dB = staging(1, bb))) return CHAMELEON_ERR_OUT_OF_RESOURCES;
-        CHB_CUDA(cudaMemcpyAsync(dB, B, bb, cudaMemcpyHostToDevice, s));
+        if (!(dB = stage_in(1, B, LDB, N, NRHS, s))) return CHAMELEON_ERR_OUT_OF_RESOURCES;
+        ldb = N;
     }
-    if (!xd && !(dX = staging(2, xb))) return CHAMELEON_ERR_OUT_OF_RESOURCES;
+    if (!xd) {
+        if (!(dX = staging(2, (size_t)N * NRHS * 8))) return CHAMELEON_ERR_OUT_OF_RESOURCES;
+        ldx = N;
+    }
     CHAM_desc_t *Ad, *Bd, *Xd;
-    desc_create_cm(&Ad, dA, LDA, N, N, c.tile_size);
-    desc_create_cm(&Bd, dB, LDB, N, NRHS, c.tile_size);
-    desc_create_cm(&Xd, dX, LDX, N, NRHS, c.tile_size);
+    desc_create_cm(&Ad, dA, lda, N, N, c.tile_size);
+    desc_create_cm(&Bd, dB, ldb, N, NRHS, c.tile_size);
+    desc_create_cm(&Xd, dX, ldx, N, NRHS, c.tile_size);
     const int prec = c.precision == CHAM_B200_PREC_FP64 ? CHAM_B200_PREC_BF16X3 : c.precision;
     int iter = 0;
     rc = mixed_posv(uplo, prec, Ad, Bd, Xd, &iter, nullptr);
     if (ITER) *ITER = iter;
-    if (!xd) cudaMemcpyAsync(X, dX, xb, cudaMemcpyDeviceToHost, s);
-    if (!ad && iter < 0) cudaMemcpyAsync(A, dA, ab, cudaMemcpyDeviceToHost, s);
+    if (!xd) stage_out(X, LDX, dX, N, NRHS, s);
+    if (!ad && iter < 0) stage_out(A, LDA, dA, N, N, s);
     cudaStreamSynchronize(s);
     CHAMELEON_Desc_Destroy(&Ad);
     CHAMELEON_Desc_Destroy(&Bd);
@@ -556,7 +556,7 @@ int CHAM_B200_Mixed_Factor_Only(cham_uplo_t uplo, int precision, CHAM_desc_t *A,
     if (rc) return rc;
     if (!A || !B || precision == CHAM_B200_PREC_FP64) return CHAMELEON_ERR_ILLEGAL_VALUE;
     cudaStream_t s = ctx().stream;
-    if ((rc = mixed_reserve(A->n, A->nb, B->n))) return rc;
+    if ((rc = mixed_reserve(g_mws, A->n, A->nb, B->n))) return rc;
     CHB_CUDA(cudaMemsetAsync(g_mws.flag, 0, sizeof(int), s));
     if ((rc = cast_desc(A, g_mws.A32, s, g_mws.flag)) || (rc = cast_desc(B, g_mws.B32, s, g_mws.flag))) return rc;
     ExecResult res;

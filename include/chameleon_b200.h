@@ -278,6 +278,49 @@ int CHAM_B200_dposv_batch(cham_uplo_t uplo, int count, const int *n, const int *
                           double *A, const int64_t *a_off, double *B, const int64_t *b_off,
                           int *info, void *cuda_stream);
 
+/* ------------------------------------------------------------------------- */
+/* Serving loop (new; the reference solves one system per call).  A server    */
+/* owns worker threads and CUDA streams; host threads submit solve requests  */
+/* of any order and right-hand-side count and read the results when          */
+/* `status` leaves CHAM_B200_REQ_PENDING (or after Serve_Drain).  Small      */
+/* systems (N <= small_n) are coalesced into one batched launch per wave of   */
+/* arrivals; larger ones run the mixed-precision solver (FP64-accurate) on    */
+/* one of `slots` streams.  A request is admitted when its device memory      */
+/* fits in the HBM budget (0: 80% of the free memory at creation).           */
+/* ------------------------------------------------------------------------- */
+#define CHAM_B200_REQ_PENDING (1 << 30)
+typedef struct cham_b200_server_s *CHAM_b200_server_t;
+typedef struct cham_b200_request_s {
+    /* in: column-major host arrays (pinned memory gives asynchronous copies) */
+    int N, nrhs;
+    int uplo;                   /* ChamLower / ChamUpper: triangle of A read     */
+    const double *A; int lda;   /* NULL: solve with the factor kept under key   */
+    const double *B; int ldb;   /* N x nrhs                                       */
+    double *X;       int ldx;   /* N x nrhs, written on completion               */
+    long long factor_key;       /* >= 0 with A: keep the factor under this key
+                                   (replaces an older one); >= 0 without A: use
+                                   it; < 0: nothing kept                          */
+    /* out */
+    int status;                 /* PENDING, then 0, > 0 (leading minor not
+                                   positive definite) or CHAMELEON_ERR_*;
+                                   CHAMELEON_ERR_NOT_FOUND: no factor under key  */
+    int iterations;             /* refinement iterations (dsposv ITER; 0 for the
+                                   FP64 batched path)                             */
+    double t_submit, t_start, t_done;   /* CHAM_B200_Serve_Now() clock          */
+} CHAM_b200_request_t;
+typedef struct cham_b200_serve_stats_s {
+    long long completed, batches, batched_requests, max_batch;
+    long long reused_factors, kept_factors;
+    double bytes_in_use, budget_bytes;
+} CHAM_b200_serve_stats_t;
+int    CHAM_B200_Serve_Create(CHAM_b200_server_t *server, int slots, double hbm_budget_bytes, int small_n);
+/* The request and its arrays must stay valid until it completes. */
+int    CHAM_B200_Serve_Submit(CHAM_b200_server_t server, CHAM_b200_request_t *request);
+int    CHAM_B200_Serve_Drain(CHAM_b200_server_t server);       /* wait for all submitted */
+int    CHAM_B200_Serve_Stats(CHAM_b200_server_t server, CHAM_b200_serve_stats_t *stats);
+int    CHAM_B200_Serve_Destroy(CHAM_b200_server_t server);     /* drains first          */
+double CHAM_B200_Serve_Now(void);
+
 #ifdef __cplusplus
 }
 #endif

@@ -99,9 +99,10 @@ SHAPES = [(15, 16, 1, 16), (37, 17, 22, 17), (300, 128, 5, 128), (700, 256, 70, 
 
 @pytest.mark.parametrize("N,NB,nrhs,NBB", SHAPES)
 @pytest.mark.parametrize("workers", [1, 7, 148])
-def test_schedule_is_deadlock_free(cb_host, N, NB, nrhs, NBB, workers):
+@pytest.mark.parametrize("prof", [0, 1, 2])
+def test_schedule_is_deadlock_free(cb_host, N, NB, nrhs, NBB, workers, prof):
     for mode in (FACT, SOLVE, FACT | SOLVE):
-        t = cb_host.schedule(mode, N, NB, nrhs if mode & SOLVE else 0, NBB, workers)
+        t = cb_host.schedule(mode, N, NB, nrhs if mode & SOLVE else 0, NBB, workers, prof)
         check_waits(t, mode, N, NB, nrhs if mode & SOLVE else 0, NBB)
 
 
