@@ -398,7 +398,7 @@ def serve_run(cb, load, reqs, arrivals, slots, key_pool=32):
     st = sv.stats()
     sv.close()
     for (Nr, kr, reuse, r, X, tarr) in pending:
-        done.append((Nr, kr, reuse, r.t_done - tarr, r.status, X, r.iterations))
+        done.append((Nr, kr, reuse, r.t_done - tarr, r.status, X, r.iterations, r.t_done - r.t_start))
     return done, t1 - t0, st
 
 
@@ -417,7 +417,13 @@ def serve_section(args, cb, rank):
     assert not bad, bad[:3]
     # accuracy on a sample of the capacity run
     worst = 0.0
-    for (Nr, kr, reuse, lat, status, X, it) in done[::max(1, len(done) // 12)]:
+    buckets = {}
+    for d in done:
+        key = "reuse" if d[2] else ("N<=512" if d[0] <= 512 else ("N<=2048" if d[0] <= 2048 else "N>2048"))
+        buckets.setdefault(key, []).append(d[7] * 1e3)
+    service = {k: {"count": len(v), "mean_ms": float(np.mean(v)), "p99_ms": float(np.percentile(v, 99))}
+               for k, v in sorted(buckets.items())}
+    for (Nr, kr, reuse, lat, status, X, it, svc) in done[::max(1, len(done) // 12)]:
         Ai = load.An[:Nr, :Nr].T
         Ai = np.tril(Ai) + np.tril(Ai, -1).T
         Bi = load.Bn[:kr, :Nr].T
@@ -460,6 +466,7 @@ def serve_section(args, cb, rank):
                     "Poisson arrivals; mixed BF16x3 + FP64 refinement for N>512, batched FP64 for N<=512; host "
                     "pinned inputs, latency = arrival -> result in host memory; %d slots" % slots,
         "capacity_solves_per_s": capacity, "capacity_requests": len(cap_reqs),
+        "capacity_service_ms": service,
         "backward_error_max_sampled": worst,
         "plain_per_request_solves_per_s": plain_rate,
         "speedup_vs_plain": (capacity / plain_rate) if plain_rate else None,

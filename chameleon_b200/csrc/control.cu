@@ -115,6 +115,42 @@ cudaStream_t meta_stream() {
     return ms;
 }
 
+// Stream-ordered workspace memory: allocation and release go through the
+// meta stream, so neither waits for kernels running on other streams (a plain
+// cudaFree synchronizes the whole device).  dev_alloc returns memory usable on
+// any stream; dev_free requires that no queued work still uses the memory.
+void *dev_alloc(size_t bytes) {
+    void *p = nullptr;
+    cudaStream_t ms = meta_stream();
+    if (cudaMallocAsync(&p, std::max<size_t>(bytes, 16), ms) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    if (cudaMemsetAsync(p, 0, std::max<size_t>(bytes, 16), ms) != cudaSuccess ||
+        cudaStreamSynchronize(ms) != cudaSuccess) {
+        cudaGetLastError();
+        cudaFreeAsync(p, ms);
+        return nullptr;
+    }
+    return p;
+}
+
+void dev_free(void *p) {
+    if (p) cudaFreeAsync(p, meta_stream());
+}
+
+int desc_create_tiled_on(CHAM_desc_t **desc, cham_flttype_t dtyp, void *storage, int nb, int m, int n) {
+    CHAM_desc_t *d = (CHAM_desc_t *)calloc(1, sizeof(CHAM_desc_t));
+    layout_init(d, dtyp, nb, nb, nb * nb, m, n, m, n);
+    d->mat = storage;
+    d->alloc_mat = 0;
+    d->schedopt = new DescPriv();
+    d->id = ctx().desc_ids++;
+    fill_tiles(d);
+    *desc = d;
+    return desc_upload(d);
+}
+
 int desc_upload(CHAM_desc_t *d) {
     DescPriv *pv = priv(d);
     if (pv->dev.off) return 0;

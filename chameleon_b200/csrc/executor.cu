@@ -487,22 +487,23 @@ Schedule *get_schedule(const Shape &s) {
 
 ExecWs g_ws;   // workspace of the synchronous API entry points
 
+// Grow-only workspace buffers, stream-ordered (no device-wide synchronization).
 int ensure_ws(ExecWs &w, size_t ctr_bytes, size_t inv_bytes) {
     if (!w.st) {
-        CHB_CUDA(cudaMalloc(&w.st, sizeof(ExecState)));
+        if (!(w.st = (ExecState *)dev_alloc(sizeof(ExecState)))) return CHAMELEON_ERR_OUT_OF_RESOURCES;
         CHB_CUDA(cudaEventCreate(&w.e0));
         CHB_CUDA(cudaEventCreate(&w.e1));
     }
     if (ctr_bytes > w.ctr_bytes) {
-        if (w.ctr) cudaFree(w.ctr);
-        w.ctr = nullptr;
-        CHB_CUDA(cudaMalloc(&w.ctr, ctr_bytes));
+        dev_free(w.ctr);
+        w.ctr_bytes = 0;
+        if (!(w.ctr = dev_alloc(ctr_bytes))) return CHAMELEON_ERR_OUT_OF_RESOURCES;
         w.ctr_bytes = ctr_bytes;
     }
     if (inv_bytes > w.inv_bytes) {
-        if (w.inv) cudaFree(w.inv);
-        w.inv = nullptr;
-        CHB_CUDA(cudaMalloc(&w.inv, inv_bytes));
+        dev_free(w.inv);
+        w.inv_bytes = 0;
+        if (!(w.inv = dev_alloc(inv_bytes))) return CHAMELEON_ERR_OUT_OF_RESOURCES;
         w.inv_bytes = inv_bytes;
     }
     return 0;
@@ -527,6 +528,16 @@ static int set_dag_smem() {
         done = true;
     }
     return 0;
+}
+
+void free_exec_ws(ExecWs &w) {
+    dev_free(w.split);
+    dev_free(w.ctr);
+    dev_free(w.inv);
+    dev_free(w.st);
+    if (w.e0) cudaEventDestroy(w.e0);
+    if (w.e1) cudaEventDestroy(w.e1);
+    w = ExecWs();
 }
 
 int run_cholesky_dag(int mode, cham_uplo_t uplo, CHAM_desc_t *A, CHAM_desc_t *B, cudaStream_t s,
@@ -607,10 +618,9 @@ int run_cholesky_dag(int mode, cham_uplo_t uplo, CHAM_desc_t *A, CHAM_desc_t *B,
         const size_t tile_bytes = (size_t)p.split_nrb * p.split_nkc * 2 * tc05::CHUNK_BYTES;
         const size_t bytes = (size_t)NT * (NT - 1) / 2 * tile_bytes;
         if (bytes > w.split_bytes) {
-            if (w.split) cudaFree(w.split);
-            w.split = nullptr;
+            dev_free(w.split);
             w.split_bytes = 0;
-            CHB_CUDA(cudaMalloc(&w.split, bytes));
+            if (!(w.split = (uint8_t *)dev_alloc(bytes))) return CHAMELEON_ERR_OUT_OF_RESOURCES;
             w.split_bytes = bytes;
         }
         p.split = w.split;

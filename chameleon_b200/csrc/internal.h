@@ -79,6 +79,13 @@ int64_t desc_tile_off(const CHAM_desc_t *d, int m, int n);
 int desc_tile_ld(const CHAM_desc_t *d, int m);
 int desc_upload(CHAM_desc_t *d);
 cudaStream_t meta_stream();   // private stream of descriptor metadata uploads
+// Workspace memory allocated / released in stream order on the meta stream
+// (no device-wide synchronization); zero-filled.
+void *dev_alloc(size_t bytes);
+void dev_free(void *p);
+// Tile-layout (CCRB) m x n descriptor on caller-owned device storage of at
+// least m * n elements (not freed by Desc_Destroy); uploaded.
+int desc_create_tiled_on(CHAM_desc_t **desc, cham_flttype_t dtyp, void *storage, int nb, int m, int n);
 // Create a descriptor viewing a device column-major array (ld = lda) with
 // tile size nb: tile (m,n) at A + m*nb + n*nb*lda (control/descriptor.h:238-252).
 int desc_create_cm(CHAM_desc_t **desc, double *dA, int lda, int m, int n, int nb);
@@ -104,10 +111,14 @@ struct ExecWs {
 
 // Workspace of one mixed-precision solve stream (mixed.cu).
 struct MixedWs {
-    CHAM_desc_t *A32 = nullptr, *B32 = nullptr, *R = nullptr;
+    CHAM_desc_t *A32 = nullptr, *B32 = nullptr, *R = nullptr;   // views on the buffers below
+    void *a32_buf = nullptr, *b32_buf = nullptr, *r_buf = nullptr;   // grow-only (dev_alloc)
+    size_t a32_cap = 0, b32_cap = 0, r_cap = 0;
     int N = -1, NB = -1, nrhs = -1;
     unsigned long long *rmax = nullptr, *xmax = nullptr;
     double *colsum = nullptr;
+    double *diag = nullptr;       // symmetric copies of the diagonal tiles (residuals)
+    size_t diag_cap = 0;
     int *flag = nullptr;
     int cap_rhs = 0, cap_n = 0;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -136,6 +147,10 @@ int bws_reserve(BatchWs &ws, size_t item_bytes, size_t scratch_bytes, size_t nin
 // One persistent launch over `items` (sorted in place, largest first).
 int launch_posv_batch(std::vector<BatchItem> &items, double *A, double *B, int upper, int *info, cudaStream_t s,
                       BatchWs &ws);
+
+// Release every buffer and descriptor of a workspace (its stream is idle).
+void free_mixed_ws(MixedWs &m);
+void free_exec_ws(ExecWs &w);
 
 // Executor entry (executor.cu).
 struct ExecResult {

@@ -95,17 +95,33 @@ __global__ void add_correction(TileMapD x, TileMapD d, int M, int N) {
 }
 
 // Logical lower tile (m,n), m >= n, of a symmetric matrix stored in `uplo`.
+// Only the `uplo` triangle is referenced (LAPACK convention): the diagonal
+// tiles are read through `diag`, full symmetric copies made by sym_diag_kernel.
 struct SymTiles {
     double *A;
     const int64_t *off;
     const int *ld;
     int NT, N, NB, upper;
+    double *diag;   // NT tiles of NB x NB, column-major, ld NB
     __device__ int tm(int m) const { return (m == NT - 1) ? N - m * NB : NB; }
     __device__ View L(int m, int n) const {
         if (!upper) return View{A + off[m + NT * n], 1, ld[m]};
         return View{A + off[n + NT * m], ld[n], 1};
     }
+    __device__ View D(int m) const { return View{diag + (int64_t)m * NB * NB, 1, NB}; }
 };
+
+// diag[m] = the full symmetric diagonal tile (m,m), from its `uplo` triangle.
+__global__ void sym_diag_kernel(SymTiles a) {
+    const int m = blockIdx.y;
+    const int n = a.tm(m);
+    const View L = a.L(m, m);
+    double *d = a.diag + (int64_t)m * a.NB * a.NB;
+    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n * n; idx += gridDim.x * blockDim.x) {
+        const int i = idx % n, j = idx / n;
+        d[i + (int64_t)j * a.NB] = (i >= j) ? *L.at(i, j) : *L.at(j, i);
+    }
+}
 
 // R = B - A X for symmetric A (one triangle stored), FP64 on DMMA.  One CTA
 // per (tile row m, 128-row block, 64-column block of the right-hand sides);
@@ -129,7 +145,7 @@ __global__ void __launch_bounds__(NT_CTA, 1) sym_residual_kernel(SymTiles a, Til
     Acc<Cfg12864<double>> acc;
     acc.zero();
     for (int n = 0; n < a.NT; ++n) {
-        const View An = (n <= m) ? a.L(m, n).sub(r0, 0) : a.L(n, m).t().sub(r0, 0);
+        const View An = (n < m) ? a.L(m, n).sub(r0, 0) : (n == m) ? a.D(m).sub(r0, 0) : a.L(n, m).t().sub(r0, 0);
         // X tile n, columns c0..c0+w: view of the N x nrhs operand in tile layout
         double *xp = xb.at<double>(n * a.NB, c0);
         const View Xn{xp, 1, xb.ld[n]};
@@ -197,13 +213,22 @@ static int ew_grid(int64_t total) {
 namespace {
 MixedWs g_mws;   // workspace of the synchronous API entry points
 
+// Grow-only buffer of a workspace: replaced (stream-ordered) when too small.
+static bool grow(void **buf, size_t *cap, size_t bytes) {
+    if (bytes <= *cap) return true;
+    dev_free(*buf);
+    *cap = 0;
+    *buf = dev_alloc(bytes);
+    if (!*buf) return false;
+    *cap = bytes;
+    return true;
+}
+
 int mixed_reserve(MixedWs &m, int N, int NB, int nrhs) {
     if (m.N != N || m.NB != NB) {
         if (m.A32) CHAMELEON_Desc_Destroy(&m.A32);
-        int rc = CHAMELEON_Desc_Create(&m.A32, CHAMELEON_MAT_ALLOC_TILE, ChamRealFloat, NB, NB, NB * NB, N, N, 0,
-                                       0, N, N, 1, 1);
-        if (rc) return rc;
-        if ((rc = desc_upload(m.A32))) return rc;
+        if (!grow(&m.a32_buf, &m.a32_cap, (size_t)N * N * sizeof(float))) return CHAMELEON_ERR_OUT_OF_RESOURCES;
+        if (int rc = desc_create_tiled_on(&m.A32, ChamRealFloat, m.a32_buf, NB, N, N)) return rc;
         m.N = N;
         m.NB = NB;
         m.nrhs = -1;
@@ -211,28 +236,29 @@ int mixed_reserve(MixedWs &m, int N, int NB, int nrhs) {
     if (m.nrhs != nrhs) {
         if (m.B32) CHAMELEON_Desc_Destroy(&m.B32);
         if (m.R) CHAMELEON_Desc_Destroy(&m.R);
-        int rc = CHAMELEON_Desc_Create(&m.B32, CHAMELEON_MAT_ALLOC_TILE, ChamRealFloat, NB, NB, NB * NB, N, nrhs,
-                                       0, 0, N, nrhs, 1, 1);
-        if (!rc)
-            rc = CHAMELEON_Desc_Create(&m.R, CHAMELEON_MAT_ALLOC_TILE, ChamRealDouble, NB, NB, NB * NB, N, nrhs, 0,
-                                       0, N, nrhs, 1, 1);
-        if (rc) return rc;
-        if ((rc = desc_upload(m.B32)) || (rc = desc_upload(m.R))) return rc;
+        if (!grow(&m.b32_buf, &m.b32_cap, (size_t)N * nrhs * sizeof(float)) ||
+            !grow(&m.r_buf, &m.r_cap, (size_t)N * nrhs * sizeof(double)))
+            return CHAMELEON_ERR_OUT_OF_RESOURCES;
+        if (int rc = desc_create_tiled_on(&m.B32, ChamRealFloat, m.b32_buf, NB, N, nrhs)) return rc;
+        if (int rc = desc_create_tiled_on(&m.R, ChamRealDouble, m.r_buf, NB, N, nrhs)) return rc;
         m.nrhs = nrhs;
     }
     if (nrhs > m.cap_rhs) {
-        if (m.rmax) cudaFree(m.rmax);
-        if (m.xmax) cudaFree(m.xmax);
-        CHB_CUDA(cudaMalloc(&m.rmax, nrhs * sizeof(unsigned long long)));
-        CHB_CUDA(cudaMalloc(&m.xmax, nrhs * sizeof(unsigned long long)));
+        dev_free(m.rmax);
+        dev_free(m.xmax);
+        m.rmax = (unsigned long long *)dev_alloc(nrhs * sizeof(unsigned long long));
+        m.xmax = (unsigned long long *)dev_alloc(nrhs * sizeof(unsigned long long));
+        if (!m.rmax || !m.xmax) return CHAMELEON_ERR_OUT_OF_RESOURCES;
         m.cap_rhs = nrhs;
     }
+    const size_t diag_bytes = (size_t)((N + NB - 1) / NB) * NB * NB * sizeof(double);
+    if (!grow((void **)&m.diag, &m.diag_cap, diag_bytes)) return CHAMELEON_ERR_OUT_OF_RESOURCES;
     if (N > m.cap_n) {
-        if (m.colsum) cudaFree(m.colsum);
-        CHB_CUDA(cudaMalloc(&m.colsum, N * sizeof(double)));
+        dev_free(m.colsum);
+        if (!(m.colsum = (double *)dev_alloc(N * sizeof(double)))) return CHAMELEON_ERR_OUT_OF_RESOURCES;
         m.cap_n = N;
     }
-    if (!m.flag) CHB_CUDA(cudaMalloc(&m.flag, sizeof(int)));
+    if (!m.flag && !(m.flag = (int *)dev_alloc(sizeof(int)))) return CHAMELEON_ERR_OUT_OF_RESOURCES;
     if (!m.e0) {
         CHB_CUDA(cudaEventCreate(&m.e0));
         CHB_CUDA(cudaEventCreate(&m.e1));
@@ -243,8 +269,9 @@ int mixed_reserve(MixedWs &m, int N, int NB, int nrhs) {
 bool g_res_attr = false;
 }  // namespace
 
-static SymTiles symtiles(CHAM_desc_t *A, cham_uplo_t uplo) {
-    return SymTiles{(double *)A->mat, priv(A)->dev.off, priv(A)->dev.ld, A->nt, A->n, A->nb, uplo == ChamUpper};
+static SymTiles symtiles(CHAM_desc_t *A, cham_uplo_t uplo, double *diag = nullptr) {
+    return SymTiles{(double *)A->mat, priv(A)->dev.off, priv(A)->dev.ld, A->nt, A->n, A->nb, uplo == ChamUpper,
+                    diag};
 }
 
 double sym_norm_inf(CHAM_desc_t *A, cham_uplo_t uplo, cudaStream_t s, MixedWs &m) {
@@ -252,7 +279,10 @@ double sym_norm_inf(CHAM_desc_t *A, cham_uplo_t uplo, cudaStream_t s, MixedWs &m
     const int NT = A->nt;
     cudaMemsetAsync(m.colsum, 0, A->n * sizeof(double), s);
     sym_absnorm_kernel<<<NT * (NT + 1) / 2, 256, 0, s>>>(symtiles(A, uplo), m.colsum);
-    CHB_LAUNCHED(1);
+    // symmetric copies of the diagonal tiles for the residuals of this solve
+    sym_diag_kernel<<<dim3(std::max(1, std::min(64, (A->nb * A->nb + 255) / 256)), NT), 256, 0, s>>>(
+        symtiles(A, uplo, m.diag));
+    CHB_LAUNCHED(2);
     std::vector<double> h(A->n);
     cudaMemcpyAsync(h.data(), m.colsum, A->n * sizeof(double), cudaMemcpyDeviceToHost, s);
     cudaStreamSynchronize(s);
@@ -276,7 +306,7 @@ static int residual(CHAM_desc_t *A, cham_uplo_t uplo, CHAM_desc_t *B, CHAM_desc_
     CHB_CUDA(cudaMemsetAsync(m.rmax, 0, nrhs * sizeof(unsigned long long), s));
     CHB_CUDA(cudaMemsetAsync(m.xmax, 0, nrhs * sizeof(unsigned long long), s));
     sym_residual_kernel<<<A->nt * nrb * ncb, NT_CTA, Cfg12864<double>::SMEM_BYTES, s>>>(
-        symtiles(A, uplo), tmap(X), tmap(B), tmap(m.R), nrhs, nrb, ncb, m.rmax);
+        symtiles(A, uplo, m.diag), tmap(X), tmap(B), tmap(m.R), nrhs, nrb, ncb, m.rmax);
     colmax_kernel<<<ew_grid((int64_t)X->m * nrhs), 256, 0, s>>>(tmap(X), X->m, nrhs, m.xmax);
     CHB_LAUNCHED(2);
     CHB_CUDA(cudaGetLastError());
@@ -350,6 +380,23 @@ struct PhaseClock {
 };
 
 // The refinement driver.  A: FP64 (uplo triangle), B: N x nrhs FP64, X: output.
+void free_mixed_ws(MixedWs &m) {
+    if (m.A32) CHAMELEON_Desc_Destroy(&m.A32);
+    if (m.B32) CHAMELEON_Desc_Destroy(&m.B32);
+    if (m.R) CHAMELEON_Desc_Destroy(&m.R);
+    dev_free(m.a32_buf);
+    dev_free(m.b32_buf);
+    dev_free(m.r_buf);
+    dev_free(m.rmax);
+    dev_free(m.xmax);
+    dev_free(m.colsum);
+    dev_free(m.diag);
+    dev_free(m.flag);
+    if (m.e0) cudaEventDestroy(m.e0);
+    if (m.e1) cudaEventDestroy(m.e1);
+    m = MixedWs();
+}
+
 int mixed_posv_ws(cham_uplo_t uplo, int precision, CHAM_desc_t *A, CHAM_desc_t *B, CHAM_desc_t *X, int *iter_out,
                   CHAM_b200_refine_info_t *info, cudaStream_t s, MixedWs &m, ExecWs *ews, int grid, bool factored) {
     Context &c = ctx();

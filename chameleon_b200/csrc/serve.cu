@@ -49,46 +49,19 @@ double now_s() {
     return ts.tv_sec + 1e-9 * ts.tv_nsec;
 }
 
-void free_mixed_ws(MixedWs &m) {
-    if (m.A32) CHAMELEON_Desc_Destroy(&m.A32);
-    if (m.B32) CHAMELEON_Desc_Destroy(&m.B32);
-    if (m.R) CHAMELEON_Desc_Destroy(&m.R);
-    cudaFree(m.rmax);
-    cudaFree(m.xmax);
-    cudaFree(m.colsum);
-    cudaFree(m.flag);
-    if (m.e0) cudaEventDestroy(m.e0);
-    if (m.e1) cudaEventDestroy(m.e1);
-    m = MixedWs();
-}
-
-void free_exec_ws(ExecWs &w) {
-    cudaFree(w.split);
-    cudaFree(w.ctr);
-    cudaFree(w.inv);
-    cudaFree(w.st);
-    if (w.e0) cudaEventDestroy(w.e0);
-    if (w.e1) cudaEventDestroy(w.e1);
-    w = ExecWs();
-}
-
 // Grow-only device buffer.
 struct DevBuf {
     void *p = nullptr;
     size_t cap = 0;
     int reserve(size_t bytes) {
         if (bytes <= cap) return 0;
-        cudaFree(p);
-        p = nullptr;
+        dev_free(p);
         cap = 0;
-        if (cudaMalloc(&p, bytes) != cudaSuccess) {
-            cudaGetLastError();
-            return CHAMELEON_ERR_OUT_OF_RESOURCES;
-        }
+        if (!(p = dev_alloc(bytes))) return CHAMELEON_ERR_OUT_OF_RESOURCES;
         cap = bytes;
         return 0;
     }
-    ~DevBuf() { cudaFree(p); }
+    ~DevBuf() { dev_free(p); }
 };
 
 // A factor kept on the device for later right-hand sides.
@@ -103,7 +76,7 @@ struct Kept {
     int users = 0;         // requests running on it (guarded by the server mutex)
     std::mutex mu;         // one solve at a time per kept factor
     ~Kept() {
-        cudaFree(A);
+        dev_free(A);
         free_mixed_ws(mws);
         free_exec_ws(ews);
     }
@@ -229,10 +202,7 @@ int solve_large(Server *sv, Slot &sl, CHAM_b200_request_t *r, int *iters) {
         kp->N = N;
         kp->uplo = uplo;
         kp->bytes = kept_bytes(N);
-        if (cudaMalloc(&kp->A, (size_t)N * N * 8) != cudaSuccess) {
-            cudaGetLastError();
-            return CHAMELEON_ERR_OUT_OF_RESOURCES;
-        }
+        if (!(kp->A = (double *)dev_alloc((size_t)N * N * 8))) return CHAMELEON_ERR_OUT_OF_RESOURCES;
     }
     const bool reuse = kp && !r->A;
     int iter = 0, rc = 0;
@@ -268,6 +238,7 @@ int solve_large(Server *sv, Slot &sl, CHAM_b200_request_t *r, int *iters) {
         if (cudaStreamSynchronize(s) != cudaSuccess && !rc) rc = CHAMELEON_ERR_UNEXPECTED;
     }
     *iters = iter;
+    std::shared_ptr<Kept> replaced;   // released after the lock
     std::lock_guard<std::mutex> lk(sv->mu);
     if (reuse) {
         kp->users--;
@@ -276,6 +247,7 @@ int solve_large(Server *sv, Slot &sl, CHAM_b200_request_t *r, int *iters) {
         if (old != sv->kept.end()) {   // replaced; freed when its last user drops it
             sv->used -= old->second->bytes;
             sv->lru.remove(r->factor_key);
+            replaced = old->second;
         }
         sv->kept[r->factor_key] = kp;
         sv->lru.push_back(r->factor_key);
@@ -493,6 +465,9 @@ int CHAM_B200_Serve_Destroy(CHAM_b200_server_t srv) {
     cudaFree(sv->bws.scratch);
     cudaFree(sv->bws.cursor);
     cudaFree(sv->bws.info);
+    sv->bA = DevBuf();
+    sv->bB = DevBuf();
+    sv->binfo = DevBuf();
     cudaStreamDestroy(sv->bs);
     delete sv;
     return 0;

@@ -82,10 +82,15 @@ def test_uneven_batch_dposv(cb, orc, uplo):
     ns, rs, As, Bs = _uneven_batch(orc, 300, 16, 512, 8, 2024)
     a_off = np.cumsum([0] + [n * n for n in ns[:-1]]).astype(np.int64)
     b_off = np.cumsum([0] + [n * r for n, r in zip(ns[:-1], rs[:-1])]).astype(np.int64)
-    A = np.concatenate([a.ravel(order="F") for a in As])
-    B = np.concatenate([b.ravel(order="F") for b in Bs])
     As[17] = As[17].copy(); As[17][5, 5] = -1.0      # one matrix not SPD
-    A[a_off[17]:a_off[17] + ns[17] ** 2] = As[17].ravel(order="F")
+
+    def poisoned(a):   # only the uplo triangle is referenced: NaN elsewhere
+        a = np.array(a, order="F")
+        a[np.tril_indices(a.shape[0], -1) if uplo == 121 else np.triu_indices(a.shape[0], 1)] = np.nan
+        return a
+
+    A = np.concatenate([poisoned(a).ravel(order="F") for a in As])
+    B = np.concatenate([b.ravel(order="F") for b in Bs])
     dev = lambda x, dt=None: torch.from_numpy(np.ascontiguousarray(x)).cuda()
     tA, tB = dev(A), dev(B)
     tn, tr = dev(ns.astype(np.int32)), dev(rs.astype(np.int32))

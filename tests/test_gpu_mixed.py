@@ -123,3 +123,38 @@ def test_dsposv_tile_api(cb, orc):
     assert rc == 0 and it >= 0
     A0 = orc.dplgsy(float(N), N, 51)
     assert np_check_solve(A0, dX.to_numpy(), dB.to_numpy()) < 60
+
+
+def poison_other_triangle(A, uplo):
+    """LAPACK convention: only the `uplo` triangle is referenced.  NaN in the
+    other strict triangle must not reach any result."""
+    P = np.asfortranarray(A.copy())
+    if uplo == 121:
+        P[np.tril_indices(A.shape[0], -1)] = np.nan
+    else:
+        P[np.triu_indices(A.shape[0], 1)] = np.nan
+    return P
+
+
+@pytest.mark.parametrize("prec", [2, 1])
+@pytest.mark.parametrize("uplo", [121, 122])
+@pytest.mark.parametrize("N,NB,nrhs", [(513, 256, 4), (1000, 384, 3), (130, 64, 2)])
+def test_mixed_reads_only_uplo_triangle(cb, orc, prec, uplo, N, NB, nrhs):
+    A0 = orc.dplgsy(float(N), N, 61)
+    B0 = orc.dplrnt(N, nrhs, 62)
+    rc, info, X, Aout = solve_mixed(cb, uplo, prec, poison_other_triangle(A0, uplo), B0, NB)
+    assert rc == 0 and info.iterations >= 0 and info.fallback == 0
+    assert np.isfinite(X).all()
+    assert np_check_solve(A0, X, B0) < 60
+
+
+@pytest.mark.parametrize("uplo", [121, 122])
+def test_dsposv_lapack_reads_only_uplo_triangle(cb, orc, uplo):
+    N, nrhs = 700, 5
+    A0 = orc.dplgsy(float(N), N, 63)
+    B0 = orc.dplrnt(N, nrhs, 64)
+    A = poison_other_triangle(A0, uplo)
+    X = np.zeros((N, nrhs), order="F")
+    rc, it = cb.dsposv(uplo, N, nrhs, A, N, np.asfortranarray(B0.copy()), N, X, N)
+    assert rc == 0 and it >= 0
+    assert np_check_solve(A0, X, B0) < 60

@@ -307,3 +307,22 @@ def test_cuda_lag2(cb, handle):
                                 handle) == 0
     torch.cuda.synchronize()
     assert np.array_equal(_host(dB, (m, n)), A.astype(np.float32).astype(np.float64))
+
+
+@pytest.mark.parametrize("uplo", [121, 122])
+@pytest.mark.parametrize("N,NB", [(700, 256), (1000, 512)])
+def test_fp64_reads_only_uplo_triangle(cb, orc, uplo, N, NB):
+    """LAPACK convention: NaN in the unreferenced strict triangle reaches no result."""
+    nrhs = 3
+    A0 = orc.dplgsy(float(N), N, 71)
+    B0 = orc.dplrnt(N, nrhs, 72)
+    A = np.asfortranarray(A0.copy())
+    if uplo == 121:
+        A[np.tril_indices(N, -1)] = np.nan
+    else:
+        A[np.triu_indices(N, 1)] = np.nan
+    cb.set_param(cb.CHAMELEON_TILE_SIZE, NB)
+    B = np.asfortranarray(B0.copy())
+    assert cb.dposv(uplo, N, nrhs, A, N, B, N) == 0
+    assert np.isfinite(B).all()
+    assert orc.check_solve(A0, B, B0) < 60
