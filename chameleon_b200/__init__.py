@@ -31,6 +31,8 @@ CHAMELEON_B200_REFINE_MAXITER = 102
 CHAMELEON_B200_WAIT_BUDGET_MS = 103
 CHAMELEON_B200_WAIT_BUDGET_US = 104
 CHAMELEON_B200_TCGEN05 = 105
+CHAMELEON_B200_REC_TILE = 106
+CHAMELEON_B200_XINV_SOLVE = 107
 PREC_FP64, PREC_FP32, PREC_BF16X3 = 0, 1, 2
 CHAMELEON_SUCCESS = 0
 CHAMELEON_ERR_NOT_INITIALIZED = -101

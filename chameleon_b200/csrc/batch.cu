@@ -19,6 +19,7 @@
 #include <vector>
 
 #include "core.cuh"
+#include "rec.cuh"
 #include "internal.h"
 
 namespace chb {
@@ -38,7 +39,7 @@ __global__ void __launch_bounds__(NT_CTA, 1) dposv_batch_kernel(const BatchItem 
         if (i >= count) break;
         const BatchItem it = items[i];
         const View T = upper ? View{A + it.a_off, it.lda, 1} : View{A + it.a_off, 1, it.lda};
-        const int r = tile_potrf<double, SPLIT_BF16X3>(T, it.n, invd, smem);
+        const int r = rec::tile_potrf_blk<double, SPLIT_BF16X3>(T, it.n, invd, smem);
         if (threadIdx.x == 0 && info) info[it.info_idx] = r;
         if (r == 0 && it.nrhs > 0) {
             const View X{B + it.b_off, 1, it.ldb};

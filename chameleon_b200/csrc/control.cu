@@ -384,6 +384,12 @@ int CHAMELEON_Set(int param, int value) {
     case CHAMELEON_B200_TCGEN05:
         c.use_tcgen05 = (value != 0);
         return 0;
+    case CHAMELEON_B200_REC_TILE:
+        c.rec_tile = (value != 0);
+        return 0;
+    case CHAMELEON_B200_XINV_SOLVE:
+        c.xinv_solve = (value != 0);
+        return 0;
     case CHAMELEON_TRANSLATION_MODE:
     case CHAMELEON_LOOKAHEAD:
     case CHAMELEON_CONCURRENCY:
@@ -403,6 +409,8 @@ int CHAMELEON_Get(int param, int *value) {
     case CHAMELEON_B200_WAIT_BUDGET_MS: *value = (int)(c.wait_budget_us / 1000); return 0;
     case CHAMELEON_B200_WAIT_BUDGET_US: *value = (int)std::min<long long>(c.wait_budget_us, INT_MAX); return 0;
     case CHAMELEON_B200_TCGEN05: *value = c.use_tcgen05 ? 1 : 0; return 0;
+    case CHAMELEON_B200_REC_TILE: *value = c.rec_tile ? 1 : 0; return 0;
+    case CHAMELEON_B200_XINV_SOLVE: *value = c.xinv_solve ? 1 : 0; return 0;
     }
     return CHAMELEON_ERR_ILLEGAL_VALUE;
 }

@@ -18,6 +18,7 @@
 
 #include "core.cuh"
 #include "internal.h"
+#include "rec.cuh"
 #include "tc05.cuh"
 
 namespace chb {
@@ -44,7 +45,15 @@ struct Dims {
     __device__ ViewT<T> Bt(int m, int bn) const {
         return ViewT<T>{static_cast<T *>(p.B) + p.b_off[m + p.NT * bn], 1, p.b_ld[m]};
     }
-    __device__ T *inv(int k) const { return static_cast<T *>(p.invd) + (int64_t)k * p.NIB * IB * IB; }
+    __device__ T *inv(int k) const {
+        return static_cast<T *>(p.invd) + (p.full_inv ? (int64_t)k * p.NB * p.NB : (int64_t)k * p.NIB * IB * IB);
+    }
+    // Full inverse of diagonal tile k (full_inv mode), lower, ld NB.
+    __device__ ViewT<T> X(int k) const { return ViewT<T>{inv(k), 1, p.NB}; }
+    // Full inverse of diagonal tile k (MODE_XINV), lower, ld NB.
+    __device__ ViewT<T> XI(int k) const {
+        return ViewT<T>{static_cast<T *>(p.xinv) + (int64_t)k * p.NB * p.NB, 1, p.NB};
+    }
 };
 
 // Thread 0 only.  Returns false when the run aborted or the wait ran out.
@@ -81,9 +90,14 @@ __device__ bool task_wait(const Task &t, const ExecParams &p, const Dims<T> &d, 
                wait_geq(&p.updA[t.m + p.NT * t.n], t.k * d.S(t.m, t.n), p, ti);
     case TK_INV:
         return true;
-    case TK_FWD_TRSM:
-        return wait_geq(&p.panA[t.k + p.NT * t.k], 1, p, ti) &&
-               wait_geq(&p.fwdB[t.k + p.NT * t.bn], t.k * d.nbi(t.k), p, ti);
+    case TK_XINV:
+        return !fact || wait_geq(&p.panA[t.k + p.NT * t.k], 1, p, ti);
+    case TK_FWD_TRSM: {
+        bool ok = true;
+        if (!(p.mode & MODE_XINV)) ok = wait_geq(&p.panA[t.k + p.NT * t.k], 1, p, ti);
+        else if (!(p.mode & MODE_NOINV)) ok = wait_geq(&p.xinvDone[t.k], 1, p, ti);
+        return ok && wait_geq(&p.fwdB[t.k + p.NT * t.bn], t.k * d.nbi(t.k), p, ti);
+    }
     case TK_FWD_UPD:
         return wait_geq(&p.fwdDone[t.k + p.NT * t.bn], 1, p, ti) &&
                (!fact || wait_geq(&p.panA[t.m + p.NT * t.k], d.nbi(t.m), p, ti)) &&
@@ -110,7 +124,13 @@ __device__ void run_task(const Task &t, const ExecParams &p, const Dims<T> &d, T
     using VT = ViewT<T>;
     switch (t.kind) {
     case TK_POTRF: {
-        const int info = tile_potrf<T, SP>(d.A(t.k, t.k), d.tm(t.k), d.inv(t.k), smem);
+        int info;
+        if constexpr (std::is_same<T, float>::value) {
+            if (p.full_inv) info = rec::tile_potrf_inv<T, SP>(d.A(t.k, t.k), d.X(t.k), d.tm(t.k), smem);
+            else info = rec::tile_potrf_blk<T, SP>(d.A(t.k, t.k), d.tm(t.k), d.inv(t.k), smem);
+        } else {
+            info = rec::tile_potrf_blk<T, SP>(d.A(t.k, t.k), d.tm(t.k), d.inv(t.k), smem);
+        }
         if (info && threadIdx.x == 0) {
             atomicMin(&p.st->info, t.k * p.NB + info);
             atomicExch(&p.st->abort, 1);
@@ -118,21 +138,37 @@ __device__ void run_task(const Task &t, const ExecParams &p, const Dims<T> &d, T
         break;
     }
     case TK_INV:
-        tile_inv<T>(d.A(t.k, t.k), d.tm(t.k), d.inv(t.k), smem);
+        if constexpr (std::is_same<T, float>::value) {
+            if (p.full_inv) {
+                rec::tile_trtri<T, SP>(d.A(t.k, t.k), d.X(t.k), d.tm(t.k), smem);
+                break;
+            }
+        }
+        rec::tile_inv_blk<T>(d.A(t.k, t.k), d.tm(t.k), d.inv(t.k), smem);
         break;
     case TK_TRSM: {
         const int r0 = t.sub * SUBB;
         const int rows = min(SUBB, d.tm(t.m) - r0);
-        trsm_rows<T, SP>(d.A(t.m, t.k).sub(r0, 0), rows, d.A(t.k, t.k), d.tm(t.k), d.inv(t.k), smem);
+        bool done = false;
+        if constexpr (std::is_same<T, float>::value) {
+            if (p.full_inv) {
+                rec::apply_inv_right<T, SP>(d.A(t.m, t.k).sub(r0, 0), rows, d.X(t.k), d.tm(t.k), smem);
+                done = true;
+            }
+        }
+        if (!done) trsm_rows<T, SP>(d.A(t.m, t.k).sub(r0, 0), rows, d.A(t.k, t.k), d.tm(t.k), d.inv(t.k), smem);
         if constexpr (TC) {
             // emit the split-BF16 chunks of these 128 rows for the tcgen05 updates
             const VT X = d.A(t.m, t.k).sub(r0, 0);
             const int K = d.tm(t.k);
             uint8_t *base = split_tile(p, t.m, t.k) + (size_t)t.sub * p.split_nkc * 2 * tc05::CHUNK_BYTES;
-            for (int idx = threadIdx.x; idx < 128 * K; idx += NT_CTA) {
-                const int r = idx % 128, c = idx / 128;
-                const float v = (r < rows) ? (float)*X.at(r, c) : 0.f;
-                tc05::split_store(base + (size_t)(c / tc05::BK) * 2 * tc05::CHUNK_BYTES, r, c % tc05::BK, v);
+            // one thread per (row, group of 8 columns): 16-byte stores
+            for (int idx = threadIdx.x; idx < 16 * K; idx += NT_CTA) {
+                const int r = idx % 128, c0 = (idx / 128) * 8;
+                float v[8];
+#pragma unroll
+                for (int e = 0; e < 8; ++e) v[e] = (r < rows) ? (float)*X.at(r, c0 + e) : 0.f;
+                tc05::split_store8(base + (size_t)(c0 / tc05::BK) * 2 * tc05::CHUNK_BYTES, r, c0 % tc05::BK, v);
             }
             tc05::fence_proxy_async();
             cta_sync_global();
@@ -176,10 +212,21 @@ __device__ void run_task(const Task &t, const ExecParams &p, const Dims<T> &d, T
         acc.sub_from(C, rows, cols, diag);
         break;
     }
+    case TK_XINV:
+        if constexpr (std::is_same<T, float>::value) rec::tile_trtri<T, SP>(d.A(t.k, t.k), d.XI(t.k), d.tm(t.k), smem);
+        break;
     case TK_FWD_TRSM:
     case TK_BWD_TRSM: {
         const VT X = d.Bt(t.k, t.bn);
         const int w = d.wB(t.bn);
+        if constexpr (std::is_same<T, float>::value) {
+            if (p.full_inv || (p.mode & MODE_XINV)) {
+                const VT Xk = p.full_inv ? d.X(t.k) : d.XI(t.k);
+                if (t.kind == TK_FWD_TRSM) rec::apply_inv_left<T, SP, false>(X, w, Xk, d.tm(t.k), smem);
+                else rec::apply_inv_left<T, SP, true>(X, w, Xk, d.tm(t.k), smem);
+                break;
+            }
+        }
         for (int c0 = 0; c0 < w; c0 += IB)
             trsm_left<T, SP>(X.sub(0, c0), min(IB, w - c0), d.A(t.k, t.k), d.tm(t.k), d.inv(t.k),
                       t.kind == TK_BWD_TRSM, smem);
@@ -209,6 +256,7 @@ __device__ int *task_counter(const Task &t, const ExecParams &p) {
     switch (t.kind) {
     case TK_POTRF:
     case TK_INV: return &p.panA[t.k + p.NT * t.k];
+    case TK_XINV: return &p.xinvDone[t.k];
     case TK_TRSM: return &p.panA[t.m + p.NT * t.k];
     case TK_UPD: return &p.updA[t.m + p.NT * t.n];
     case TK_FWD_TRSM: return &p.fwdDone[t.k + p.NT * t.bn];
@@ -334,7 +382,8 @@ std::vector<Task> build_order(const Shape &s) {
         ct[b].npred++;
     };
     // ids: potrf[k], trsm[m,k], upd[m,n,k] (last update of tile (m,n) so far)
-    std::vector<int> P(NT, -1), Tr((size_t)NT * NT, -1), lastU((size_t)NT * NT, -1);
+    std::vector<int> P(NT, -1), XI(NT, -1), Tr((size_t)NT * NT, -1), lastU((size_t)NT * NT, -1);
+    const bool xinv = s.mode & MODE_XINV;
     const double nb = s.NB;
     const Calib &cal = kCalib[(s.prof >= 0 && s.prof < 3) ? s.prof : 0];
     if (fact) {
@@ -342,6 +391,10 @@ std::vector<Task> build_order(const Shape &s) {
             const double tk = tm(k);
             P[k] = add(TK_POTRF, k, k, k, 0, 1, cal.potrf * 6.0 * tk * tk * tk / 3.0);
             edge(lastU[k + (size_t)NT * k], P[k]);
+            if (xinv && solve) {
+                XI[k] = add(TK_XINV, k, k, k, 0, 1, cal.potrf * 6.0 * tk * tk * tk / 3.0);
+                edge(P[k], XI[k]);
+            }
             for (int m = k + 1; m < NT; ++m) {
                 const int id = add(TK_TRSM, m, k, k, 0, nbi(m), cal.trsm * 2.0 * SUBB * nb * nb);
                 edge(P[k], id);
@@ -359,8 +412,11 @@ std::vector<Task> build_order(const Shape &s) {
                 }
             }
         }
-    } else if (solve) {
-        for (int k = 0; k < NT; ++k) P[k] = add(TK_INV, k, k, k, 0, 1, 1.0 * tm(k) * IB * IB);
+    } else if (solve && !(s.mode & MODE_NOINV)) {
+        for (int k = 0; k < NT; ++k) {
+            if (xinv) XI[k] = add(TK_XINV, k, k, k, 0, 1, cal.potrf * 6.0 * tm(k) * tm(k) * tm(k) / 3.0);
+            else P[k] = add(TK_INV, k, k, k, 0, 1, 1.0 * tm(k) * IB * IB);
+        }
     }
     if (solve) {
         std::vector<int> F((size_t)NT * NTB, -1), lastFU((size_t)NT * NTB, -1);
@@ -369,7 +425,7 @@ std::vector<Task> build_order(const Shape &s) {
             const double w = wB(bn);
             for (int k = 0; k < NT; ++k) {
                 const int f = add(TK_FWD_TRSM, k, k, k, bn, 1, cal.strsm * 3.0 * tm(k) * tm(k) * w);
-                edge(P[k], f);
+                edge(xinv ? XI[k] : P[k], f);
                 edge(lastFU[k + (size_t)NT * bn], f);
                 F[k + (size_t)NT * bn] = f;
                 for (int m = k + 1; m < NT; ++m) {
@@ -531,6 +587,7 @@ static int set_dag_smem() {
 }
 
 void free_exec_ws(ExecWs &w) {
+    dev_free(w.xinv);
     dev_free(w.split);
     dev_free(w.ctr);
     dev_free(w.inv);
@@ -541,7 +598,7 @@ void free_exec_ws(ExecWs &w) {
 }
 
 int run_cholesky_dag(int mode, cham_uplo_t uplo, CHAM_desc_t *A, CHAM_desc_t *B, cudaStream_t s,
-                     ExecResult *res, int split, ExecWs *wsp, int grid_req) {
+                     ExecResult *res, int split, ExecWs *wsp, int grid_req, int flags) {
     Context &c = ctx();
     ExecWs &w = wsp ? *wsp : g_ws;
     const int N = A->n;
@@ -566,6 +623,18 @@ int run_cholesky_dag(int mode, cham_uplo_t uplo, CHAM_desc_t *A, CHAM_desc_t *B,
     if (rc) return rc;
     const int grid = (grid_req > 0) ? std::min(grid_req, c.num_sms) : c.num_sms;
     const int prof = !f32 ? PROF_FP64 : (tc ? PROF_F32_TC05 : PROF_F32_MMA);
+    const bool full_inv = f32 && c.rec_tile && NB <= (64 << rec::MAX_LVL);
+    // FP32 substitutions with full diagonal-tile inverses: computed off the
+    // critical path in a factor+solve launch, reused by later solve-only
+    // launches on the same factor and workspace (flags & EXEC_REUSE_INV).
+    const bool xinv = f32 && !full_inv && c.xinv_solve && (mode & MODE_SOLVE) && nrhs > 0 &&
+                      NB <= (64 << rec::MAX_LVL);
+    if (xinv) {
+        mode |= MODE_XINV;
+        if (!(mode & MODE_FACT) && (flags & EXEC_REUSE_INV) && w.xinv_owner == A->mat && w.xinv_nt == NT &&
+            w.xinv_nb == NB && w.xinv_n == N)
+            mode |= MODE_NOINV;
+    }
     // The task list depends on N only through NT and the number of SUBB-row
     // blocks of the last tile row, and on nrhs only through NTB (the kernel
     // takes the exact sizes from the parameters): key the cache on that
@@ -576,9 +645,10 @@ int run_cholesky_dag(int mode, cham_uplo_t uplo, CHAM_desc_t *A, CHAM_desc_t *B,
     Schedule *sch = get_schedule(sh);
     if (!sch) return CHAMELEON_ERR_OUT_OF_RESOURCES;
     const int NIB = (NB + IB - 1) / IB;
-    const size_t nctr = (size_t)2 * NT * NT + (size_t)4 * NT * std::max(NTB, 1);
+    const size_t nctr = (size_t)2 * NT * NT + (size_t)4 * NT * std::max(NTB, 1) + NT;
     const size_t esz = f32 ? sizeof(float) : sizeof(double);
-    rc = ensure_ws(w, nctr * sizeof(int), (size_t)NT * NIB * IB * IB * esz);
+    const size_t inv_elems = full_inv ? (size_t)NT * NB * NB : (size_t)NT * NIB * IB * IB;
+    rc = ensure_ws(w, nctr * sizeof(int), inv_elems * esz);
     if (rc) return rc;
     int rcA = desc_upload(A);
     if (rcA) return rcA;
@@ -609,6 +679,21 @@ int run_cholesky_dag(int mode, cham_uplo_t uplo, CHAM_desc_t *A, CHAM_desc_t *B,
     p.bwdDone = p.bwdB + nb4;
     p.invd = w.inv;
     p.NIB = NIB;
+    p.full_inv = full_inv ? 1 : 0;
+    p.xinvDone = p.bwdDone + nb4;
+    p.xinv = nullptr;
+    if (xinv) {
+        const size_t xbytes = (size_t)NT * NB * NB * sizeof(float);
+        if (xbytes > w.xinv_bytes) {
+            dev_free(w.xinv);
+            w.xinv_bytes = 0;
+            w.xinv_owner = nullptr;
+            if (!(w.xinv = dev_alloc(xbytes))) return CHAMELEON_ERR_OUT_OF_RESOURCES;
+            w.xinv_bytes = xbytes;
+        }
+        p.xinv = w.xinv;
+        if (!(mode & MODE_NOINV)) w.xinv_owner = nullptr;   // rewritten by this launch
+    }
     p.st = w.st;
     p.trace = (g_trace_buf && g_trace_cap >= p.ntasks) ? g_trace_buf : nullptr;
     p.wait_budget_ns = (unsigned long long)c.wait_budget_us * 1000ull;
@@ -654,6 +739,12 @@ int run_cholesky_dag(int mode, cham_uplo_t uplo, CHAM_desc_t *A, CHAM_desc_t *B,
     CHB_CUDA(cudaEventElapsedTime(&res->ms, w.e0, w.e1));
     res->info = (out.info == INT_MAX) ? 0 : out.info;
     res->error = out.error;
+    if (xinv && !(mode & MODE_NOINV) && res->info == 0 && res->error == 0) {
+        w.xinv_owner = A->mat;   // the inverses now match this factor
+        w.xinv_n = N;
+        w.xinv_nt = NT;
+        w.xinv_nb = NB;
+    }
     if (out.error) {
         char msg[160];
         snprintf(msg, sizeof msg, "device wait budget exhausted at task %d (%d of %d done)",

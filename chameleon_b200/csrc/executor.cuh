@@ -23,6 +23,7 @@ enum TaskKind : int16_t {
     TK_BWD_TRSM = 6,  // B(k) <- L(k,k)^{-T} B(k)
     TK_BWD_UPD = 7,   // B(m) -= L(k,m)^T B(k)          (m < k)
     TK_INV = 8,       // invert inner diagonal blocks of an existing factor (potrs alone)
+    TK_XINV = 9,      // full inverse of diagonal tile k (FP32 substitution steps)
 };
 
 struct Task {
@@ -32,7 +33,10 @@ struct Task {
 };
 static_assert(sizeof(Task) == 16, "Task is 16 bytes");
 
-enum ExecMode : int { MODE_FACT = 1, MODE_SOLVE = 2 };
+// MODE_XINV: the substitution steps apply full inverses of the diagonal tiles
+// (one GEMM per tile), computed by TK_XINV tasks; with MODE_NOINV (solve only)
+// the inverses are already in place from an earlier launch on the same factor.
+enum ExecMode : int { MODE_FACT = 1, MODE_SOLVE = 2, MODE_XINV = 4, MODE_NOINV = 8 };
 
 constexpr int SUBB = 128;      // sub-block edge of trailing updates / row blocks
 
@@ -65,8 +69,12 @@ struct ExecParams {
     const int64_t *b_off;   // b_off[m + NT*bn]
     const int *b_ld;
     int *updA, *panA, *fwdB, *fwdDone, *bwdB, *bwdDone;
-    void *invd;             // NT * NIB inverted IB x IB blocks (element type of A)
+    void *invd;             // full_inv: NT inverted NB x NB diagonal tiles (ld NB);
+                            // else NT * NIB inverted IB x IB blocks (element type of A)
     int NIB;
+    int full_inv;           // FP32 path: recursive tile factorization with full tile inverses
+    void *xinv;             // MODE_XINV: NT full inverses of the diagonal tiles (ld NB)
+    int *xinvDone;          // MODE_XINV: TK_XINV(k) done
     ExecState *st;
     TraceRec *trace;        // optional per-task trace (nullptr: off)
     // tcgen05 trailing update of the FP32 factorization (split-BF16 operands):

@@ -29,6 +29,8 @@ struct Context {
     int refine_maxiter = 30;
     long long wait_budget_us = 20000000;
     bool use_tcgen05 = true;      // tcgen05 trailing updates in the BF16x3 factorization
+    bool rec_tile = false;        // FP32 factorization: recursive tile POTRF with full tile inverses
+    bool xinv_solve = true;       // FP32 substitutions with full diagonal-tile inverses
     int desc_ids = 0;
     std::mutex mu;
 };
@@ -102,6 +104,10 @@ int stage_out(double *host, int ld, const double *dev, int rows, int cols, cudaS
 struct ExecWs {
     uint8_t *split = nullptr;
     size_t split_bytes = 0;
+    void *xinv = nullptr;               // full inverses of the diagonal tiles (FP32 solves)
+    size_t xinv_bytes = 0;
+    const void *xinv_owner = nullptr;   // factor storage the inverses belong to (nullptr: none)
+    int xinv_n = 0, xinv_nt = 0, xinv_nb = 0;
     size_t ctr_bytes = 0, inv_bytes = 0;
     void *ctr = nullptr;
     void *inv = nullptr;
@@ -162,8 +168,11 @@ struct ExecResult {
 // path, `split` = SPLIT_BF16X3 or SPLIT_TF32X3 from core.cuh).
 // ws: workspace (nullptr: the global one of the synchronous API); grid:
 // number of persistent CTAs (0: one per SM).
+// flags: EXEC_REUSE_INV -- a solve-only launch may reuse the full diagonal-tile
+// inverses a previous launch on the same workspace computed for this factor.
+enum ExecFlags : int { EXEC_REUSE_INV = 1 };
 int run_cholesky_dag(int mode, cham_uplo_t uplo, CHAM_desc_t *A, CHAM_desc_t *B, cudaStream_t s,
-                     ExecResult *res, int split = 0, ExecWs *ws = nullptr, int grid = 0);
+                     ExecResult *res, int split = 0, ExecWs *ws = nullptr, int grid = 0, int flags = 0);
 
 // Mixed-precision solve on an explicit stream and workspaces (mixed.cu).
 // factored = true: m.A32 already holds the low-precision factor of A (resident

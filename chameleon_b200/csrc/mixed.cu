@@ -430,7 +430,9 @@ int mixed_posv_ws(cham_uplo_t uplo, int precision, CHAM_desc_t *A, CHAM_desc_t *
             fallback = true;
         }
         if (!fallback) {
-            if ((rc = run_cholesky_dag(factored ? MODE_SOLVE : (MODE_FACT | MODE_SOLVE), uplo, m.A32, m.B32, s, &res, split, ews, grid))) return rc;
+            if ((rc = run_cholesky_dag(factored ? MODE_SOLVE : (MODE_FACT | MODE_SOLVE), uplo, m.A32, m.B32, s, &res,
+                                       split, ews, grid, EXEC_REUSE_INV)))
+                return rc;
             st.factor_ms += res.ms;
             if (res.error) return res.error;
             if (res.info) {
@@ -449,7 +451,8 @@ int mixed_posv_ws(cham_uplo_t uplo, int precision, CHAM_desc_t *A, CHAM_desc_t *
             while (!ok && it < c.refine_maxiter) {
                 ++it;
                 if ((rc = cast_desc(m.R, m.B32, s, nullptr))) return rc;
-                if ((rc = run_cholesky_dag(MODE_SOLVE, uplo, m.A32, m.B32, s, &res, split, ews, grid))) return rc;
+                if ((rc = run_cholesky_dag(MODE_SOLVE, uplo, m.A32, m.B32, s, &res, split, ews, grid, EXEC_REUSE_INV)))
+                    return rc;
                 st.refine_solve_ms += res.ms;
                 if (res.error) return res.error;
                 if (!uploaded(X) || !uploaded(m.B32)) return CHAMELEON_ERR_UNEXPECTED;

@@ -189,6 +189,20 @@ __device__ __forceinline__ void split_store(uint8_t *chunk, int r, int c, float 
     *reinterpret_cast<__nv_bfloat16 *>(chunk + CHUNK_BYTES + off) = l;
 }
 
+// Eight consecutive elements (r, c0 .. c0+7), c0 % 8 == 0, of one row: the
+// same hi / lo values as eight split_store calls, written as one 16-byte
+// group into each half.
+__device__ __forceinline__ void split_store8(uint8_t *chunk, int r, int c0, const float (&v)[8]) {
+    uint4 hi, lo;
+    split_bf16(v[0], v[1], hi.x, lo.x);
+    split_bf16(v[2], v[3], hi.y, lo.y);
+    split_bf16(v[4], v[5], hi.z, lo.z);
+    split_bf16(v[6], v[7], hi.w, lo.w);
+    const int off = swz_off(r, c0);
+    *reinterpret_cast<uint4 *>(chunk + off) = hi;
+    *reinterpret_cast<uint4 *>(chunk + CHUNK_BYTES + off) = lo;
+}
+
 // acc = A * B^T over nkc chunks, A chunks at a_chunks[kc], B at b_chunks[kc]
 // (each chunk = hi 16 KB + lo 16 KB, consecutive chunks 32 KB apart), then
 // f(row, col0, v[16]) for accumulator row `row`, columns col0..col0+15, by the

@@ -11,6 +11,7 @@
 #include <algorithm>
 
 #include "core.cuh"
+#include "rec.cuh"
 #include "gen.cuh"
 #include "internal.h"
 
@@ -91,7 +92,7 @@ __global__ void __launch_bounds__(NT_CTA, 1) trsm_kernel(View L, int n, const do
 
 __global__ void __launch_bounds__(NT_CTA, 1) potrf_kernel(View T, int n, double *invd, int *info) {
     extern __shared__ __align__(128) double smem[];
-    const int r = tile_potrf<double, SPLIT_BF16X3>(T, n, invd, smem);
+    const int r = rec::tile_potrf_blk<double, SPLIT_BF16X3>(T, n, invd, smem);
     if (threadIdx.x == 0 && info) *info = r;
 }
 

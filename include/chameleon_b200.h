@@ -63,6 +63,10 @@ typedef enum {
 #define CHAMELEON_B200_WAIT_BUDGET_MS 103 /* bound on any device-side dependency wait     */
 #define CHAMELEON_B200_WAIT_BUDGET_US 104 /* the same bound in microseconds              */
 #define CHAMELEON_B200_TCGEN05        105 /* 1: tcgen05 trailing updates in BF16x3 (default) */
+#define CHAMELEON_B200_REC_TILE       106 /* 1: FP32 factorization with recursive diagonal tiles
+                                             and full tile inverses; 0: blocked (default) */
+#define CHAMELEON_B200_XINV_SOLVE     107 /* 1: FP32 substitutions apply full inverses of the
+                                             diagonal tiles, kept across refinement solves (default) */
 
 /* Factorization precisions for CHAMELEON_B200_PRECISION */
 #define CHAM_B200_PREC_FP64   0

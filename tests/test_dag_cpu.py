@@ -12,9 +12,9 @@ import numpy as np
 import pytest
 import scipy.linalg as sla
 
-TK_POTRF, TK_TRSM, TK_UPD, TK_FWD_TRSM, TK_FWD_UPD, TK_BWD_TRSM, TK_BWD_UPD, TK_INV = range(1, 9)
+TK_POTRF, TK_TRSM, TK_UPD, TK_FWD_TRSM, TK_FWD_UPD, TK_BWD_TRSM, TK_BWD_UPD, TK_INV, TK_XINV = range(1, 10)
 SUBB = 128
-FACT, SOLVE = 1, 2
+FACT, SOLVE, XINV, NOINV = 1, 2, 4, 8
 
 
 def geometry(N, NB, nrhs, NBB):
@@ -31,18 +31,25 @@ def check_waits(tasks, mode, N, NB, nrhs, NBB):
     upd = np.zeros((NT, NT), int); pan = np.zeros((NT, NT), int)
     fwdB = np.zeros((NT, max(NTB, 1)), int); fwdD = np.zeros_like(fwdB)
     bwdB = np.zeros_like(fwdB); bwdD = np.zeros_like(fwdB)
+    xinv = np.zeros(NT, int)
     fact = bool(mode & FACT)
     for kind, sub, m, n, k, bn in tasks:
         if kind == TK_POTRF:
             ok = upd[k, k] >= k * S(k, k); pan[k, k] += 1
         elif kind == TK_INV:
             ok = True; pan[k, k] += 1
+        elif kind == TK_XINV:
+            ok = (not fact) or pan[k, k] >= 1; xinv[k] += 1
         elif kind == TK_TRSM:
             ok = pan[k, k] >= 1 and upd[m, k] >= k * S(m, k); pan[m, k] += 1
         elif kind == TK_UPD:
             ok = pan[m, k] >= nbi(m) and pan[n, k] >= nbi(n) and upd[m, n] >= k * S(m, n); upd[m, n] += 1
         elif kind == TK_FWD_TRSM:
-            ok = pan[k, k] >= 1 and fwdB[k, bn] >= k * nbi(k); fwdD[k, bn] += 1
+            if mode & XINV:
+                inv_ok = bool(mode & NOINV) or xinv[k] >= 1
+            else:
+                inv_ok = pan[k, k] >= 1
+            ok = inv_ok and fwdB[k, bn] >= k * nbi(k); fwdD[k, bn] += 1
         elif kind == TK_FWD_UPD:
             ok = fwdD[k, bn] >= 1 and (not fact or pan[m, k] >= nbi(m)) and fwdB[m, bn] >= k * nbi(m)
             fwdB[m, bn] += 1
@@ -60,6 +67,10 @@ def check_waits(tasks, mode, N, NB, nrhs, NBB):
                 assert upd[m, n] == n * S(m, n)
     if mode & SOLVE:
         assert (fwdD[:, :NTB] == 1).all() and (bwdD[:, :NTB] == 1).all()
+    if (mode & XINV) and (mode & SOLVE) and not (mode & NOINV):
+        assert (xinv == 1).all()
+    else:
+        assert (xinv == 0).all()
 
 
 def emulate(tasks, A, B, uplo, N, NB, NBB):
@@ -83,6 +94,8 @@ def emulate(tasks, A, B, uplo, N, NB, NBB):
             if m == n and bi == bj:
                 upd = np.tril(upd)
             C -= upd
+        elif kind in (TK_INV, TK_XINV):
+            pass   # inverses of diagonal tiles: the emulation solves triangular systems directly
         elif kind == TK_FWD_TRSM:
             X = Bt(k, bn); X[:] = sla.solve_triangular(np.tril(L(k, k)), X, lower=True)
         elif kind == TK_BWD_TRSM:
@@ -104,6 +117,20 @@ def test_schedule_is_deadlock_free(cb_host, N, NB, nrhs, NBB, workers, prof):
     for mode in (FACT, SOLVE, FACT | SOLVE):
         t = cb_host.schedule(mode, N, NB, nrhs if mode & SOLVE else 0, NBB, workers, prof)
         check_waits(t, mode, N, NB, nrhs if mode & SOLVE else 0, NBB)
+
+
+@pytest.mark.parametrize("N,NB,nrhs,NBB", SHAPES)
+@pytest.mark.parametrize("workers", [1, 148])
+def test_schedule_with_full_tile_inverses_is_deadlock_free(cb_host, N, NB, nrhs, NBB, workers):
+    """FP32 substitutions with full diagonal-tile inverses: TK_XINV after each
+    POTRF in a factor+solve launch, instead of TK_INV in a solve launch, and no
+    inversion task at all when the inverses are reused (NOINV)."""
+    for mode in (FACT | SOLVE | XINV, SOLVE | XINV, SOLVE | XINV | NOINV):
+        t = cb_host.schedule(mode, N, NB, nrhs, NBB, workers, 2)
+        check_waits(t, mode, N, NB, nrhs, NBB)
+        kinds = set(int(x) for x in t[:, 0])
+        assert (TK_XINV in kinds) == (not mode & NOINV)
+        assert TK_INV not in kinds
 
 
 @pytest.mark.parametrize("uplo", [121, 122])

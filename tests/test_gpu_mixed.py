@@ -158,3 +158,48 @@ def test_dsposv_lapack_reads_only_uplo_triangle(cb, orc, uplo):
     rc, it = cb.dsposv(uplo, N, nrhs, A, N, np.asfortranarray(B0.copy()), N, X, N)
     assert rc == 0 and it >= 0
     assert np_check_solve(A0, X, B0) < 60
+
+
+@pytest.mark.parametrize("rec", [1, 0])
+@pytest.mark.parametrize("uplo", [121, 122])
+@pytest.mark.parametrize("N,NB,nrhs", [(1000, 512, 3), (777, 384, 5), (2048, 320, 2), (37, 17, 1), (1500, 1000, 2),
+                                       (130, 64, 3), (600, 1100, 1)])
+def test_recursive_tile_path_matches_blocked(cb, orc, rec, uplo, N, NB, nrhs):
+    """FP32 factorization with recursive diagonal tiles + full tile inverses
+    (CHAMELEON_B200_REC_TILE=1, tiles up to 1024) and the blocked one (=0,
+    default) both refine to FP64 accuracy in a few iterations on dplgsy
+    matrices."""
+    A0 = orc.dplgsy(float(N), N, 81)
+    B0 = orc.dplrnt(N, nrhs, 82)
+    old = cb.get_param(cb.CHAMELEON_B200_REC_TILE)
+    assert cb.lib().CHAMELEON_Set(cb.CHAMELEON_B200_REC_TILE, rec) == 0
+    try:
+        for prec in (2, 1):
+            rc, info, X, _ = solve_mixed(cb, uplo, prec, A0, B0, NB)
+            assert rc == 0 and info.fallback == 0 and 0 <= info.iterations <= 5, (prec, info.iterations)
+            assert np_check_solve(A0, X, B0) < 60
+    finally:
+        cb.lib().CHAMELEON_Set(cb.CHAMELEON_B200_REC_TILE, old)
+
+
+def test_recursive_tile_not_spd_reports_info(cb):
+    """A non-positive pivot inside the recursion (second leaf of the second
+    half) is reported with the same LAPACK order as the blocked path."""
+    N, NB = 512, 512
+    A0 = np.eye(N) * 4.0
+    A0[300, 300] = -1.0
+    B0 = np.ones((N, 1))
+    import ctypes
+    old = cb.get_param(cb.CHAMELEON_B200_REC_TILE)
+    for rec in (1, 0):
+        assert cb.lib().CHAMELEON_Set(cb.CHAMELEON_B200_REC_TILE, rec) == 0
+        rc, info, X, _ = solve_mixed(cb, 122, 2, np.asfortranarray(A0), np.asfortranarray(B0), NB)
+        assert rc == 301, (rec, rc)
+        # the FP32 factorization alone reports the same order
+        dA = cb.Desc.create(N, N, NB)
+        dB = cb.Desc.create(N, 1, NB)
+        dA.from_numpy(np.asfortranarray(A0))
+        dB.from_numpy(np.asfortranarray(B0))
+        ms = ctypes.c_float()
+        assert cb.lib().CHAM_B200_Mixed_Factor_Only(122, 2, dA.ptr, dB.ptr, ctypes.byref(ms)) == 301
+    cb.lib().CHAMELEON_Set(cb.CHAMELEON_B200_REC_TILE, old)
