@@ -136,7 +136,9 @@ std::vector<Task> build_order(const Shape &s) {
         for (int bn = 0; bn < NTB; ++bn) {
             const double w = wB(bn);
             for (int k = 0; k < NT; ++k) {
-                const int f = add(TK_FWD_TRSM, k, k, k, bn, 1, cal.strsm * 3.0 * tm(k) * tm(k) * w);
+                // MODE_XINV: one sub-task per row block (each applies its rows of the inverse)
+                const int f = add(TK_FWD_TRSM, k, k, k, bn, xinv ? nbi(k) : 1,
+                                  cal.strsm * 3.0 * tm(k) * tm(k) * w / (xinv ? nbi(k) : 1));
                 edge(xinv ? XI[k] : P[k], f);
                 edge(lastFU[k + (size_t)NT * bn], f);
                 F[k + (size_t)NT * bn] = f;
@@ -149,7 +151,8 @@ std::vector<Task> build_order(const Shape &s) {
                 }
             }
             for (int k = NT - 1; k >= 0; --k) {
-                const int b = add(TK_BWD_TRSM, k, k, k, bn, 1, cal.strsm * 3.0 * tm(k) * tm(k) * w);
+                const int b = add(TK_BWD_TRSM, k, k, k, bn, xinv ? nbi(k) : 1,
+                                  cal.strsm * 3.0 * tm(k) * tm(k) * w / (xinv ? nbi(k) : 1));
                 edge(F[k + (size_t)NT * bn], b);
                 edge(lastBU[k + (size_t)NT * bn], b);
                 Bk[k + (size_t)NT * bn] = b;
@@ -205,8 +208,9 @@ std::vector<Task> build_order(const Shape &s) {
             }
             (void)a;
             t.sub = (int16_t)(bi | (bj << 8));
-        } else if (c.kind == TK_TRSM || c.kind == TK_FWD_UPD || c.kind == TK_BWD_UPD) {
-            t.sub = (int16_t)j;
+        } else if (c.kind == TK_TRSM || c.kind == TK_FWD_UPD || c.kind == TK_BWD_UPD || c.kind == TK_FWD_TRSM ||
+                   c.kind == TK_BWD_TRSM) {
+            t.sub = (int16_t)j;   // row block (the substitutions have one unless MODE_XINV)
         }
         out.push_back(t);
     };
@@ -290,6 +294,7 @@ int launch_dag_tf32(const ExecParams &p, int grid, cudaStream_t s);
 
 void free_exec_ws(ExecWs &w) {
     dev_free(w.xinv);
+    dev_free(w.y);
     dev_free(w.split);
     dev_free(w.ctr);
     dev_free(w.inv);
@@ -390,6 +395,15 @@ int run_cholesky_dag(int mode, cham_uplo_t uplo, CHAM_desc_t *A, CHAM_desc_t *B,
         }
         p.xinv = w.xinv;
         if (!(mode & MODE_NOINV)) w.xinv_owner = nullptr;   // rewritten by this launch
+        // forward-substitution results, same tile layout as B
+        const size_t ybytes = (size_t)(priv(B)->cm_view ? B->lda : B->lm) * B->ln * sizeof(float);
+        if (ybytes > w.y_bytes) {
+            dev_free(w.y);
+            w.y_bytes = 0;
+            if (!(w.y = dev_alloc(ybytes))) return CHAMELEON_ERR_OUT_OF_RESOURCES;
+            w.y_bytes = ybytes;
+        }
+        p.Y = w.y;
     }
     p.st = w.st;
     p.trace = (g_trace_buf && g_trace_cap >= p.ntasks) ? g_trace_buf : nullptr;

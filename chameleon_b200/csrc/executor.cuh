@@ -74,6 +74,8 @@ struct ExecParams {
     int NIB;
     int full_inv;           // FP32 path: recursive tile factorization with full tile inverses
     void *xinv;             // MODE_XINV: NT full inverses of the diagonal tiles (ld NB)
+    void *Y;                // MODE_XINV: forward results (layout of B): the substitutions
+                            // read B and write Y (forward), read Y and write B (backward)
     int *xinvDone;          // MODE_XINV: TK_XINV(k) done
     ExecState *st;
     TraceRec *trace;        // optional per-task trace (nullptr: off)

@@ -37,6 +37,12 @@ struct Dims {
     __device__ ViewT<T> Bt(int m, int bn) const {
         return ViewT<T>{static_cast<T *>(p.B) + p.b_off[m + p.NT * bn], 1, p.b_ld[m]};
     }
+    // Tile (m, bn) of the forward results (MODE_XINV), layout of B.
+    __device__ ViewT<T> Yt(int m, int bn) const {
+        return ViewT<T>{static_cast<T *>(p.Y) + p.b_off[m + p.NT * bn], 1, p.b_ld[m]};
+    }
+    // Sub-tasks a substitution of tile k is split into (its row blocks, MODE_XINV).
+    __device__ int nsolve(int k) const { return (p.mode & MODE_XINV) ? nbi(k) : 1; }
     __device__ T *inv(int k) const {
         return static_cast<T *>(p.invd) + (p.full_inv ? (int64_t)k * p.NB * p.NB : (int64_t)k * p.NIB * IB * IB);
     }
@@ -91,14 +97,14 @@ __device__ bool task_wait(const Task &t, const ExecParams &p, const Dims<T> &d, 
         return ok && wait_geq(&p.fwdB[t.k + p.NT * t.bn], t.k * d.nbi(t.k), p, ti);
     }
     case TK_FWD_UPD:
-        return wait_geq(&p.fwdDone[t.k + p.NT * t.bn], 1, p, ti) &&
+        return wait_geq(&p.fwdDone[t.k + p.NT * t.bn], d.nsolve(t.k), p, ti) &&
                (!fact || wait_geq(&p.panA[t.m + p.NT * t.k], d.nbi(t.m), p, ti)) &&
                wait_geq(&p.fwdB[t.m + p.NT * t.bn], t.k * d.nbi(t.m), p, ti);
     case TK_BWD_TRSM:
-        return wait_geq(&p.fwdDone[t.k + p.NT * t.bn], 1, p, ti) &&
+        return wait_geq(&p.fwdDone[t.k + p.NT * t.bn], d.nsolve(t.k), p, ti) &&
                wait_geq(&p.bwdB[t.k + p.NT * t.bn], (p.NT - 1 - t.k) * d.nbi(t.k), p, ti);
     case TK_BWD_UPD:
-        return wait_geq(&p.bwdDone[t.k + p.NT * t.bn], 1, p, ti) &&
+        return wait_geq(&p.bwdDone[t.k + p.NT * t.bn], d.nsolve(t.k), p, ti) &&
                wait_geq(&p.bwdB[t.m + p.NT * t.bn], (p.NT - 1 - t.k) * d.nbi(t.m), p, ti);
     }
     return false;
@@ -212,8 +218,28 @@ __device__ void run_task(const Task &t, const ExecParams &p, const Dims<T> &d, T
         const VT X = d.Bt(t.k, t.bn);
         const int w = d.wB(t.bn);
         if constexpr (std::is_same<T, float>::value) {
-            if (p.full_inv || (p.mode & MODE_XINV)) {
-                const VT Xk = p.full_inv ? d.X(t.k) : d.XI(t.k);
+            if (p.mode & MODE_XINV) {
+                // row block t.sub of the tile: forward Y_k = X_k B_k, backward B_k = X_k^T Y_k
+                const int r0 = t.sub * SUBB, n = d.tm(t.k);
+                const int mr = min(SUBB, n - r0);
+                const VT Xk = d.XI(t.k);
+                const VT Yk = d.Yt(t.k, t.bn);
+                for (int c0 = 0; c0 < w; c0 += 64) {
+                    const int wc = min(64, w - c0);
+                    Acc<Cfg12864<T, SP>> acc;
+                    acc.zero();
+                    if (t.kind == TK_FWD_TRSM) {
+                        cta_gemm(acc, Xk.sub(r0, 0), X.sub(0, c0).t(), mr, wc, r0 + mr, smem);
+                        acc.store_to(Yk.sub(r0, c0), mr, wc);
+                    } else {
+                        cta_gemm(acc, Xk.sub(r0, r0).t(), Yk.sub(r0, c0).t(), mr, wc, n - r0, smem);
+                        acc.store_to(X.sub(r0, c0), mr, wc);
+                    }
+                }
+                break;
+            }
+            if (p.full_inv) {
+                const VT Xk = d.X(t.k);
                 if (t.kind == TK_FWD_TRSM) rec::apply_inv_left<T, SP, false>(X, w, Xk, d.tm(t.k), smem);
                 else rec::apply_inv_left<T, SP, true>(X, w, Xk, d.tm(t.k), smem);
                 break;
@@ -229,8 +255,10 @@ __device__ void run_task(const Task &t, const ExecParams &p, const Dims<T> &d, T
         const int r0 = t.sub * SUBB;
         const int rows = min(SUBB, d.tm(t.m) - r0);
         const int w = d.wB(t.bn);
-        const VT Bm = d.Bt(t.m, t.bn).sub(r0, 0);
-        const VT Bk = d.Bt(t.k, t.bn);
+        // MODE_XINV: forward updates read Y_k into B_m, backward ones read B_k into Y_m
+        const bool y = p.mode & MODE_XINV;
+        const VT Bm = ((y && t.kind == TK_BWD_UPD) ? d.Yt(t.m, t.bn) : d.Bt(t.m, t.bn)).sub(r0, 0);
+        const VT Bk = (y && t.kind == TK_FWD_UPD) ? d.Yt(t.k, t.bn) : d.Bt(t.k, t.bn);
         const VT L = (t.kind == TK_FWD_UPD) ? d.A(t.m, t.k).sub(r0, 0) : d.A(t.k, t.m).t().sub(r0, 0);
         for (int c0 = 0; c0 < w; c0 += 64) {
             const int wc = min(64, w - c0);

@@ -108,6 +108,8 @@ struct ExecWs {
     size_t xinv_bytes = 0;
     const void *xinv_owner = nullptr;   // factor storage the inverses belong to (nullptr: none)
     int xinv_n = 0, xinv_nt = 0, xinv_nb = 0;
+    void *y = nullptr;                  // forward-substitution results (MODE_XINV)
+    size_t y_bytes = 0;
     size_t ctr_bytes = 0, inv_bytes = 0;
     void *ctr = nullptr;
     void *inv = nullptr;

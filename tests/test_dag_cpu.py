@@ -33,6 +33,8 @@ def check_waits(tasks, mode, N, NB, nrhs, NBB):
     bwdB = np.zeros_like(fwdB); bwdD = np.zeros_like(fwdB)
     xinv = np.zeros(NT, int)
     fact = bool(mode & FACT)
+    # with full tile inverses (XINV) each substitution is split into row blocks
+    ns = (lambda k: nbi(k)) if mode & XINV else (lambda k: 1)
     for kind, sub, m, n, k, bn in tasks:
         if kind == TK_POTRF:
             ok = upd[k, k] >= k * S(k, k); pan[k, k] += 1
@@ -51,12 +53,12 @@ def check_waits(tasks, mode, N, NB, nrhs, NBB):
                 inv_ok = pan[k, k] >= 1
             ok = inv_ok and fwdB[k, bn] >= k * nbi(k); fwdD[k, bn] += 1
         elif kind == TK_FWD_UPD:
-            ok = fwdD[k, bn] >= 1 and (not fact or pan[m, k] >= nbi(m)) and fwdB[m, bn] >= k * nbi(m)
+            ok = fwdD[k, bn] >= ns(k) and (not fact or pan[m, k] >= nbi(m)) and fwdB[m, bn] >= k * nbi(m)
             fwdB[m, bn] += 1
         elif kind == TK_BWD_TRSM:
-            ok = fwdD[k, bn] >= 1 and bwdB[k, bn] >= (NT - 1 - k) * nbi(k); bwdD[k, bn] += 1
+            ok = fwdD[k, bn] >= ns(k) and bwdB[k, bn] >= (NT - 1 - k) * nbi(k); bwdD[k, bn] += 1
         elif kind == TK_BWD_UPD:
-            ok = bwdD[k, bn] >= 1 and bwdB[m, bn] >= (NT - 1 - k) * nbi(m); bwdB[m, bn] += 1
+            ok = bwdD[k, bn] >= ns(k) and bwdB[m, bn] >= (NT - 1 - k) * nbi(m); bwdB[m, bn] += 1
         else:
             raise AssertionError(kind)
         assert ok, (kind, sub, m, n, k, bn)
@@ -66,19 +68,24 @@ def check_waits(tasks, mode, N, NB, nrhs, NBB):
             for n in range(m + 1):
                 assert upd[m, n] == n * S(m, n)
     if mode & SOLVE:
-        assert (fwdD[:, :NTB] == 1).all() and (bwdD[:, :NTB] == 1).all()
+        want = np.array([ns(k) for k in range(NT)])[:, None]
+        assert (fwdD[:, :NTB] == want).all() and (bwdD[:, :NTB] == want).all()
     if (mode & XINV) and (mode & SOLVE) and not (mode & NOINV):
         assert (xinv == 1).all()
     else:
         assert (xinv == 0).all()
 
 
-def emulate(tasks, A, B, uplo, N, NB, NBB):
-    """Run the task list on host arrays with the device tasks' arithmetic."""
+def emulate(tasks, A, B, uplo, N, NB, NBB, xinv=False):
+    """Run the task list on host arrays with the device tasks' arithmetic.
+    xinv: substitutions split into row blocks, forward results in a separate
+    array Y (forward reads B writes Y, backward reads Y writes B)."""
     NT, NTB, tm, nbi, S = geometry(N, NB, B.shape[1] if B is not None else 0, NBB)
     M = A if uplo == 122 else A.T          # logical lower view (writes land in A)
     L = lambda m, n: M[m * NB:m * NB + tm(m), n * NB:n * NB + tm(n)]
     Bt = lambda m, bn: B[m * NB:m * NB + tm(m), bn * NBB:min((bn + 1) * NBB, B.shape[1])]
+    Y = np.full_like(B, np.nan) if B is not None else None
+    Yt = lambda m, bn: Y[m * NB:m * NB + tm(m), bn * NBB:min((bn + 1) * NBB, B.shape[1])]
     for kind, sub, m, n, k, bn in tasks:
         if kind == TK_POTRF:
             T = L(k, k)
@@ -96,14 +103,22 @@ def emulate(tasks, A, B, uplo, N, NB, NBB):
             C -= upd
         elif kind in (TK_INV, TK_XINV):
             pass   # inverses of diagonal tiles: the emulation solves triangular systems directly
+        elif kind == TK_FWD_TRSM and xinv:
+            r = slice(sub * SUBB, (sub + 1) * SUBB)
+            Yt(k, bn)[r] = np.linalg.inv(np.tril(L(k, k)))[r] @ Bt(k, bn)
+        elif kind == TK_BWD_TRSM and xinv:
+            r = slice(sub * SUBB, (sub + 1) * SUBB)
+            Bt(k, bn)[r] = np.linalg.inv(np.tril(L(k, k))).T[r] @ Yt(k, bn)
         elif kind == TK_FWD_TRSM:
             X = Bt(k, bn); X[:] = sla.solve_triangular(np.tril(L(k, k)), X, lower=True)
         elif kind == TK_BWD_TRSM:
             X = Bt(k, bn); X[:] = sla.solve_triangular(np.tril(L(k, k)), X, lower=True, trans=1)
         elif kind == TK_FWD_UPD:
-            Bt(m, bn)[sub * SUBB:(sub + 1) * SUBB] -= L(m, k)[sub * SUBB:(sub + 1) * SUBB] @ Bt(k, bn)
+            src = Yt(k, bn) if xinv else Bt(k, bn)
+            Bt(m, bn)[sub * SUBB:(sub + 1) * SUBB] -= L(m, k)[sub * SUBB:(sub + 1) * SUBB] @ src
         elif kind == TK_BWD_UPD:
-            Bt(m, bn)[sub * SUBB:(sub + 1) * SUBB] -= L(k, m)[:, sub * SUBB:(sub + 1) * SUBB].T @ Bt(k, bn)
+            dst = Yt(m, bn) if xinv else Bt(m, bn)
+            dst[sub * SUBB:(sub + 1) * SUBB] -= L(k, m)[:, sub * SUBB:(sub + 1) * SUBB].T @ Bt(k, bn)
 
 
 SHAPES = [(15, 16, 1, 16), (37, 17, 22, 17), (300, 128, 5, 128), (700, 256, 70, 64), (1000, 384, 3, 384),
@@ -151,3 +166,18 @@ def test_schedule_dataflow_reproduces_cholesky(cb_host, orc, uplo, N, NB, nrhs, 
 def cb_host():
     import chameleon_b200 as cb
     return cb
+
+
+@pytest.mark.parametrize("uplo", [121, 122])
+@pytest.mark.parametrize("N,NB,nrhs,NBB", SHAPES[:6])
+def test_schedule_dataflow_with_full_tile_inverses(cb_host, orc, uplo, N, NB, nrhs, NBB):
+    """The split substitutions (row blocks, forward results in Y) produce the
+    solution, in a factor+solve launch and in a solve-only launch."""
+    A0 = orc.dplgsy(float(N), N, 52)
+    B0 = orc.dplrnt(N, nrhs, 5674)
+    A = A0.copy(); B = B0.copy()
+    emulate(cb_host.schedule(FACT | SOLVE | XINV, N, NB, nrhs, NBB, 13, 2), A, B, uplo, N, NB, NBB, xinv=True)
+    assert orc.check_solve(A0, B, B0) < 60
+    B2 = B0.copy()
+    emulate(cb_host.schedule(SOLVE | XINV | NOINV, N, NB, nrhs, NBB, 13, 2), A, B2, uplo, N, NB, NBB, xinv=True)
+    assert np.allclose(B2, B, rtol=1e-12, atol=1e-14)
