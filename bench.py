@@ -398,7 +398,8 @@ def serve_run(cb, load, reqs, arrivals, slots, key_pool=32):
     st = sv.stats()
     sv.close()
     for (Nr, kr, reuse, r, X, tarr) in pending:
-        done.append((Nr, kr, reuse, r.t_done - tarr, r.status, X, r.iterations, r.t_done - r.t_start))
+        done.append((Nr, kr, reuse, r.t_done - tarr, r.status, X, r.iterations, r.t_done - r.t_start,
+                     r.t_start - r.t_submit, r.t_submit - tarr))
     return done, t1 - t0, st
 
 
@@ -423,7 +424,7 @@ def serve_section(args, cb, rank):
         buckets.setdefault(key, []).append(d[7] * 1e3)
     service = {k: {"count": len(v), "mean_ms": float(np.mean(v)), "p99_ms": float(np.percentile(v, 99))}
                for k, v in sorted(buckets.items())}
-    for (Nr, kr, reuse, lat, status, X, it, svc) in done[::max(1, len(done) // 12)]:
+    for (Nr, kr, reuse, lat, status, X, it, svc, _q, _lag) in done[::max(1, len(done) // 12)]:
         Ai = load.An[:Nr, :Nr].T
         Ai = np.tril(Ai) + np.tril(Ai, -1).T
         Bi = load.Bn[:kr, :Nr].T
@@ -456,7 +457,11 @@ def serve_section(args, cb, rank):
         warm = int(0.1 * len(done))
         lat = np.array([d[3] for d in done[warm:]]) * 1e3
         assert all(d[4] == 0 for d in done)
+        slow = sorted(done[warm:], key=lambda d: -d[3])[:6]
         loads.append({"load_frac": frac, "offered_per_s": rate, "requests": len(done),
+                      "slowest": [{"N": d[0], "nrhs": d[1], "reuse": d[2], "latency_ms": round(d[3] * 1e3, 2),
+                                   "queue_ms": round(d[8] * 1e3, 2), "service_ms": round(d[7] * 1e3, 2),
+                                   "submit_lag_ms": round(d[9] * 1e3, 2)} for d in slow],
                       "solves_per_s": len(done) / el, "p50_ms": float(np.percentile(lat, 50)),
                       "p99_ms": float(np.percentile(lat, 99)), "batches": st["batches"],
                       "batched_requests": st["batched_requests"], "max_batch": st["max_batch"],

@@ -105,24 +105,25 @@ __global__ void __launch_bounds__(NT_CTA, 1) trsm_batch_kernel(const TrsmItem *i
 
 BatchWs g_bws;
 
+// Grow-only, stream-ordered (no device-wide synchronization when growing).
 int bws_reserve(BatchWs &ws, size_t item_bytes, size_t scratch_bytes, size_t ninfo) {
-    if (!ws.cursor) CHB_CUDA(cudaMalloc(&ws.cursor, sizeof(int)));
+    if (!ws.cursor && !(ws.cursor = (int *)dev_alloc(sizeof(int)))) return CHAMELEON_ERR_OUT_OF_RESOURCES;
     if (item_bytes > ws.items_bytes) {
-        if (ws.items) cudaFree(ws.items);
-        ws.items = nullptr;
-        CHB_CUDA(cudaMalloc(&ws.items, item_bytes));
+        dev_free(ws.items);
+        ws.items_bytes = 0;
+        if (!(ws.items = dev_alloc(item_bytes))) return CHAMELEON_ERR_OUT_OF_RESOURCES;
         ws.items_bytes = item_bytes;
     }
     if (scratch_bytes > ws.scratch_bytes) {
-        if (ws.scratch) cudaFree(ws.scratch);
-        ws.scratch = nullptr;
-        CHB_CUDA(cudaMalloc(&ws.scratch, scratch_bytes));
+        dev_free(ws.scratch);
+        ws.scratch_bytes = 0;
+        if (!(ws.scratch = (double *)dev_alloc(scratch_bytes))) return CHAMELEON_ERR_OUT_OF_RESOURCES;
         ws.scratch_bytes = scratch_bytes;
     }
     if (ninfo > ws.info_n) {
-        if (ws.info) cudaFree(ws.info);
-        ws.info = nullptr;
-        CHB_CUDA(cudaMalloc(&ws.info, ninfo * sizeof(int)));
+        dev_free(ws.info);
+        ws.info_n = 0;
+        if (!(ws.info = (int *)dev_alloc(ninfo * sizeof(int)))) return CHAMELEON_ERR_OUT_OF_RESOURCES;
         ws.info_n = ninfo;
     }
     return 0;

@@ -119,10 +119,36 @@ cudaStream_t meta_stream() {
 // meta stream, so neither waits for kernels running on other streams (a plain
 // cudaFree synchronizes the whole device).  dev_alloc returns memory usable on
 // any stream; dev_free requires that no queued work still uses the memory.
+// The library's own memory pool: freed blocks stay mapped for reuse (release
+// threshold = max), so workspace churn never returns memory to the driver and
+// re-maps it -- which can stall every stream of the device.  The pool is an
+// object of this process; no device setting changes.
+static cudaMemPool_t lib_pool() {
+    static std::once_flag once;
+    static cudaMemPool_t pool = nullptr;
+    std::call_once(once, [] {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = ctx().device;
+        if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) {
+            cudaGetLastError();
+            pool = nullptr;
+            return;
+        }
+        uint64_t thr = ~0ull;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    });
+    return pool;
+}
+
 void *dev_alloc(size_t bytes) {
     void *p = nullptr;
     cudaStream_t ms = meta_stream();
-    if (cudaMallocAsync(&p, std::max<size_t>(bytes, 16), ms) != cudaSuccess) {
+    cudaMemPool_t pool = lib_pool();
+    const cudaError_t e = pool ? cudaMallocFromPoolAsync(&p, std::max<size_t>(bytes, 16), pool, ms)
+                               : cudaMallocAsync(&p, std::max<size_t>(bytes, 16), ms);
+    if (e != cudaSuccess) {
         cudaGetLastError();
         return nullptr;
     }
@@ -164,8 +190,14 @@ int desc_upload(CHAM_desc_t *d) {
     // descriptors does not synchronize the device (cudaFree would), so
     // concurrent solvers on other streams keep running.
     cudaStream_t ms = meta_stream();
-    CHB_CUDA(cudaMallocAsync(&pv->dev.off, nt * sizeof(int64_t), ms));
-    CHB_CUDA(cudaMallocAsync(&pv->dev.ld, d->mt * sizeof(int), ms));
+    cudaMemPool_t pool = lib_pool();
+    if (pool) {
+        CHB_CUDA(cudaMallocFromPoolAsync((void **)&pv->dev.off, nt * sizeof(int64_t), pool, ms));
+        CHB_CUDA(cudaMallocFromPoolAsync((void **)&pv->dev.ld, d->mt * sizeof(int), pool, ms));
+    } else {
+        CHB_CUDA(cudaMallocAsync(&pv->dev.off, nt * sizeof(int64_t), ms));
+        CHB_CUDA(cudaMallocAsync(&pv->dev.ld, d->mt * sizeof(int), ms));
+    }
     CHB_CUDA(cudaMemcpyAsync(pv->dev.off, off.data(), nt * sizeof(int64_t), cudaMemcpyHostToDevice, ms));
     CHB_CUDA(cudaMemcpyAsync(pv->dev.ld, ld.data(), d->mt * sizeof(int), cudaMemcpyHostToDevice, ms));
     CHB_CUDA(cudaStreamSynchronize(ms));

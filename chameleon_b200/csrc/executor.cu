@@ -247,9 +247,11 @@ Schedule *get_schedule(const Shape &s) {
     auto sch = std::make_unique<Schedule>();
     sch->tasks = build_order(s);
     if (!sch->tasks.empty()) {
-        if (cudaMalloc(&sch->d_tasks, sch->tasks.size() * sizeof(Task)) != cudaSuccess) return nullptr;
-        if (cudaMemcpy(sch->d_tasks, sch->tasks.data(), sch->tasks.size() * sizeof(Task),
-                       cudaMemcpyHostToDevice) != cudaSuccess)
+        const size_t bytes = sch->tasks.size() * sizeof(Task);
+        if (!(sch->d_tasks = (Task *)dev_alloc(bytes))) return nullptr;
+        cudaStream_t ms = meta_stream();
+        if (cudaMemcpyAsync(sch->d_tasks, sch->tasks.data(), bytes, cudaMemcpyHostToDevice, ms) != cudaSuccess ||
+            cudaStreamSynchronize(ms) != cudaSuccess)
             return nullptr;
     }
     Schedule *raw = sch.get();

@@ -461,10 +461,10 @@ int CHAM_B200_Serve_Destroy(CHAM_b200_server_t srv) {
     }
     sv->slots.clear();
     cudaStreamSynchronize(sv->bs);
-    cudaFree(sv->bws.items);
-    cudaFree(sv->bws.scratch);
-    cudaFree(sv->bws.cursor);
-    cudaFree(sv->bws.info);
+    dev_free(sv->bws.items);
+    dev_free(sv->bws.scratch);
+    dev_free(sv->bws.cursor);
+    dev_free(sv->bws.info);
     sv->bA = DevBuf();
     sv->bB = DevBuf();
     sv->binfo = DevBuf();
