@@ -541,8 +541,15 @@ def b200_arm(args, world, rank, local):
     else:
         peak, peak_src = pk.get("fp64_tflops"), "fp64"
     achieved = mult * fact_flops / (fact_ms * 1e-3) / 1e12 if fact_ms > 0 else None
+    # DRAM bytes of the factor+solve launch: one ncu capture at N = 8192
+    # (profiles/cholesky_dag_f32_bf16x3_tcgen05_N8192.md: 750.0 MB read + 773.4 MB
+    # written), scaled by the update work (N/8192)^3 -- the traffic is dominated by
+    # the trailing updates' panel reads, which grow with the flops
+    traffic = 1.5234e9 * (N / 8192.0) ** 3 if args.precision == "bf16x3" else None
     roofline = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                "frac": (achieved / peak) if (achieved and peak) else None, "traffic": None,
+                "frac": (achieved / peak) if (achieved and peak) else None, "traffic": traffic,
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum at N=8192 scaled by (N/8192)^3"
+                if traffic else None,
                 "kernel": "cholesky_dag_kernel<float,%s> (factorization + first solve)" % args.precision,
                 "flops_per_launch": mult * fact_flops,
                 "peak_source": peak_src + (" of measured" if peak else "")}

@@ -171,13 +171,32 @@ __global__ void __launch_bounds__(NT_CTA, 1) sym_residual_kernel(SymTiles a, Til
     if (threadIdx.x < w) atomicMax(&rmax[c0 + threadIdx.x], cmax[threadIdx.x]);
 }
 
-// Per-column max |X| of an N x nrhs operand.
+// Per-column max |X| of an M x N operand: block (bx, j) reduces a strided
+// share of column j's rows in registers and a warp/block tree, then issues one
+// atomic (non-negative doubles order like their bit patterns).
 __global__ void colmax_kernel(TileMapD x, int M, int N, unsigned long long *out) {
-    const int64_t total = (int64_t)M * N;
-    for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
-         idx += (int64_t)gridDim.x * blockDim.x) {
-        const int i = (int)(idx % M), j = (int)(idx / M);
-        atomicMax(&out[j], (unsigned long long)__double_as_longlong(fabs(*x.at<double>(i, j))));
+    __shared__ unsigned long long red[32];
+    const int j = blockIdx.y;
+    unsigned long long m = 0ull;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < M; i += gridDim.x * blockDim.x) {
+        const unsigned long long v = (unsigned long long)__double_as_longlong(fabs(*x.at<double>(i, j)));
+        m = v > m ? v : m;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long v = __shfl_xor_sync(0xffffffffu, m, o);
+        m = v > m ? v : m;
+    }
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        m = (threadIdx.x < (blockDim.x >> 5)) ? red[threadIdx.x] : 0ull;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const unsigned long long v = __shfl_xor_sync(0xffffffffu, m, o);
+            m = v > m ? v : m;
+        }
+        if (threadIdx.x == 0 && m) atomicMax(&out[j], m);
     }
 }
 
@@ -307,7 +326,8 @@ static int residual(CHAM_desc_t *A, cham_uplo_t uplo, CHAM_desc_t *B, CHAM_desc_
     CHB_CUDA(cudaMemsetAsync(m.xmax, 0, nrhs * sizeof(unsigned long long), s));
     sym_residual_kernel<<<A->nt * nrb * ncb, NT_CTA, Cfg12864<double>::SMEM_BYTES, s>>>(
         symtiles(A, uplo, m.diag), tmap(X), tmap(B), tmap(m.R), nrhs, nrb, ncb, m.rmax);
-    colmax_kernel<<<ew_grid((int64_t)X->m * nrhs), 256, 0, s>>>(tmap(X), X->m, nrhs, m.xmax);
+    colmax_kernel<<<dim3(std::max(1, std::min(32, (X->m + 4095) / 4096)), nrhs), 256, 0, s>>>(tmap(X), X->m, nrhs,
+                                                                                           m.xmax);
     CHB_LAUNCHED(2);
     CHB_CUDA(cudaGetLastError());
     std::vector<unsigned long long> hr(nrhs), hx(nrhs);
