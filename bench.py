@@ -214,6 +214,61 @@ def cpu_baseline_sample():
 
 
 # ---------------------------------------------------------------------------
+# Ill-conditioned systems: A = Q diag(s) Q^T, s geometric from 1 to 1/cond
+# ---------------------------------------------------------------------------
+COND_SEED = 1234
+
+
+def conditioning_section(args, cb, rank):
+    """C3: refinement convergence vs condition number and the FP64 fallback.
+    Inputs are built on the GPU (input setup, outside any timed region): Q from
+    the QR factorization of a seeded Gaussian matrix, B = A x_true."""
+    if rank != 0:
+        return None
+    import torch
+    N, nrhs, NB = args.cond_n, 16, 512
+    g = torch.Generator(device="cuda").manual_seed(COND_SEED)
+    Q, _ = torch.linalg.qr(torch.randn(N, N, dtype=torch.float64, device="cuda", generator=g))
+    xt = torch.randn(nrhs, N, dtype=torch.float64, device="cuda", generator=g)   # column-major N x nrhs
+    out = []
+    for cond in args.conds:
+        sv = torch.logspace(0.0, -np.log10(cond), N, dtype=torch.float64, device="cuda")
+        A0 = (Q * sv) @ Q.T
+        A0 = 0.5 * (A0 + A0.T)
+        B0 = (A0 @ xt.T).T.contiguous()
+        row = {"cond": cond}
+        for arm in ("mixed", "fp64"):
+            A = A0.clone()
+            B = B0.clone()
+            X = torch.zeros_like(B0)
+            dA = cb.Desc.create(N, N, NB, mat=A)
+            dB = cb.Desc.create(N, nrhs, NB, mat=B)
+            dX = cb.Desc.create(N, nrhs, NB, mat=X)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()   # both calls end synchronized
+            if arm == "mixed":
+                rc, info = cb.dposv_mixed_Tile(cb.ChamLower, cb.PREC_BF16X3, dA, dB, dX)
+            else:
+                rc = cb.dposv_Tile(cb.ChamLower, dA, dB)
+                X = B
+            ms = (time.perf_counter() - t0) * 1e3
+            torch.cuda.synchronize()
+            ferr = float((X - xt).abs().max() / xt.abs().max())
+            R = B0 - (A0 @ X.T).T
+            berr = float((R.abs().amax(dim=1) / (A0.abs().sum(dim=1).max() * X.abs().amax(dim=1))).max())
+            entry = {"rc": rc, "ms_wall": ms, "forward_error": ferr, "backward_error": berr}
+            if arm == "mixed":
+                entry.update({"iterations": info.iterations, "fallback": bool(info.fallback)})
+            row[arm] = entry
+            del dA, dB, dX
+        out.append(row)
+    return {"workload": "N=%d nrhs=%d, A = Q diag(s) Q^T (Q from QR of a Gaussian matrix, seed %d), s geometric "
+                        "from 1 to 1/cond, B = A x_true; mixed BF16x3 + FP64 refinement (dsposv rules, 30 "
+                        "iterations max, then FP64) vs plain FP64" % (N, nrhs, COND_SEED),
+            "cases": out}
+
+
+# ---------------------------------------------------------------------------
 # Uneven batch: 8192 systems, n ~ U{16..512}, nrhs ~ U{1..8}
 # ---------------------------------------------------------------------------
 BATCH_COUNT, BATCH_SEED, BATCH_NMIN, BATCH_NMAX = 8192, 2024, 16, 512
@@ -599,6 +654,7 @@ def b200_arm(args, world, rank, local):
                "api": "CHAMELEON_dsposv (LAPACK layout, pinned host A/B/X)"}
         del hA
 
+    cond = conditioning_section(args, cb, rank) if args.cond else None
     batch = batch_section(args, cb, world, rank) if args.batch else None
     serving = serve_section(args, cb, rank) if args.serve else None
     cpu = cpu_baseline_sample() if (rank == 0 and not args.no_cpu) else None
@@ -622,6 +678,7 @@ def b200_arm(args, world, rank, local):
         "e2e": e2e,
         "clocks": clk,
         "gpu_launches": launches,
+        "conditioning": cond,
         "batch": batch,
         "serving": serving,
     }
@@ -644,6 +701,9 @@ def main():
     ap.add_argument("--no-e2e", dest="e2e", action="store_false")
     ap.add_argument("--no-fp64", dest="compare_fp64", action="store_false")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-cond", dest="cond", action="store_false")
+    ap.add_argument("--cond-n", type=int, default=16384)
+    ap.add_argument("--conds", type=float, nargs="+", default=[1e4, 1e6, 1e8, 1e12])
     ap.add_argument("--no-batch", dest="batch", action="store_false")
     ap.add_argument("--batch-count", type=int, default=BATCH_COUNT)
     ap.add_argument("--batch-plain", type=int, default=BATCH_COUNT,
