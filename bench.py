@@ -360,7 +360,25 @@ def batch_section(args, cb, world, rank):
             assert rc == 0, rc
         torch.cuda.synchronize()
         plain_ms = (time.perf_counter() - t0) * 1e3 * count / m
-    del A0, B0, A, B
+    tune = (ctypes.c_double * 5)()
+    L.CHAM_B200_Batch_Tuning(cb.ChamRealDouble, tune)
+    # FP32 systems: the same batch cast to FP32 through CHAM_B200_sposv_batch
+    A32, B32 = A0.float(), B0.float()
+    A, B = A32.clone(), B32.clone()
+    t32 = []
+    for it in range(args.warmup + args.steps):
+        A.copy_(A32)
+        B.copy_(B32)
+        torch.cuda.synchronize()
+        L.CHAM_B200_Event_Record(6)
+        rc = L.CHAM_B200_sposv_batch(cb.ChamLower, count, ptr(dn), ptr(dk), ptr(A), ptr(da), ptr(B), ptr(db),
+                                     ptr(info), None)
+        assert rc == 0, rc
+        L.CHAM_B200_Event_Record(7)
+        if it >= args.warmup:
+            t32.append(L.CHAM_B200_Event_Elapsed(6, 7))
+    ms32 = allreduce_max(statistics.median(t32), world)
+    del A0, B0, A, B, A32, B32
     sps = count * world / (ms_max * 1e-3)
     return {
         "workload": "%d SPD systems, n~U{%d..%d}, nrhs~U{1..8} (seed %d), dplgsy(bump=n, seed=%d+i, bigM=n), "
@@ -372,6 +390,13 @@ def batch_section(args, cb, world, rank):
                               "sampled_matrices": min(count, args.batch_plain),
                               "api": "CHAMELEON_dposv per matrix (device arrays)"} if plain_ms else None),
         "speedup_vs_plain": (plain_ms / ms_max) if plain_ms else None,
+        "fp32": {"solves_per_s": count * world / (ms32 * 1e-3), "ms_per_step": ms32,
+                 "api": "CHAM_B200_sposv_batch (FP32 systems)"},
+        "size_bins": {"small_n_max": 64, "small_bin_mode": int(tune[0]),
+                      "small_bin_modes_ms": {"generic": tune[1], "small_x1": tune[2], "small_x2": tune[3],
+                                             "small_x3": tune[4]},
+                      "note": "autotuner: the small bin runs on the generic kernel or the small-system kernel at "
+                              "1..3 CTAs per SM, whichever was fastest on 4096 synthetic systems"},
         "roofline": {"bound": "fp64", "achieved": flops / (ms_max * 1e-3) / 1e12, "peak": 40.0,
                      "unit": "TFLOP/s", "frac": flops / (ms_max * 1e-3) / 1e12 / 40.0,
                      "peak_source": "FP64 spec 40 TFLOP/s (fallback: no FP64 entry in the measured peaks)"},

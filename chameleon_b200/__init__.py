@@ -156,6 +156,7 @@ PROTOS = {
     "CUDA_dlag2s": (_i, [_i, _i, _vp, _i, _vp, _i, _vp]),
     "CUDA_slag2d": (_i, [_i, _i, _vp, _i, _vp, _i, _vp]),
     "CHAM_B200_dposv_batch": (_i, [_i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "CHAM_B200_sposv_batch": (_i, [_i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "CHAM_B200_Serve_Create": (_i, [ctypes.POINTER(_vp), _i, ctypes.c_double, _i]),
     "CHAM_B200_Serve_Submit": (_i, [_vp, ctypes.POINTER(Request)]),
     "CHAM_B200_Serve_Drain": (_i, [_vp]),
@@ -178,6 +179,7 @@ EXTRAS = {
     "CHAM_B200_Mixed_Stats": (_i, [_dp]),
     "CHAM_B200_Test_TC05": (_i, [_vp, _vp, _i, _vp]),
     "CHAM_B200_Mixed_Factor_Only": (_i, [_i, _i, _D, _D, ctypes.POINTER(ctypes.c_float)]),
+    "CHAM_B200_Batch_Tuning": (_i, [_i, _dp]),
 }
 
 _lib = None

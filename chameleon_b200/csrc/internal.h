@@ -149,6 +149,8 @@ struct BatchWs {
     int *cursor = nullptr;
     int *info = nullptr;
     size_t info_n = 0;
+    cudaStream_t side = nullptr;          // small-bin stream (joined back before return)
+    cudaEvent_t fork = nullptr, join = nullptr;
 };
 extern BatchWs g_bws;   // the synchronous API's
 int bws_reserve(BatchWs &ws, size_t item_bytes, size_t scratch_bytes, size_t ninfo);

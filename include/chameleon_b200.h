@@ -281,6 +281,10 @@ int CUDA_slag2d(int m, int n, const float *SA, int ldsa, double *A, int lda,
 int CHAM_B200_dposv_batch(cham_uplo_t uplo, int count, const int *n, const int *nrhs,
                           double *A, const int64_t *a_off, double *B, const int64_t *b_off,
                           int *info, void *cuda_stream);
+/* The same for FP32 systems (FP32 storage and arithmetic). */
+int CHAM_B200_sposv_batch(cham_uplo_t uplo, int count, const int *n, const int *nrhs,
+                          float *A, const int64_t *a_off, float *B, const int64_t *b_off,
+                          int *info, void *cuda_stream);
 
 /* ------------------------------------------------------------------------- */
 /* Serving loop (new; the reference solves one system per call).  A server    */

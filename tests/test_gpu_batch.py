@@ -109,3 +109,71 @@ def test_uneven_batch_dposv(cb, orc, uplo):
         R = Bs[i] - As[i] @ Xi
         res = np.abs(R).sum(0).max() / (np.abs(As[i]).sum(0).max() * np.abs(Xi).sum(0).max() * n * EPS)
         assert res < 60, (i, n, res)
+
+
+def _run_batch(cb, fn, uplo, ns, rs, As, Bs, dtype):
+    import torch
+    a_off = np.cumsum([0] + [n * n for n in ns[:-1]]).astype(np.int64)
+    b_off = np.cumsum([0] + [n * r for n, r in zip(ns[:-1], rs[:-1])]).astype(np.int64)
+    A = np.concatenate([a.ravel(order="F") for a in As]).astype(dtype)
+    B = np.concatenate([b.ravel(order="F") for b in Bs]).astype(dtype)
+    dev = lambda x: torch.from_numpy(np.ascontiguousarray(x)).cuda()
+    tA, tB = dev(A), dev(B)
+    tn, tr, ta, tb = dev(ns.astype(np.int32)), dev(rs.astype(np.int32)), dev(a_off), dev(b_off)
+    info = torch.full((len(ns),), 7, dtype=torch.int32, device="cuda")
+    p = lambda t: ctypes.c_void_p(t.data_ptr())
+    rc = getattr(cb.lib(), fn)(uplo, len(ns), p(tn), p(tr), p(tA), p(ta), p(tB), p(tb), p(info), None)
+    assert rc == 0
+    X = tB.cpu().numpy()
+    return [X[b_off[i]:b_off[i] + n * r].reshape((n, r), order="F") for i, (n, r) in enumerate(zip(ns, rs))], \
+        info.cpu().numpy()
+
+
+def _residual(A, X, B, eps):
+    R = B - A @ X
+    return np.abs(R).sum(0).max() / (np.abs(A).sum(0).max() * np.abs(X).sum(0).max() * A.shape[0] * eps)
+
+
+@pytest.mark.parametrize("uplo", [121, 122])
+def test_small_bin_systems(cb, orc, uplo):
+    """n <= 64 runs in the small-system kernel (or wherever the autotuner put
+    the small bin): every order from 1 to 64, the solve check per system."""
+    ns = np.arange(1, 65)
+    rs = (ns % 5) + 1
+    As = [orc.dplgsy(float(n), int(n), 3000 + int(n)) for n in ns]
+    Bs = [orc.dplrnt(int(n), int(r), 4000 + int(n)) for n, r in zip(ns, rs)]
+    Xs, inf = _run_batch(cb, "CHAM_B200_dposv_batch", uplo, ns, rs, As, Bs, np.float64)
+    assert (inf == 0).all()
+    for A, X, B in zip(As, Xs, Bs):
+        assert _residual(A, X, B, EPS) < 60
+
+
+def test_batch_replay_is_identical(cb, orc):
+    """The second call with the same batch replays the captured graph: same bits."""
+    ns, rs, As, Bs = _uneven_batch(orc, 200, 16, 300, 6, 77)
+    X1, i1 = _run_batch(cb, "CHAM_B200_dposv_batch", 122, ns, rs, As, Bs, np.float64)
+    X2, i2 = _run_batch(cb, "CHAM_B200_dposv_batch", 122, ns, rs, As, Bs, np.float64)
+    assert (i1 == 0).all() and (i2 == 0).all()
+    for a, b in zip(X1, X2):
+        assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("uplo", [121, 122])
+def test_sposv_batch_fp32(cb, orc, uplo):
+    """FP32 systems: solve check at FP32 precision (eps = 2^-24)."""
+    ns, rs, As, Bs = _uneven_batch(orc, 150, 16, 400, 8, 88)
+    Xs, inf = _run_batch(cb, "CHAM_B200_sposv_batch", uplo, ns, rs, As, Bs, np.float32)
+    assert (inf == 0).all()
+    for A, X, B in zip(As, Xs, Bs):
+        assert _residual(A.astype(np.float32).astype(np.float64), X.astype(np.float64),
+                         B.astype(np.float32).astype(np.float64), 2.0 ** -24) < 60
+
+
+def test_batch_autotuner_picked_the_fastest(cb, orc):
+    ns, rs, As, Bs = _uneven_batch(orc, 20, 16, 64, 2, 99)
+    _run_batch(cb, "CHAM_B200_dposv_batch", 122, ns, rs, As, Bs, np.float64)   # tunes on first use
+    out = (ctypes.c_double * 5)()
+    assert cb.lib().CHAM_B200_Batch_Tuning(cb.ChamRealDouble, out) == 0
+    mode, times = int(out[0]), [t for t in out[1:] if t >= 0]
+    assert 0 <= mode <= 3 and len(times) >= 2
+    assert out[1 + mode] == min(times)
