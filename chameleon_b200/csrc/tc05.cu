@@ -32,10 +32,12 @@ __global__ void __launch_bounds__(NT_CTA, 1) tc05_test_kernel(const uint8_t *a, 
     tc05::init(&tsm);
     // two GEMMs in a row exercise the phase bookkeeping across tasks
     for (int rep = 0; rep < 2; ++rep) {
-        const bool ok = tc05::gemm_bf16x3(&tsm, stage, a, b, nkc, [&](int r, int c0, const float *v) {
-            if (rep == 1)
-                for (int i = 0; i < 16; ++i) C[r + (c0 + i) * 128] = v[i];
-        });
+        const bool ok = tc05::gemm_bf16x3(
+            &tsm, stage, a, b, nkc, [](int, int) {},
+            [&](int r, int c0, const float *v, int) {
+                if (rep == 1)
+                    for (int i = 0; i < 16; ++i) C[r + (c0 + i) * 128] = v[i];
+            });
         if (!ok && threadIdx.x == 0) *err = 1;
     }
     tc05::finish(&tsm);

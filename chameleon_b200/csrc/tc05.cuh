@@ -206,10 +206,14 @@ __device__ __forceinline__ void split_store8(uint8_t *chunk, int r, int c0, cons
 // acc = A * B^T over nkc chunks, A chunks at a_chunks[kc], B at b_chunks[kc]
 // (each chunk = hi 16 KB + lo 16 KB, consecutive chunks 32 KB apart), then
 // f(row, col0, v[16]) for accumulator row `row`, columns col0..col0+15, by the
-// owning thread.  Call with all 256 threads.  Returns false on a wait timeout.
-template <class F>
+// owning thread.  pre(row, col0) runs first, once per thread for the 64
+// columns it owns (col0 = its column half), so that the epilogue's global reads
+// can be issued before the accumulator is read; epilogue then gets
+// (row, col0 + 16 p, v, p) for p = 0..3.  Call with all 256 threads.  Returns
+// false on a wait timeout.
+template <class P, class F>
 __device__ bool gemm_bf16x3(Smem *sm, uint8_t *stage_base, const uint8_t *a_chunks, const uint8_t *b_chunks,
-                            int nkc, F &&epilogue) {
+                            int nkc, P &&pre, F &&epilogue) {
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const uint32_t base = sm->chunks;      // k chunks issued by this CTA before this GEMM
     const uint32_t gnum = sm->gemms;       // GEMMs finished by this CTA before this one
@@ -263,11 +267,12 @@ __device__ bool gemm_bf16x3(Smem *sm, uint8_t *stage_base, const uint8_t *a_chun
         const int q = warp & 3;                 // TMEM lane quarter of this warp
         const int cbase = (warp >> 2) * 64;     // column half
         const int row = q * 32 + lane;
+        pre(row, cbase);
 #pragma unroll
         for (int cc = 0; cc < 64; cc += 16) {
             float v[16];
             tmem_ld16(sm->tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(cbase + cc), v);
-            epilogue(row, cbase + cc, (const float *)v);
+            epilogue(row, cbase + cc, (const float *)v, cc >> 4);
         }
     }
     fence_before_sync();
