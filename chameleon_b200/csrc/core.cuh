@@ -117,6 +117,12 @@ __device__ __forceinline__ void cta_sync_global() {
     __threadfence();
     __syncthreads();
 }
+// Join the CTA after global writes that only this CTA reads back: bar.sync
+// orders every participating thread's earlier memory accesses before the
+// others' later ones (cp.async reads included), with no GPU-scope fence, which
+// is slow while the memory system is loaded.  Visibility to other CTAs is
+// established once per task by the executor (fence + release).
+__device__ __forceinline__ void cta_sync() { __syncthreads(); }
 __device__ __forceinline__ uint64_t globaltimer() {
     uint64_t t;
     asm volatile("mov.u64 %0, %%globaltimer;\n" : "=l"(t));
@@ -220,7 +226,10 @@ struct GemmCfg {
     static_assert(WM * WN * 32 == NT_CTA, "8 warps");
     static_assert(FM >= 1 && FN >= 1, "warp tile too small");
     static constexpr int SA = stage_elems_max<T_, BM>(), SB = stage_elems_max<T_, BN>();
-    static constexpr int SMEM_ELEMS = 2 * (SA + SB);   // two pipeline stages
+    // cp.async pipeline depth (2: deeper pipelines measured slower in the
+    // executor kernel, and FP64 tiles would not fit more in shared memory)
+    static constexpr int ST = 2;
+    static constexpr int SMEM_ELEMS = ST * (SA + SB);
     static constexpr size_t SMEM_BYTES = sizeof(T_) * SMEM_ELEMS;
 };
 template <class T, int SP = SPLIT_BF16X3>
@@ -399,26 +408,33 @@ template <class C, bool AK, bool BK>
 __device__ void cta_gemm_impl(Acc<C> &acc, const ViewT<typename C::T> &A, const ViewT<typename C::T> &B, int M,
                               int N, int K, typename C::T *smem, bool alA, bool alB) {
     using T = typename C::T;
-    T *sA0 = smem, *sA1 = smem + C::SA;
-    T *sB0 = smem + 2 * C::SA, *sB1 = smem + 2 * C::SA + C::SB;
+    constexpr int ST = C::ST;
+    T *sA = smem, *sB = smem + ST * C::SA;
     const int nk = (K + KC - 1) / KC;
-    load_stage<T, C::BM, AK>(sA0, A, M, K, 0, alA);
-    load_stage<T, C::BN, BK>(sB0, B, N, K, 0, alB);
-    cp_async_commit();
-    for (int c = 0; c < nk; ++c) {
-        const bool odd = c & 1;
-        if (c + 1 < nk) {
-            load_stage<T, C::BM, AK>(odd ? sA0 : sA1, A, M, K, (c + 1) * KC, alA);
-            load_stage<T, C::BN, BK>(odd ? sB0 : sB1, B, N, K, (c + 1) * KC, alB);
-            cp_async_commit();
-            cp_async_wait<1>();
-        } else {
-            cp_async_wait<0>();
+    // prologue: stages 0 .. ST-2 in flight (one commit group each, possibly empty)
+#pragma unroll
+    for (int st = 0; st < ST - 1; ++st) {
+        if (st < nk) {
+            load_stage<T, C::BM, AK>(sA + st * C::SA, A, M, K, st * KC, alA);
+            load_stage<T, C::BN, BK>(sB + st * C::SB, B, N, K, st * KC, alB);
         }
+        cp_async_commit();
+    }
+    for (int c = 0; c < nk; ++c) {
+        const int nxt = c + ST - 1;
+        if (nxt < nk) {
+            const int slot = nxt % ST;
+            load_stage<T, C::BM, AK>(sA + slot * C::SA, A, M, K, nxt * KC, alA);
+            load_stage<T, C::BN, BK>(sB + slot * C::SB, B, N, K, nxt * KC, alB);
+        }
+        cp_async_commit();
+        cp_async_wait<ST - 1>();   // stage c has landed
         __syncthreads();
-        mma_stage<C, AK, BK>(acc, odd ? sA1 : sA0, odd ? sB1 : sB0);
+        const int slot = c % ST;
+        mma_stage<C, AK, BK>(acc, sA + slot * C::SA, sB + slot * C::SB);
         __syncthreads();
     }
+    cp_async_wait<0>();
 }
 
 template <class T>
@@ -531,13 +547,13 @@ __device__ inline void trsm_rows(const ViewT<T> &X, int rows, const ViewT<T> &L,
             acc.zero();
             cta_gemm(acc, X, L.sub(jb, 0), rows, nbk, jb, smem);
             acc.sub_from(X.sub(0, jb), rows, nbk, false);
-            cta_sync_global();
+            cta_sync();
         }
         acc.zero();
         const ViewT<T> Inv{const_cast<T *>(invd) + (int64_t)(jb / IB) * IB * IB, 1, IB};
         cta_gemm(acc, X.sub(0, jb), Inv, rows, nbk, nbk, smem);
         acc.store_to(X.sub(0, jb), rows, nbk);
-        cta_sync_global();
+        cta_sync();
     }
 }
 
@@ -568,7 +584,7 @@ __device__ inline void trsm_left(const ViewT<T> &X, int w, const ViewT<T> &L, in
         const ViewT<T> Xj = X.sub(jb, 0);
         if (had) {
             acc.sub_from(Xj, nbk, w, false);
-            cta_sync_global();
+            cta_sync();
         }
         acc.zero();
         ViewT<T> Inv{const_cast<T *>(invd) + (int64_t)b * IB * IB, 1, IB};
@@ -576,7 +592,7 @@ __device__ inline void trsm_left(const ViewT<T> &X, int w, const ViewT<T> &L, in
         // acc(i,c) = sum_k op(Inv)(i,k) Xj(k,c)
         cta_gemm(acc, Inv, Xj.t(), nbk, w, nbk, smem);
         acc.store_to(Xj, nbk, w);
-        cta_sync_global();
+        cta_sync();
     }
 }
 

@@ -168,8 +168,8 @@ __device__ void run_task(const Task &t, const ExecParams &p, const Dims<T> &d, T
                 for (int e = 0; e < 8; ++e) v[e] = (r < rows) ? (float)*X.at(r, c0 + e) : 0.f;
                 tc05::split_store8(base + (size_t)(c0 / tc05::BK) * 2 * tc05::CHUNK_BYTES, r, c0 % tc05::BK, v);
             }
-            tc05::fence_proxy_async();
-            cta_sync_global();
+            tc05::fence_proxy_async();   // published by the executor's fence + release at task end
+            cta_sync();
         }
         break;
     }

@@ -217,7 +217,7 @@ __device__ __noinline__ int leaf64(const ViewT<T> &A, const ViewT<T> &X, int n, 
         if (FACT && r >= c) *A.at(r, c) = sD[r + c * LDS];
         *X.at(r, c) = sX[r + c * LDS];
     }
-    cta_sync_global();
+    cta_sync();
     return 0;
 }
 
@@ -251,7 +251,7 @@ __device__ int tile_potrf_blk(const ViewT<T> &Tv, int n, T *invd, T *smem) {
             if (r < nbk && c < nbk && r >= c) *Tv.at(jb + r, jb + c) = sD[r + c * LDS];
             inv[idx] = (r < nbk && c < nbk) ? sX[r + c * LDS] : T(0);
         }
-        cta_sync_global();
+        cta_sync();
         // panel below the inner diagonal block
         for (int r0 = jb + nbk; r0 < n; r0 += 128) {
             const int mr = min(128, n - r0);
@@ -260,13 +260,13 @@ __device__ int tile_potrf_blk(const ViewT<T> &Tv, int n, T *invd, T *smem) {
                 pa.zero();
                 cta_gemm(pa, Tv.sub(r0, 0), Tv.sub(jb, 0), mr, nbk, jb, smem);
                 pa.sub_from(Tv.sub(r0, jb), mr, nbk, false);
-                cta_sync_global();
+                cta_sync();
             }
             pa.zero();
             const ViewT<T> Inv{inv, 1, IB};
             cta_gemm(pa, Tv.sub(r0, jb), Inv, mr, nbk, nbk, smem);
             pa.store_to(Tv.sub(r0, jb), mr, nbk);
-            cta_sync_global();
+            cta_sync();
         }
     }
     return 0;
@@ -309,7 +309,7 @@ __device__ __noinline__ void apply_inv_right(const ViewT<T> &A, int rows, const 
             acc.zero();
             cta_gemm(acc, A.sub(r0, 0), X.sub(c0, 0), mr, w, c0 + w, smem);
             acc.store_to(A.sub(r0, c0), mr, w);
-            cta_sync_global();
+            cta_sync();
         }
     }
 }
@@ -331,7 +331,7 @@ __device__ __noinline__ void apply_inv_left(const ViewT<T> &B, int w, const View
             if (!TRANS) cta_gemm(acc, X.sub(r0, 0), B.sub(0, c0).t(), mr, wc, r0 + mr, smem);
             else cta_gemm(acc, X.sub(r0, r0).t(), B.sub(r0, c0).t(), mr, wc, n - r0, smem);
             acc.store_to(B.sub(r0, c0), mr, wc);
-            cta_sync_global();
+            cta_sync();
         }
     }
 }
@@ -367,7 +367,7 @@ __device__ __noinline__ int rec_tile(const ViewT<T> &A, const ViewT<T> &X, int n
                     acc.sub_from(A22.sub(r0, c0), mr, w, r0 == c0);
                 }
             }
-            cta_sync_global();
+            cta_sync();
         }
         info = rec_tile<T, SP, FACT, LVL - 1>(A22, X22, n2, smem);
         if (info) return n1 + info;
@@ -382,7 +382,7 @@ __device__ __noinline__ int rec_tile(const ViewT<T> &A, const ViewT<T> &X, int n
                 acc.store_to(X21.sub(r0, c0), mr, w);
             }
         }
-        cta_sync_global();
+        cta_sync();
         // X21 = -X22 W in place, row blocks from the last
         const int nrb = (n2 + C::BM - 1) / C::BM;
         for (int rb = nrb - 1; rb >= 0; --rb) {
@@ -395,12 +395,12 @@ __device__ __noinline__ int rec_tile(const ViewT<T> &A, const ViewT<T> &X, int n
                 acc.for_each([&](int r, int c, T v) {
                     if (r < mr && c < w) *X21.at(r0 + r, c0 + c) = -v;
                 });
-                cta_sync_global();
+                cta_sync();
             }
         }
         // the upper-right block of the inverse is zero
         for (int idx = threadIdx.x; idx < n1 * n2; idx += NT_CTA) *X.at(idx % n1, n1 + idx / n1) = T(0);
-        cta_sync_global();
+        cta_sync();
         return 0;
     }
 }
