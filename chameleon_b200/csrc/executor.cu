@@ -40,7 +40,7 @@ struct Calib {
 static const Calib kCalib[3] = {
     {4.9, 4.7, 5.8, 3.9, 7.1},   // FP64 DMMA
     {4.0, 4.7, 2.1, 2.4, 3.3},   // FP32, split products on mma.sync
-    {4.0, 4.7, 0.92, 2.4, 3.3},  // FP32, tcgen05 updates
+    {4.2, 2.7, 0.92, 1.9, 4.0},  // FP32, tcgen05 updates, full-inverse substitutions (row-block sub-tasks)
 };
 
 struct Shape {
@@ -345,7 +345,11 @@ int run_cholesky_dag(int mode, cham_uplo_t uplo, CHAM_desc_t *A, CHAM_desc_t *B,
     // canonical shape so that callers with many distinct N share schedules.
     const int last_sub = ((N - (NT - 1) * NB) + SUBB - 1) / SUBB;
     const int canonN = (NT - 1) * NB + std::min(NB, last_sub * SUBB);
-    Shape sh{mode, canonN, NB, nrhs ? NTB * NBB : 0, NBB, grid, prof};
+    // nrhs enters the cost model (not the task list): keep it, with the last
+    // block's width rounded up to 16, so that the costs stay close and the
+    // number of distinct schedules stays small
+    const int canonR = nrhs ? (NTB - 1) * NBB + std::min(NBB, ((nrhs - (NTB - 1) * NBB + 15) / 16) * 16) : 0;
+    Shape sh{mode, canonN, NB, canonR, NBB, grid, prof};
     Schedule *sch = get_schedule(sh);
     if (!sch) return CHAMELEON_ERR_OUT_OF_RESOURCES;
     const int NIB = (NB + IB - 1) / IB;
