@@ -213,7 +213,7 @@ __device__ __forceinline__ T frag(const T *s, int row, int kk) {
 }
 
 // Tile configuration of cta_gemm: BM x BN outputs, WM x WN warps (8 warps).
-template <class T_, int BM_, int BN_, int WM_, int WN_, int SP_ = SPLIT_BF16X3>
+template <class T_, int BM_, int BN_, int WM_, int WN_, int SP_ = SPLIT_BF16X3, int ST_ = 2>
 struct GemmCfg {
     using T = T_;
     static constexpr bool F64 = std::is_same<T_, double>::value;
@@ -226,9 +226,10 @@ struct GemmCfg {
     static_assert(WM * WN * 32 == NT_CTA, "8 warps");
     static_assert(FM >= 1 && FN >= 1, "warp tile too small");
     static constexpr int SA = stage_elems_max<T_, BM>(), SB = stage_elems_max<T_, BN>();
-    // cp.async pipeline depth (2: deeper pipelines measured slower in the
-    // executor kernel, and FP64 tiles would not fit more in shared memory)
-    static constexpr int ST = 2;
+    // cp.async pipeline depth (2 in the executor kernel: deeper pipelines
+    // measured slower there, and FP64 tiles would not fit more; standalone
+    // long-K kernels such as the residual use 3)
+    static constexpr int ST = ST_;
     static constexpr int SMEM_ELEMS = ST * (SA + SB);
     static constexpr size_t SMEM_BYTES = sizeof(T_) * SMEM_ELEMS;
 };

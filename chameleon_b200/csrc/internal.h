@@ -127,6 +127,8 @@ struct MixedWs {
     double *colsum = nullptr;
     double *diag = nullptr;       // symmetric copies of the diagonal tiles (residuals)
     size_t diag_cap = 0;
+    double *part = nullptr;       // split-K partial products of the residual
+    size_t part_cap = 0;
     int *flag = nullptr;
     int cap_rhs = 0, cap_n = 0;
     cudaEvent_t e0 = nullptr, e1 = nullptr;

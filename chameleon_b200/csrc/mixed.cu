@@ -123,14 +123,22 @@ __global__ void sym_diag_kernel(SymTiles a) {
     }
 }
 
+// Residual GEMM tile: 128 x 64 FP64 outputs, 3-stage cp.async pipeline (the
+// block row of A is a long K sweep).
+using CfgRes = GemmCfg<double, 128, 64, 4, 2, SPLIT_BF16X3, 3>;
+
 // R = B - A X for symmetric A (one triangle stored), FP64 on DMMA.  One CTA
-// per (tile row m, 128-row block, 64-column block of the right-hand sides);
-// it sweeps the whole block row of A.  Also records per-column max |R|.
+// per (tile row m, 128-row block, 64-column block of the right-hand sides, K
+// part): it sweeps tile columns [kp NT / ksplit, (kp + 1) NT / ksplit) of the
+// block row of A.  ksplit == 1: writes R and the per-column max |R|; else the
+// partial product goes to part[kp] (N x nrhs, ld N) for residual_reduce_kernel,
+// which adds the parts in a fixed order (deterministic).
 __global__ void __launch_bounds__(NT_CTA, 1) sym_residual_kernel(SymTiles a, TileMapD xb, TileMapD bb, TileMapD rb,
-                                                                 int nrhs, int nrb, int ncb,
-                                                                 unsigned long long *rmax) {
+                                                                 int nrhs, int nrb, int ncb, int ksplit,
+                                                                 double *part, unsigned long long *rmax) {
     extern __shared__ __align__(128) double smem[];
-    const int task = blockIdx.x;
+    const int kp = blockIdx.x % ksplit;
+    const int task = blockIdx.x / ksplit;
     const int cb = task % ncb;            // 64-column block, aligned to the tile columns of X
     const int mr = task / ncb;            // (m, row block) flattened
     const int m = mr / nrb, rblk = mr % nrb;
@@ -142,21 +150,29 @@ __global__ void __launch_bounds__(NT_CTA, 1) sym_residual_kernel(SymTiles a, Til
     const int c0 = bn * xb.nb + (cb % per_tile) * 64;
     const int w = min(min(64, (bn + 1) * xb.nb - c0), nrhs - c0);
     if (w <= 0) return;
-    Acc<Cfg12864<double>> acc;
+    Acc<CfgRes> acc;
     acc.zero();
-    for (int n = 0; n < a.NT; ++n) {
+    const int n0 = kp * a.NT / ksplit, n1 = (kp + 1) * a.NT / ksplit;
+    for (int n = n0; n < n1; ++n) {
         const View An = (n < m) ? a.L(m, n).sub(r0, 0) : (n == m) ? a.D(m).sub(r0, 0) : a.L(n, m).t().sub(r0, 0);
         // X tile n, columns c0..c0+w: view of the N x nrhs operand in tile layout
         double *xp = xb.at<double>(n * a.NB, c0);
         const View Xn{xp, 1, xb.ld[n]};
         cta_gemm(acc, An, Xn.t(), rows, w, a.tm(n), smem);
     }
+    const int gi0 = m * a.NB + r0;
+    if (ksplit > 1) {
+        double *P = part + (size_t)kp * a.N * nrhs;
+        acc.for_each([&](int r, int c, double v) {
+            if (r < rows && c < w) P[(gi0 + r) + (size_t)(c0 + c) * a.N] = v;
+        });
+        return;
+    }
     __shared__ unsigned long long cmax[64];
     if (threadIdx.x < 64) cmax[threadIdx.x] = 0ull;
     __syncthreads();
-    const int gi0 = m * a.NB + r0;
     // R = B - acc: B and R are different arrays; all B loads go first
-    Acc<Cfg12864<double>> bv;
+    Acc<CfgRes> bv;
     acc.for_each_idx([&](int a2, int b2, int e, int r, int c, double) {
         bv.v[a2][b2][e] = (r < rows && c < w) ? __ldcg(bb.at<double>(gi0 + r, c0 + c)) : 0.0;
     });
@@ -169,6 +185,39 @@ __global__ void __launch_bounds__(NT_CTA, 1) sym_residual_kernel(SymTiles a, Til
     });
     __syncthreads();
     if (threadIdx.x < w) atomicMax(&rmax[c0 + threadIdx.x], cmax[threadIdx.x]);
+}
+
+// R = B - sum_kp part[kp] (parts added in order), and per-column max |R|:
+// block (bx, j) handles a strided share of column j's rows.
+__global__ void residual_reduce_kernel(const double *part, int ksplit, int N, TileMapD bb, TileMapD rb,
+                                       unsigned long long *rmax) {
+    __shared__ unsigned long long red[32];
+    const int j = blockIdx.y;
+    unsigned long long mx = 0ull;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+        double sum = 0.0;
+        for (int kp = 0; kp < ksplit; ++kp) sum += part[(size_t)kp * N * gridDim.y + i + (size_t)j * N];
+        const double res = *bb.at<double>(i, j) - sum;
+        *rb.at<double>(i, j) = res;
+        const unsigned long long v = (unsigned long long)__double_as_longlong(fabs(res));
+        mx = v > mx ? v : mx;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long v = __shfl_xor_sync(0xffffffffu, mx, o);
+        mx = v > mx ? v : mx;
+    }
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        mx = (threadIdx.x < (blockDim.x >> 5)) ? red[threadIdx.x] : 0ull;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const unsigned long long v = __shfl_xor_sync(0xffffffffu, mx, o);
+            mx = v > mx ? v : mx;
+        }
+        if (threadIdx.x == 0 && mx) atomicMax(&rmax[j], mx);
+    }
 }
 
 // Per-column max |X| of an M x N operand: block (bx, j) reduces a strided
@@ -316,16 +365,44 @@ static int residual(CHAM_desc_t *A, cham_uplo_t uplo, CHAM_desc_t *B, CHAM_desc_
     if (!uploaded(A) || !uploaded(B) || !uploaded(X) || !uploaded(m.R)) return CHAMELEON_ERR_UNEXPECTED;
     if (!g_res_attr) {
         CHB_CUDA(cudaFuncSetAttribute(sym_residual_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)Cfg12864<double>::SMEM_BYTES));
+                                      (int)CfgRes::SMEM_BYTES));
         g_res_attr = true;
     }
     const int nrhs = B->n;
     const int nrb = (A->nb + 127) / 128;
     const int ncb = X->nt * ((X->nb + 63) / 64);
+    // split the K sweep so that the working CTAs fill whole waves of SMs
+    const int sms = ctx().num_sms;
+    int nwork = 0;
+    for (int mm = 0; mm < A->nt; ++mm) nwork += (desc_tile_rows(A, mm) + 127) / 128;
+    nwork *= (nrhs + 63) / 64;
+    int ksplit = 1;
+    double best = 0;
+    for (int k = 1; k <= std::min(8, std::max(1, A->nt / 4)); ++k) {
+        const double eff = (double)nwork * k / ((double)((nwork * k + sms - 1) / sms) * sms);
+        if (eff > best + 0.02) {
+            best = eff;
+            ksplit = k;
+        }
+    }
+    if (ksplit > 1) {
+        const size_t bytes = (size_t)ksplit * A->n * nrhs * sizeof(double);
+        if (bytes > m.part_cap) {
+            dev_free(m.part);
+            m.part_cap = 0;
+            if (!(m.part = (double *)dev_alloc(bytes))) return CHAMELEON_ERR_OUT_OF_RESOURCES;
+            m.part_cap = bytes;
+        }
+    }
     CHB_CUDA(cudaMemsetAsync(m.rmax, 0, nrhs * sizeof(unsigned long long), s));
     CHB_CUDA(cudaMemsetAsync(m.xmax, 0, nrhs * sizeof(unsigned long long), s));
-    sym_residual_kernel<<<A->nt * nrb * ncb, NT_CTA, Cfg12864<double>::SMEM_BYTES, s>>>(
-        symtiles(A, uplo, m.diag), tmap(X), tmap(B), tmap(m.R), nrhs, nrb, ncb, m.rmax);
+    sym_residual_kernel<<<A->nt * nrb * ncb * ksplit, NT_CTA, CfgRes::SMEM_BYTES, s>>>(
+        symtiles(A, uplo, m.diag), tmap(X), tmap(B), tmap(m.R), nrhs, nrb, ncb, ksplit, m.part, m.rmax);
+    if (ksplit > 1) {
+        residual_reduce_kernel<<<dim3(std::max(1, std::min(32, (A->n + 4095) / 4096)), nrhs), 256, 0, s>>>(
+            m.part, ksplit, A->n, tmap(B), tmap(m.R), m.rmax);
+        CHB_LAUNCHED(1);
+    }
     colmax_kernel<<<dim3(std::max(1, std::min(32, (X->m + 4095) / 4096)), nrhs), 256, 0, s>>>(tmap(X), X->m, nrhs,
                                                                                            m.xmax);
     CHB_LAUNCHED(2);
@@ -411,6 +488,7 @@ void free_mixed_ws(MixedWs &m) {
     dev_free(m.xmax);
     dev_free(m.colsum);
     dev_free(m.diag);
+    dev_free(m.part);
     dev_free(m.flag);
     if (m.e0) cudaEventDestroy(m.e0);
     if (m.e1) cudaEventDestroy(m.e1);
@@ -470,16 +548,22 @@ int mixed_posv_ws(cham_uplo_t uplo, int precision, CHAM_desc_t *A, CHAM_desc_t *
             int it = 0;
             while (!ok && it < c.refine_maxiter) {
                 ++it;
+                clk.tic();
                 if ((rc = cast_desc(m.R, m.B32, s, nullptr))) return rc;
+                clk.toc(st.cast_ms);
                 if ((rc = run_cholesky_dag(MODE_SOLVE, uplo, m.A32, m.B32, s, &res, split, ews, grid, EXEC_REUSE_INV)))
                     return rc;
                 st.refine_solve_ms += res.ms;
                 if (res.error) return res.error;
                 if (!uploaded(X) || !uploaded(m.B32)) return CHAMELEON_ERR_UNEXPECTED;
+                clk.tic();
                 add_correction<<<ew_grid((int64_t)N * nrhs), 256, 0, s>>>(tmap(X), tmap(m.B32), N, nrhs);
                 CHB_LAUNCHED(1);
                 CHB_CUDA(cudaGetLastError());
+                clk.toc(st.cast_ms);
+                clk.tic();
                 if ((rc = residual(A, uplo, B, X, s, rn, xn, m))) return rc;
+                clk.toc(st.residual_ms);
                 ok = converged(rn, xn, cte, &berr);
             }
             if (ok) {
