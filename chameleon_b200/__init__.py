@@ -33,6 +33,7 @@ CHAMELEON_B200_WAIT_BUDGET_US = 104
 CHAMELEON_B200_TCGEN05 = 105
 CHAMELEON_B200_REC_TILE = 106
 CHAMELEON_B200_XINV_SOLVE = 107
+CHAMELEON_B200_POTRF_CTA = 108
 PREC_FP64, PREC_FP32, PREC_BF16X3 = 0, 1, 2
 CHAMELEON_SUCCESS = 0
 CHAMELEON_ERR_NOT_INITIALIZED = -101

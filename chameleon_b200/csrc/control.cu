@@ -422,6 +422,9 @@ int CHAMELEON_Set(int param, int value) {
     case CHAMELEON_B200_XINV_SOLVE:
         c.xinv_solve = (value != 0);
         return 0;
+    case CHAMELEON_B200_POTRF_CTA:
+        c.potrf_cta = (value != 0);
+        return 0;
     case CHAMELEON_TRANSLATION_MODE:
     case CHAMELEON_LOOKAHEAD:
     case CHAMELEON_CONCURRENCY:
@@ -443,6 +446,7 @@ int CHAMELEON_Get(int param, int *value) {
     case CHAMELEON_B200_TCGEN05: *value = c.use_tcgen05 ? 1 : 0; return 0;
     case CHAMELEON_B200_REC_TILE: *value = c.rec_tile ? 1 : 0; return 0;
     case CHAMELEON_B200_XINV_SOLVE: *value = c.xinv_solve ? 1 : 0; return 0;
+    case CHAMELEON_B200_POTRF_CTA: *value = c.potrf_cta ? 1 : 0; return 0;
     }
     return CHAMELEON_ERR_ILLEGAL_VALUE;
 }

@@ -70,6 +70,8 @@ struct Coarse {
 struct Schedule {
     std::vector<Task> tasks;
     Task *d_tasks = nullptr;
+    int npotrf = 0;              // POTRF tasks (for the dedicated CTA), their indices after the tasks
+    const int *d_potrf = nullptr;
 };
 
 std::vector<Task> build_order(const Shape &s) {
@@ -247,10 +249,18 @@ Schedule *get_schedule(const Shape &s) {
     auto sch = std::make_unique<Schedule>();
     sch->tasks = build_order(s);
     if (!sch->tasks.empty()) {
-        const size_t bytes = sch->tasks.size() * sizeof(Task);
+        std::vector<int> pidx;
+        for (size_t i = 0; i < sch->tasks.size(); ++i)
+            if (sch->tasks[i].kind == TK_POTRF) pidx.push_back((int)i);
+        const size_t tbytes = sch->tasks.size() * sizeof(Task);
+        const size_t bytes = tbytes + pidx.size() * sizeof(int);
         if (!(sch->d_tasks = (Task *)dev_alloc(bytes))) return nullptr;
+        sch->npotrf = (int)pidx.size();
+        sch->d_potrf = reinterpret_cast<const int *>(reinterpret_cast<const uint8_t *>(sch->d_tasks) + tbytes);
         cudaStream_t ms = meta_stream();
-        if (cudaMemcpyAsync(sch->d_tasks, sch->tasks.data(), bytes, cudaMemcpyHostToDevice, ms) != cudaSuccess ||
+        if (cudaMemcpyAsync(sch->d_tasks, sch->tasks.data(), tbytes, cudaMemcpyHostToDevice, ms) != cudaSuccess ||
+            (!pidx.empty() && cudaMemcpyAsync((void *)sch->d_potrf, pidx.data(), pidx.size() * sizeof(int),
+                                              cudaMemcpyHostToDevice, ms) != cudaSuccess) ||
             cudaStreamSynchronize(ms) != cudaSuccess)
             return nullptr;
     }
@@ -367,6 +377,11 @@ int run_cholesky_dag(int mode, cham_uplo_t uplo, CHAM_desc_t *A, CHAM_desc_t *B,
     ExecParams p{};
     p.tasks = sch->d_tasks;
     p.ntasks = (int)sch->tasks.size();
+    // one CTA runs the diagonal-tile factorizations (its instruction cache stays
+    // warm for their long unrolled leaves); the others skip them
+    const bool dedicate = c.potrf_cta && grid > 1 && sch->npotrf > 1;
+    p.npotrf = dedicate ? sch->npotrf : 0;
+    p.potrf_idx = sch->d_potrf;
     p.mode = mode;
     p.upper = (uplo == ChamUpper);
     p.NT = NT; p.N = N; p.NB = NB;

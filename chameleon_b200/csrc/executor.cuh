@@ -41,23 +41,31 @@ enum ExecMode : int { MODE_FACT = 1, MODE_SOLVE = 2, MODE_XINV = 4, MODE_NOINV =
 constexpr int SUBB = 128;      // sub-block edge of trailing updates / row blocks
 
 struct ExecState {
-    int next;          // dispatch cursor
+    int next;          // dispatch cursor (alone in its 128-byte line: the contended atomic)
+    int pad0[31];
     int abort;         // set on failure: remaining tasks are skipped
     int info;          // min global 1-based index of a non-positive pivot (INT_MAX: none)
     int error;         // 0 or a CHAMELEON_ERR_* code (device timeout)
-    int done;          // tasks completed
+    int done;          // tasks completed (each CTA adds its count when it exits)
     int stuck_task;    // task index whose wait ran out (-1)
     int pad[2];
 };
 
 struct TraceRec {
     int32_t task, smid;
-    uint64_t t0, t1;
+    uint64_t t0, t1;   // globaltimer after the dependency wait, at the end of the task
+    uint32_t wait_ns;  // time from taking the task to its dependencies being met
+    uint32_t ph[3];    // POTRF: clock cycles in (block-column update, leaf, panel)
 };
 
 struct ExecParams {
     const Task *tasks;
     int ntasks;
+    // npotrf > 0: CTA 0 runs exactly the POTRF tasks potrf_idx[0..npotrf) in
+    // order and the other CTAs skip them (both are sub-orders of one
+    // topological order, so the launch still always progresses)
+    int npotrf;
+    const int *potrf_idx;
     int mode;
     int upper;
     int NT, N, NB;          // A: NT x NT tiles, order N, tile size NB (square tiles)

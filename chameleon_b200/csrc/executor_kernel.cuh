@@ -6,6 +6,7 @@
 // instantiated in its own translation unit (exec_*.cu) so that the variants
 // compile in parallel; executor.cu holds the host side.
 #pragma once
+#include <climits>
 #include <cuda_runtime.h>
 
 #include "core.cuh"
@@ -54,15 +55,92 @@ struct Dims {
     }
 };
 
-// Thread 0 only.  Returns false when the run aborted or the wait ran out.
-__device__ inline bool wait_geq(const int *ctr, int target, const ExecParams &p, int task) {
-    if (ld_acquire(ctr) >= target) return true;
-    const uint64_t t0 = globaltimer();
+// The counters a task waits on and the values they must reach (up to three;
+// unused entries have a null counter).  bad: unknown task kind.
+struct Deps {
+    const int *c[3];
+    int v[3];
+    bool bad;
+};
+
+template <class T>
+__device__ Deps task_deps(const Task &t, const ExecParams &p, const Dims<T> &d) {
+    const bool fact = p.mode & MODE_FACT;
+    Deps r{{nullptr, nullptr, nullptr}, {0, 0, 0}, false};
+    auto need = [&](int i, const int *c, int v) {
+        r.c[i] = c;
+        r.v[i] = v;
+    };
+    switch (t.kind) {
+    case TK_POTRF:
+        need(0, &p.updA[t.k + p.NT * t.k], t.k * d.S(t.k, t.k));
+        break;
+    case TK_TRSM:
+        need(0, &p.panA[t.k + p.NT * t.k], 1);
+        need(1, &p.updA[t.m + p.NT * t.k], t.k * d.S(t.m, t.k));
+        break;
+    case TK_UPD:
+        need(0, &p.panA[t.m + p.NT * t.k], d.nbi(t.m));
+        need(1, &p.panA[t.n + p.NT * t.k], d.nbi(t.n));
+        need(2, &p.updA[t.m + p.NT * t.n], t.k * d.S(t.m, t.n));
+        break;
+    case TK_INV:
+        break;
+    case TK_XINV:
+        if (fact) need(0, &p.panA[t.k + p.NT * t.k], 1);
+        break;
+    case TK_FWD_TRSM:
+        if (!(p.mode & MODE_XINV)) need(0, &p.panA[t.k + p.NT * t.k], 1);
+        else if (!(p.mode & MODE_NOINV)) need(0, &p.xinvDone[t.k], 1);
+        need(1, &p.fwdB[t.k + p.NT * t.bn], t.k * d.nbi(t.k));
+        break;
+    case TK_FWD_UPD:
+        need(0, &p.fwdDone[t.k + p.NT * t.bn], d.nsolve(t.k));
+        if (fact) need(1, &p.panA[t.m + p.NT * t.k], d.nbi(t.m));
+        need(2, &p.fwdB[t.m + p.NT * t.bn], t.k * d.nbi(t.m));
+        break;
+    case TK_BWD_TRSM:
+        need(0, &p.fwdDone[t.k + p.NT * t.bn], d.nsolve(t.k));
+        need(1, &p.bwdB[t.k + p.NT * t.bn], (p.NT - 1 - t.k) * d.nbi(t.k));
+        break;
+    case TK_BWD_UPD:
+        need(0, &p.bwdDone[t.k + p.NT * t.bn], d.nsolve(t.k));
+        need(1, &p.bwdB[t.m + p.NT * t.bn], (p.NT - 1 - t.k) * d.nbi(t.m));
+        break;
+    default:
+        r.bad = true;
+    }
+    return r;
+}
+
+// Thread 0 only.  Each round reads every counter of the task and the abort
+// flag together (relaxed loads: one memory round trip, where acquire loads
+// would serialize); once all counters have reached their values one acquire
+// fence orders the task's reads after the producers' releases, and the
+// CTA barrier that follows extends that order to every thread.  Returns false
+// when the run aborted or the wait ran out.
+__device__ __forceinline__ bool deps_met(const Deps &dp) {
+    int v[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) v[i] = dp.c[i] ? ld_relaxed(dp.c[i]) : INT_MAX;
+    return v[0] >= dp.v[0] && v[1] >= dp.v[1] && v[2] >= dp.v[2];
+}
+
+__device__ inline bool wait_deps(const Deps &dp, const ExecParams &p, int task) {
+    if (dp.bad) return false;
+    uint64_t t0 = 0;
     unsigned ns = 32;
     while (true) {
-        if (ld_acquire(ctr) >= target) return true;
-        if (*(volatile int *)&p.st->abort) return false;
-        if (globaltimer() - t0 > p.wait_budget_ns) {
+        const int ab = ld_relaxed(&p.st->abort);
+        if (deps_met(dp)) {
+            fence_acq_rel_gpu();
+            return true;
+        }
+        if (ab) return false;
+        const uint64_t now = globaltimer();
+        if (t0 == 0) {
+            t0 = now;
+        } else if (now - t0 > p.wait_budget_ns) {
             atomicCAS(&p.st->error, 0, CHAMELEON_ERR_DEVICE_TIMEOUT);
             atomicExch(&p.st->stuck_task, task);
             atomicExch(&p.st->abort, 1);
@@ -73,61 +151,41 @@ __device__ inline bool wait_geq(const int *ctr, int target, const ExecParams &p,
     }
 }
 
-template <class T>
-__device__ bool task_wait(const Task &t, const ExecParams &p, const Dims<T> &d, int ti) {
-    const bool fact = p.mode & MODE_FACT;
-    switch (t.kind) {
-    case TK_POTRF:
-        return wait_geq(&p.updA[t.k + p.NT * t.k], t.k * d.S(t.k, t.k), p, ti);
-    case TK_TRSM:
-        return wait_geq(&p.panA[t.k + p.NT * t.k], 1, p, ti) &&
-               wait_geq(&p.updA[t.m + p.NT * t.k], t.k * d.S(t.m, t.k), p, ti);
-    case TK_UPD:
-        return wait_geq(&p.panA[t.m + p.NT * t.k], d.nbi(t.m), p, ti) &&
-               wait_geq(&p.panA[t.n + p.NT * t.k], d.nbi(t.n), p, ti) &&
-               wait_geq(&p.updA[t.m + p.NT * t.n], t.k * d.S(t.m, t.n), p, ti);
-    case TK_INV:
-        return true;
-    case TK_XINV:
-        return !fact || wait_geq(&p.panA[t.k + p.NT * t.k], 1, p, ti);
-    case TK_FWD_TRSM: {
-        bool ok = true;
-        if (!(p.mode & MODE_XINV)) ok = wait_geq(&p.panA[t.k + p.NT * t.k], 1, p, ti);
-        else if (!(p.mode & MODE_NOINV)) ok = wait_geq(&p.xinvDone[t.k], 1, p, ti);
-        return ok && wait_geq(&p.fwdB[t.k + p.NT * t.bn], t.k * d.nbi(t.k), p, ti);
-    }
-    case TK_FWD_UPD:
-        return wait_geq(&p.fwdDone[t.k + p.NT * t.bn], d.nsolve(t.k), p, ti) &&
-               (!fact || wait_geq(&p.panA[t.m + p.NT * t.k], d.nbi(t.m), p, ti)) &&
-               wait_geq(&p.fwdB[t.m + p.NT * t.bn], t.k * d.nbi(t.m), p, ti);
-    case TK_BWD_TRSM:
-        return wait_geq(&p.fwdDone[t.k + p.NT * t.bn], d.nsolve(t.k), p, ti) &&
-               wait_geq(&p.bwdB[t.k + p.NT * t.bn], (p.NT - 1 - t.k) * d.nbi(t.k), p, ti);
-    case TK_BWD_UPD:
-        return wait_geq(&p.bwdDone[t.k + p.NT * t.bn], d.nsolve(t.k), p, ti) &&
-               wait_geq(&p.bwdB[t.m + p.NT * t.bn], (p.NT - 1 - t.k) * d.nbi(t.m), p, ti);
-    }
-    return false;
-}
-
 // Split chunks (hi/lo BF16, swizzled) of panel tile (m,k), m > k.
 __device__ __forceinline__ uint8_t *split_tile(const ExecParams &p, int m, int k) {
     const size_t tile_bytes = (size_t)p.split_nrb * p.split_nkc * 2 * tc05::CHUNK_BYTES;
     return p.split + ((size_t)m * (m - 1) / 2 + k) * tile_bytes;
 }
 
+// Look-ahead of the dispatch loop, in shared memory.  A tcgen05 update task
+// does the dispatch work of the next task on a thread that is idle while the
+// copies and MMAs run: it claims the next cursor position, loads that task's
+// descriptor and checks its dependencies once (acquire fence if met), so the
+// dispatch round trips overlap the task; thread 0 consumes the result at the
+// top of the loop.  When the next task is a tcgen05 update that is ready, the
+// finished task's release is handed to that idle thread too (rel), so that
+// thread 0 does not stall on the release fence between tasks; the hand-over
+// cannot delay a dependency of the next task, which was met without it.
+struct Ahead {
+    int raw;     // cursor value claimed ahead (INT_MIN: none)
+    int have;    // t holds the descriptor of task raw
+    int ready;   // its dependencies were met (acquire fence done)
+    int *rel;    // counter whose release the next task performs (or null)
+    Task t;
+};
+
 template <class T, int SP, bool TC>
 __device__ void run_task(const Task &t, const ExecParams &p, const Dims<T> &d, T *smem, tc05::Smem *tsm,
-                         uint8_t *stage) {
+                         uint8_t *stage, unsigned *ph, Ahead *ah) {
     using VT = ViewT<T>;
     switch (t.kind) {
     case TK_POTRF: {
         int info;
         if constexpr (std::is_same<T, float>::value) {
             if (p.full_inv) info = rec::tile_potrf_inv<T, SP>(d.A(t.k, t.k), d.X(t.k), d.tm(t.k), smem);
-            else info = rec::tile_potrf_blk<T, SP>(d.A(t.k, t.k), d.tm(t.k), d.inv(t.k), smem);
+            else info = rec::tile_potrf_blk<T, SP>(d.A(t.k, t.k), d.tm(t.k), d.inv(t.k), smem, ph);
         } else {
-            info = rec::tile_potrf_blk<T, SP>(d.A(t.k, t.k), d.tm(t.k), d.inv(t.k), smem);
+            info = rec::tile_potrf_blk<T, SP>(d.A(t.k, t.k), d.tm(t.k), d.inv(t.k), smem, ph);
         }
         if (info && threadIdx.x == 0) {
             atomicMin(&p.st->info, t.k * p.NB + info);
@@ -208,6 +266,27 @@ __device__ void run_task(const Task &t, const ExecParams &p, const Dims<T> &d, T
                         const int c = c0 + i;
                         if (r < rows && c < cols && (!diag || r >= c)) *C.at(r, c) = old[q][i] - v[i];
                     }
+                },
+                [&]() {
+                    if (ah->rel) {
+                        red_release_add(ah->rel, 1);
+                        ah->rel = nullptr;
+                    }
+                    if (p.npotrf > 0) return;   // the dedicated-POTRF dispatch claims by itself
+                    const int raw = atomicAdd(&p.st->next, 1);
+                    int ready = 0;
+                    if (raw < p.ntasks) {
+                        const Task nt = p.tasks[raw];
+                        ah->t = nt;
+                        const Deps dp = task_deps(nt, p, d);
+                        if (!dp.bad && deps_met(dp)) {
+                            fence_acq_rel_gpu();
+                            ready = 1;
+                        }
+                    }
+                    ah->have = raw < p.ntasks;
+                    ah->ready = ready;
+                    ah->raw = raw;
                 });
             if (!ok && threadIdx.x == 0) {
                 atomicCAS(&p.st->error, 0, CHAMELEON_ERR_DEVICE_TIMEOUT);
@@ -308,38 +387,72 @@ __global__ void __launch_bounds__(NT_CTA, 1) cholesky_dag_kernel(ExecParams p) {
     __shared__ int s_task;
     __shared__ int s_ok;
     __shared__ tc05::Smem tsm;
+    __shared__ unsigned s_ph[3];   // phase cycles of the current task (tracing only)
     const Dims<T> d{p};
     if constexpr (TC) tc05::init(&tsm);
+    __shared__ Task s_desc;
+    uint64_t tg = 0;
+    const bool potrf_cta = p.npotrf > 0 && blockIdx.x == 0;
+    int pnext = 0;   // thread 0 of the POTRF CTA: next entry of potrf_idx
+    int ndone = 0;   // thread 0: tasks this CTA completed
+    __shared__ Ahead ah;   // task claimed ahead by the previous task
+    if (threadIdx.x == 0) {
+        ah.raw = INT_MIN;
+        ah.have = ah.ready = 0;
+        ah.rel = nullptr;
+    }
     while (true) {
         if (threadIdx.x == 0) {
-            int ti = -1;
-            if (!*(volatile int *)&p.st->abort) {
-                ti = atomicAdd(&p.st->next, 1);
+            int ti;
+            if (ah.raw != INT_MIN) {
+                ti = (ah.raw < p.ntasks) ? ah.raw : -1;
+            } else if (potrf_cta) {
+                ti = (pnext < p.npotrf) ? p.potrf_idx[pnext++] : -1;
+            } else {
+                do {
+                    ti = atomicAdd(&p.st->next, 1);
+                } while (p.npotrf > 0 && ti < p.ntasks && p.tasks[ti].kind == TK_POTRF);
                 if (ti >= p.ntasks) ti = -1;
             }
+            if (p.trace) {
+                tg = globaltimer();
+                s_ph[0] = s_ph[1] = s_ph[2] = 0u;
+            }
+            bool ok = false;
+            if (ti >= 0) {
+                const Task t = ah.have ? ah.t : p.tasks[ti];
+                s_desc = t;
+                ok = ah.ready || wait_deps(task_deps(t, p, d), p, ti);
+            }
+            ah.raw = INT_MIN;
+            ah.have = ah.ready = 0;
             s_task = ti;
-            s_ok = (ti >= 0) ? (int)task_wait(p.tasks[ti], p, d, ti) : 0;
+            s_ok = ok;
         }
         __syncthreads();
         const int ti = s_task;
         if (ti < 0 || !s_ok) break;
-        __threadfence();
-        const Task t = p.tasks[ti];
+        const Task t = s_desc;
         uint64_t t0 = 0;
         if (p.trace && threadIdx.x == 0) t0 = globaltimer();
-        run_task<T, SP, TC>(t, p, d, smem, &tsm, stage);
-        __threadfence();
+        run_task<T, SP, TC>(t, p, d, smem, &tsm, stage, p.trace ? s_ph : nullptr, &ah);
+        // Every thread's writes of the task precede thread 0's release through
+        // the barrier (the release is cumulative), so no per-thread fence.
         __syncthreads();
         if (threadIdx.x == 0) {
-            red_release_add(task_counter(t, p), 1);
-            atomicAdd(&p.st->done, 1);
+            int *ctr = task_counter(t, p);
+            if (TC && ah.ready && ah.t.kind == TK_UPD) ah.rel = ctr;   // released by the next task
+            else red_release_add(ctr, 1);
+            ++ndone;
             if (p.trace) {
                 unsigned smid;
                 asm volatile("mov.u32 %0, %%smid;\n" : "=r"(smid));
-                p.trace[ti] = TraceRec{ti, (int)smid, t0, globaltimer()};
+                p.trace[ti] = TraceRec{ti, (int)smid, t0, globaltimer(), (uint32_t)(t0 - tg),
+                                       {s_ph[0], s_ph[1], s_ph[2]}};
             }
         }
     }
+    if (threadIdx.x == 0 && ndone) atomicAdd(&p.st->done, ndone);
     if constexpr (TC) tc05::finish(&tsm);
 }
 

@@ -31,6 +31,7 @@ struct Context {
     bool use_tcgen05 = true;      // tcgen05 trailing updates in the BF16x3 factorization
     bool rec_tile = false;        // FP32 factorization: recursive tile POTRF with full tile inverses
     bool xinv_solve = true;       // FP32 substitutions with full diagonal-tile inverses
+    bool potrf_cta = false;        // one executor CTA dedicated to the diagonal-tile factorizations
     int desc_ids = 0;
     std::mutex mu;
 };

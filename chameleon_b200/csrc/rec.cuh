@@ -51,7 +51,7 @@ __device__ __forceinline__ double rsqrt_wp(double d) {
 // the first non-positive pivot (uniform across the warp); after a failure the
 // remaining steps run on a unit pivot so that the loop stays branch-free.
 template <class T>
-__device__ __forceinline__ int warp_chol32(T *S) {
+__device__ __noinline__ int warp_chol32(T *S) {
     const int lane = threadIdx.x & 31;
     T a[32];
 #pragma unroll
@@ -83,7 +83,7 @@ __device__ __forceinline__ int warp_chol32(T *S) {
 // column of L do not depend on x and issue together.  X is written in full
 // (zeros above the diagonal) at Xs (shared, ld LDS).
 template <class T>
-__device__ __forceinline__ void warp_trinv32(const T *S, T *Xs) {
+__device__ __noinline__ void warp_trinv32(const T *S, T *Xs) {
     const int lane = threadIdx.x & 31;
     T rd[32], x[32];
 #pragma unroll
@@ -127,7 +127,7 @@ __device__ __forceinline__ void small_mm32(const T *P, const T *Q, T (&o)[4]) {
 // receives the full inverse (zeros above the diagonal).  Returns LAPACK info.
 // Called by all threads; ends with a barrier.
 template <class T, bool FACT>
-__device__ int leaf64_core(T *sD, T *sX) {
+__device__ __noinline__ int leaf64_core(T *sD, T *sX) {
     __shared__ int s_info;
     const int tid = threadIdx.x, warp = tid >> 5;
     if (tid == 0) s_info = 0;
@@ -228,12 +228,22 @@ __device__ __noinline__ int leaf64(const ViewT<T> &A, const ViewT<T> &X, int n, 
 // triangle (upper untouched) and the inverted diagonal blocks (IB x IB, ld
 // IB, zero outside the block) into invd.  Returns LAPACK info.  Same
 // contract as CORE_dpotrf (coreblas/compute/core_zpotrf.c:75-81).
+// ph (optional, tracing): thread 0 adds the clock cycles spent in the block-
+// column updates, the leaves and the panels to ph[0..2].
 template <class T, int SP>
-__device__ int tile_potrf_blk(const ViewT<T> &Tv, int n, T *invd, T *smem) {
+__device__ int tile_potrf_blk(const ViewT<T> &Tv, int n, T *invd, T *smem, unsigned *ph = nullptr) {
     using CP = Cfg12864<T, SP>;
     using CD = Cfg64<T, SP>;
     T *sD = smem + CP::SMEM_ELEMS;
     T *sX = sD + IB * LDS;
+    long long c0 = (ph && threadIdx.x == 0) ? clock64() : 0;
+    auto lap = [&](int i) {
+        if (ph && threadIdx.x == 0) {
+            const long long c1 = clock64();
+            ph[i] += (unsigned)(c1 - c0);
+            c0 = c1;
+        }
+    };
     for (int jb = 0; jb < n; jb += IB) {
         const int nbk = min(IB, n - jb);
         Acc<CD> acc;
@@ -243,7 +253,9 @@ __device__ int tile_potrf_blk(const ViewT<T> &Tv, int n, T *invd, T *smem) {
         acc.for_each([&](int r, int c, T v) {
             if (r < nbk && c < nbk && r >= c) sD[r + c * LDS] -= v;
         });
+        lap(0);
         const int info = leaf64_core<T, true>(sD, sX);
+        lap(1);
         if (info) return jb + info;
         T *inv = invd + (int64_t)(jb / IB) * IB * IB;
         for (int idx = threadIdx.x; idx < IB * IB; idx += NT_CTA) {
@@ -268,6 +280,7 @@ __device__ int tile_potrf_blk(const ViewT<T> &Tv, int n, T *invd, T *smem) {
             pa.store_to(Tv.sub(r0, jb), mr, nbk);
             cta_sync();
         }
+        lap(2);
     }
     return 0;
 }

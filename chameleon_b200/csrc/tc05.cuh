@@ -210,10 +210,14 @@ __device__ __forceinline__ void split_store8(uint8_t *chunk, int r, int c0, cons
 // columns it owns (col0 = its column half), so that the epilogue's global reads
 // can be issued before the accumulator is read; epilogue then gets
 // (row, col0 + 16 p, v, p) for p = 0..3.  Call with all 256 threads.  Returns
-// false on a wait timeout.
-template <class P, class F>
+// false on a wait timeout.  idle() runs on thread 64 (otherwise idle until the
+// accumulator is ready) while the copies and MMAs run.
+struct NoIdle {
+    __device__ void operator()() const {}
+};
+template <class P, class F, class I = NoIdle>
 __device__ bool gemm_bf16x3(Smem *sm, uint8_t *stage_base, const uint8_t *a_chunks, const uint8_t *b_chunks,
-                            int nkc, P &&pre, F &&epilogue) {
+                            int nkc, P &&pre, F &&epilogue, I &&idle = I{}) {
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const uint32_t base = sm->chunks;      // k chunks issued by this CTA before this GEMM
     const uint32_t gnum = sm->gemms;       // GEMMs finished by this CTA before this one
@@ -257,6 +261,8 @@ __device__ bool gemm_bf16x3(Smem *sm, uint8_t *stage_base, const uint8_t *a_chun
             mma_commit(&sm->empty[s]);   // stage free once these MMAs have read it
         }
         mma_commit(&sm->accdone);
+    } else if (tid == 64) {
+        idle();
     }
     // epilogue: everyone waits for the accumulator
     bool ok = mbar_wait(&sm->accdone, gnum & 1);

@@ -181,3 +181,74 @@ def test_schedule_dataflow_with_full_tile_inverses(cb_host, orc, uplo, N, NB, nr
     B2 = B0.copy()
     emulate(cb_host.schedule(SOLVE | XINV | NOINV, N, NB, nrhs, NBB, 13, 2), A, B2, uplo, N, NB, NBB, xinv=True)
     assert np.allclose(B2, B, rtol=1e-12, atol=1e-14)
+
+
+def replay_two_lists(tasks, mode, N, NB, nrhs, NBB):
+    """The executor's dedicated-CTA scheme: one worker runs the POTRF tasks in
+    list order, the others run the remaining tasks in list order.  Replays the
+    two sequences greedily (whichever head's wait predicate holds goes next)
+    and asserts the run never stalls; returns the interleaved order."""
+    pot = [t for t in tasks if t[0] == TK_POTRF]
+    rest = [t for t in tasks if t[0] != TK_POTRF]
+    order, i, j = [], 0, 0
+    while i < len(pot) or j < len(rest):
+        progressed = False
+        for head_list, idx_name in ((pot, 'i'), (rest, 'j')):
+            idx = i if idx_name == 'i' else j
+            if idx < len(head_list):
+                cand = order + [head_list[idx]]
+                try:
+                    check_waits_prefix(cand, mode, N, NB, nrhs, NBB)
+                except AssertionError:
+                    continue
+                order = cand
+                if idx_name == 'i':
+                    i += 1
+                else:
+                    j += 1
+                progressed = True
+                break
+        assert progressed, "stalled at POTRF %d / task %d" % (i, j)
+    return order
+
+
+def check_waits_prefix(prefix, mode, N, NB, nrhs, NBB):
+    """check_waits on a prefix of a run (no completeness checks)."""
+    NT, NTB, tm, nbi, S = geometry(N, NB, nrhs, NBB)
+    upd = np.zeros((NT, NT), int); pan = np.zeros((NT, NT), int)
+    fwdB = np.zeros((NT, max(NTB, 1)), int); fwdD = np.zeros_like(fwdB)
+    bwdB = np.zeros_like(fwdB); bwdD = np.zeros_like(fwdB)
+    xinv = np.zeros(NT, int)
+    fact = bool(mode & FACT)
+    ns = (lambda k: nbi(k)) if mode & XINV else (lambda k: 1)
+    for kind, sub, m, n, k, bn in prefix:
+        if kind == TK_POTRF:
+            ok = upd[k, k] >= k * S(k, k); pan[k, k] += 1
+        elif kind == TK_INV:
+            ok = True; pan[k, k] += 1
+        elif kind == TK_XINV:
+            ok = (not fact) or pan[k, k] >= 1; xinv[k] += 1
+        elif kind == TK_TRSM:
+            ok = pan[k, k] >= 1 and upd[m, k] >= k * S(m, k); pan[m, k] += 1
+        elif kind == TK_UPD:
+            ok = pan[m, k] >= nbi(m) and pan[n, k] >= nbi(n) and upd[m, n] >= k * S(m, n); upd[m, n] += 1
+        elif kind == TK_FWD_TRSM:
+            inv_ok = (bool(mode & NOINV) or xinv[k] >= 1) if mode & XINV else pan[k, k] >= 1
+            ok = inv_ok and fwdB[k, bn] >= k * nbi(k); fwdD[k, bn] += 1
+        elif kind == TK_FWD_UPD:
+            ok = fwdD[k, bn] >= ns(k) and (not fact or pan[m, k] >= nbi(m)) and fwdB[m, bn] >= k * nbi(m)
+            fwdB[m, bn] += 1
+        elif kind == TK_BWD_TRSM:
+            ok = fwdD[k, bn] >= ns(k) and bwdB[k, bn] >= (NT - 1 - k) * nbi(k); bwdD[k, bn] += 1
+        else:
+            ok = bwdD[k, bn] >= ns(k) and bwdB[m, bn] >= (NT - 1 - k) * nbi(m); bwdB[m, bn] += 1
+        assert ok
+
+
+@pytest.mark.parametrize("N,NB,nrhs,NBB", [(1000, 256, 3, 256), (1100, 512, 64, 512), (300, 128, 5, 128)])
+def test_dedicated_potrf_worker_never_stalls(cb_host, N, NB, nrhs, NBB):
+    for mode, prof in ((FACT, 0), (FACT | SOLVE, 0), (FACT | SOLVE | XINV, 2)):
+        t = cb_host.schedule(mode, N, NB, nrhs if mode & SOLVE else 0, NBB, 148, prof)
+        order = replay_two_lists([tuple(int(v) for v in r) for r in t], mode, N, NB,
+                                 nrhs if mode & SOLVE else 0, NBB)
+        check_waits(np.array(order), mode, N, NB, nrhs if mode & SOLVE else 0, NBB)
