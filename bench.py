@@ -621,15 +621,20 @@ def b200_arm(args, world, rank, local):
     else:
         peak, peak_src = pk.get("fp64_tflops"), "fp64"
     achieved = mult * fact_flops / (fact_ms * 1e-3) / 1e12 if fact_ms > 0 else None
-    # DRAM bytes of the factor+solve launch: one ncu capture at N = 8192
-    # (profiles/cholesky_dag_f32_bf16x3_tcgen05_N8192.md: 750.0 MB read + 773.4 MB
-    # written), scaled by the update work (N/8192)^3 -- the traffic is dominated by
-    # the trailing updates' panel reads, which grow with the flops
-    traffic = 1.5234e9 * (N / 8192.0) ** 3 if args.precision == "bf16x3" else None
+    # DRAM bytes of the factor+solve launch from 1-pass ncu captures of the whole
+    # launch (profiles/launches_dposv_mixed_N32768.md: 91.0 GB read + 27.4 GB
+    # written at N = 32768; profiles/cholesky_dag_f32_bf16x3_tcgen05_N8192.md:
+    # 1.52 GB at N = 8192); other sizes scale the nearer capture by the update
+    # work (N/N0)^3, the traffic being dominated by the trailing updates
+    traffic, traffic_src = None, None
+    if args.precision == "bf16x3":
+        n0, b0 = (32768, 1.1841e11) if N >= 16384 else (8192, 1.5234e9)
+        traffic = b0 * (N / float(n0)) ** 3
+        traffic_src = "ncu dram__bytes_read.sum + dram__bytes_write.sum of the launch at N=%d%s" % (
+            n0, "" if N == n0 else " scaled by (N/%d)^3" % n0)
     roofline = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                 "frac": (achieved / peak) if (achieved and peak) else None, "traffic": traffic,
-                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum at N=8192 scaled by (N/8192)^3"
-                if traffic else None,
+                "traffic_source": traffic_src,
                 "kernel": "cholesky_dag_kernel<float,%s> (factorization + first solve)" % args.precision,
                 "flops_per_launch": mult * fact_flops,
                 "peak_source": peak_src + (" of measured" if peak else "")}
