@@ -68,7 +68,7 @@ typedef enum {
 #define CHAMELEON_B200_XINV_SOLVE     107 /* 1: FP32 substitutions apply full inverses of the
                                              diagonal tiles, kept across refinement solves (default) */
 #define CHAMELEON_B200_POTRF_CTA      108 /* 1: one executor CTA runs all diagonal-tile
-                                             factorizations (default) */
+                                             factorizations; 0: any CTA (default) */
 
 /* Factorization precisions for CHAMELEON_B200_PRECISION */
 #define CHAM_B200_PREC_FP64   0
