@@ -240,32 +240,14 @@ __device__ void run_task(const Task &t, const ExecParams &p, const Dims<T> &d, T
             const size_t rbytes = (size_t)p.split_nkc * 2 * tc05::CHUNK_BYTES;
             const uint8_t *a = split_tile(p, t.m, t.k) + bi * rbytes;
             const uint8_t *b = split_tile(p, t.n, t.k) + bj * rbytes;
-            // C block into L2 while the MMAs run: one prefetch per 128-byte
-            // line (32 rows) of each column
-            for (int idx = threadIdx.x; idx < 4 * cols; idx += NT_CTA) {
-                const int line = idx & 3, c = idx >> 2;
-                if (line * 32 < rows) asm volatile("prefetch.global.L2 [%0];\n" ::"l"(C.at(line * 32, c)));
-            }
-            // epilogue: each thread reads its 64 old values of C first, then
-            // subtracts the accumulator 16 columns at a time
-            float old[4][16];
-            const bool ok = tc05::gemm_bf16x3(
+            // warps 4-7 stage the old C block in TMEM while the MMAs run; the
+            // epilogue subtracts the accumulator from it
+            auto owned = [&](int r, int c) { return r < rows && c < cols && (!diag || r >= c); };
+            const bool ok = tc05::gemm_bf16x3_sub(
                 tsm, stage, a, b, p.split_nkc,
-                [&](int r, int c0) {
-#pragma unroll
-                    for (int q = 0; q < 4; ++q)
-#pragma unroll
-                        for (int i = 0; i < 16; ++i) {
-                            const int c = c0 + 16 * q + i;
-                            old[q][i] = (r < rows && c < cols && (!diag || r >= c)) ? __ldcg(C.at(r, c)) : 0.f;
-                        }
-                },
-                [&](int r, int c0, const float *v, int q) {
-#pragma unroll
-                    for (int i = 0; i < 16; ++i) {
-                        const int c = c0 + i;
-                        if (r < rows && c < cols && (!diag || r >= c)) *C.at(r, c) = old[q][i] - v[i];
-                    }
+                [&](int r, int c) { return owned(r, c) ? __ldcg(C.at(r, c)) : 0.f; },
+                [&](int r, int c, float v) {
+                    if (owned(r, c)) *C.at(r, c) = v;
                 },
                 [&]() {
                     if (ah->rel) {

@@ -29,7 +29,7 @@ constexpr int CHUNK_BYTES = 128 * BK * 2;     // one operand half (hi or lo): 16
 constexpr int STAGES = 3;
 constexpr int STAGE_BYTES = 4 * CHUNK_BYTES;  // A hi, A lo, B hi, B lo
 constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 /*alignment*/ + 256 /*barriers*/;
-constexpr int TMEM_COLS = 128;
+constexpr int TMEM_COLS = 256;   // accumulator (columns 0-127) + staged C (128-255)
 constexpr unsigned long long WAIT_NS = 2000000000ull;   // bound of one mbarrier wait (2 s)
 
 // Byte offset of element (r, c) (r < 128, c < 64) inside one swizzled chunk half.
@@ -125,6 +125,22 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
 #pragma unroll
     for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
+
+// Warp-collective store of 16 consecutive 32-bit columns of this warp's TMEM
+// lanes (v[i] -> column taddr + i of the thread's lane); complete with tmem_wait_st.
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const float *v) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};\n" ::"r"(
+            taddr),
+        "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])),
+        "r"(__float_as_uint(v[3])), "r"(__float_as_uint(v[4])), "r"(__float_as_uint(v[5])),
+        "r"(__float_as_uint(v[6])), "r"(__float_as_uint(v[7])), "r"(__float_as_uint(v[8])),
+        "r"(__float_as_uint(v[9])), "r"(__float_as_uint(v[10])), "r"(__float_as_uint(v[11])),
+        "r"(__float_as_uint(v[12])), "r"(__float_as_uint(v[13])), "r"(__float_as_uint(v[14])),
+        "r"(__float_as_uint(v[15]))
+        : "memory");
+}
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;\n" ::: "memory"); }
 
 // One warp allocates TMEM_COLS columns; the address lands in *slot.
 __device__ __forceinline__ void tmem_alloc(uint32_t *slot) {
@@ -279,6 +295,106 @@ __device__ bool gemm_bf16x3(Smem *sm, uint8_t *stage_base, const uint8_t *a_chun
             float v[16];
             tmem_ld16(sm->tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(cbase + cc), v);
             epilogue(row, cbase + cc, (const float *)v, cc >> 4);
+        }
+    }
+    fence_before_sync();
+    __syncthreads();
+    if (tid == 0) {
+        sm->chunks = base + nkc;
+        sm->gemms = gnum + 1;
+    }
+    __syncthreads();
+    return ok;
+}
+
+// C -= A * B^T for one 128 x 128 block of the executor's trailing update,
+// operands and roles as in gemm_bf16x3 (thread 0 copies, thread 32 MMAs,
+// idle() on thread 64).  The old values of C are staged in TMEM (columns
+// 128-255) by warps 4-7 while the copies and MMAs run: each of those warps
+// owns one TMEM lane quarter (32 rows), reads its 128 columns 64 at a time
+// and stores them with tcgen05.st, so no value stays in registers across the
+// roles and the producer and MMA threads never wait on C.  The epilogue (all
+// 8 warps, 64 columns each) then reads accumulator and old value from TMEM.
+// load(row, col): old value (0 where nothing is written); store(row, col, v):
+// writes where the task owns the element.  Call with all 256 threads.
+// Returns false on a wait timeout.
+template <class L, class S, class I>
+__device__ bool gemm_bf16x3_sub(Smem *sm, uint8_t *stage_base, const uint8_t *a_chunks, const uint8_t *b_chunks,
+                                int nkc, L &&load, S &&store, I &&idle) {
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint32_t base = sm->chunks;   // k chunks issued by this CTA before this GEMM
+    const uint32_t gnum = sm->gemms;    // GEMMs finished by this CTA before this one
+    __syncthreads();
+    if (tid == 0) {
+        fence_proxy_async();   // generic-proxy writes of the operands (other SMs) -> async-proxy reads
+        for (int kc = 0; kc < nkc; ++kc) {
+            const uint32_t g = base + kc;
+            const int s = g % STAGES;
+            if (g >= STAGES && !mbar_wait(&sm->empty[s], ((g / STAGES) - 1) & 1)) {
+                sm->err = 1;
+                break;
+            }
+            uint8_t *st = stage_base + s * STAGE_BYTES;
+            mbar_expect_tx(&sm->full[s], STAGE_BYTES);
+            bulk_g2s(st, a_chunks + (size_t)kc * 2 * CHUNK_BYTES, 2 * CHUNK_BYTES, &sm->full[s]);
+            bulk_g2s(st + 2 * CHUNK_BYTES, b_chunks + (size_t)kc * 2 * CHUNK_BYTES, 2 * CHUNK_BYTES, &sm->full[s]);
+        }
+    } else if (tid == 32) {
+        for (int kc = 0; kc < nkc; ++kc) {
+            const uint32_t g = base + kc;
+            const int s = g % STAGES;
+            if (!mbar_wait(&sm->full[s], (g / STAGES) & 1)) {
+                sm->err = 1;
+                break;
+            }
+            fence_after_sync();
+            uint8_t *st = stage_base + s * STAGE_BYTES;
+            const uint64_t ahi = sdesc(st), alo = sdesc(st + CHUNK_BYTES);
+            const uint64_t bhi = sdesc(st + 2 * CHUNK_BYTES), blo = sdesc(st + 3 * CHUNK_BYTES);
+#pragma unroll
+            for (int k16 = 0; k16 < BK / 16; ++k16) {
+                const uint64_t dk = (uint64_t)(k16 * 32) >> 4;   // +32 bytes inside the swizzle atom
+                const uint32_t acc0 = (kc > 0 || k16 > 0) ? 1u : 0u;
+                mma_bf16(sm->tmem, alo + dk, bhi + dk, acc0);
+                mma_bf16(sm->tmem, ahi + dk, blo + dk, 1u);
+                mma_bf16(sm->tmem, ahi + dk, bhi + dk, 1u);
+            }
+            mma_commit(&sm->empty[s]);   // stage free once these MMAs have read it
+        }
+        mma_commit(&sm->accdone);
+    } else if (tid == 64) {
+        idle();
+    } else if (warp >= 4) {
+        const int q = warp & 3, row = q * 32 + lane;
+        const uint32_t tc = sm->tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)BN;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            float v[64];
+#pragma unroll
+            for (int i = 0; i < 64; ++i) v[i] = load(row, h * 64 + i);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) tmem_st16(tc + (uint32_t)(h * 64 + j * 16), v + j * 16);
+        }
+        tmem_wait_st();
+    }
+    // epilogue: everyone waits for the accumulator
+    bool ok = mbar_wait(&sm->accdone, gnum & 1);
+    fence_before_sync();   // the staging warps' TMEM stores before the other warps' reads
+    __syncthreads();
+    if (sm->err) ok = false;
+    if (ok) {
+        fence_after_sync();
+        const int q = warp & 3;                 // TMEM lane quarter of this warp
+        const int cbase = (warp >> 2) * 64;     // column half
+        const int row = q * 32 + lane;
+        const uint32_t tl = sm->tmem + ((uint32_t)(q * 32) << 16);
+#pragma unroll
+        for (int cc = 0; cc < 64; cc += 16) {
+            float v[16], o[16];
+            tmem_ld16(tl + (uint32_t)(cbase + cc), v);
+            tmem_ld16(tl + (uint32_t)(BN + cbase + cc), o);
+#pragma unroll
+            for (int i = 0; i < 16; ++i) store(row, cbase + cc + i, o[i] - v[i]);
         }
     }
     fence_before_sync();
