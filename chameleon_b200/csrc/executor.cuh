@@ -55,7 +55,8 @@ struct TraceRec {
     int32_t task, smid;
     uint64_t t0, t1;   // globaltimer after the dependency wait, at the end of the task
     uint32_t wait_ns;  // time from taking the task to its dependencies being met
-    uint32_t ph[3];    // POTRF: clock cycles in (block-column update, leaf, panel)
+    uint32_t ph[3];    // clock cycles: POTRF in (block-column update, leaf, panel); tcgen05
+                       // update from its start to (C staged, accumulator ready, end)
 };
 
 struct ExecParams {

@@ -269,7 +269,8 @@ __device__ void run_task(const Task &t, const ExecParams &p, const Dims<T> &d, T
                     ah->have = raw < p.ntasks;
                     ah->ready = ready;
                     ah->raw = raw;
-                });
+                },
+                ph);
             if (!ok && threadIdx.x == 0) {
                 atomicCAS(&p.st->error, 0, CHAMELEON_ERR_DEVICE_TIMEOUT);
                 atomicExch(&p.st->abort, 1);

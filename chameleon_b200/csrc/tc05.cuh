@@ -316,15 +316,18 @@ __device__ bool gemm_bf16x3(Smem *sm, uint8_t *stage_base, const uint8_t *a_chun
 // roles and the producer and MMA threads never wait on C.  The epilogue (all
 // 8 warps, 64 columns each) then reads accumulator and old value from TMEM.
 // load(row, col): old value (0 where nothing is written); store(row, col, v):
-// writes where the task owns the element.  Call with all 256 threads.
-// Returns false on a wait timeout.
+// writes where the task owns the element.  ph (tracing, may be null): clock
+// cycles from the start to the staging of C being done (ph[0], warp 4), to the
+// accumulator being ready (ph[1]) and to the end (ph[2]).  Call with all 256
+// threads.  Returns false on a wait timeout.
 template <class L, class S, class I>
 __device__ bool gemm_bf16x3_sub(Smem *sm, uint8_t *stage_base, const uint8_t *a_chunks, const uint8_t *b_chunks,
-                                int nkc, L &&load, S &&store, I &&idle) {
+                                int nkc, L &&load, S &&store, I &&idle, unsigned *ph = nullptr) {
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const uint32_t base = sm->chunks;   // k chunks issued by this CTA before this GEMM
     const uint32_t gnum = sm->gemms;    // GEMMs finished by this CTA before this one
     __syncthreads();
+    const long long c_start = ph ? clock64() : 0;
     if (tid == 0) {
         fence_proxy_async();   // generic-proxy writes of the operands (other SMs) -> async-proxy reads
         for (int kc = 0; kc < nkc; ++kc) {
@@ -376,9 +379,11 @@ __device__ bool gemm_bf16x3_sub(Smem *sm, uint8_t *stage_base, const uint8_t *a_
             for (int j = 0; j < 4; ++j) tmem_st16(tc + (uint32_t)(h * 64 + j * 16), v + j * 16);
         }
         tmem_wait_st();
+        if (ph && tid == 128) ph[0] += (unsigned)(clock64() - c_start);
     }
     // epilogue: everyone waits for the accumulator
     bool ok = mbar_wait(&sm->accdone, gnum & 1);
+    if (ph && tid == 0) ph[1] += (unsigned)(clock64() - c_start);
     fence_before_sync();   // the staging warps' TMEM stores before the other warps' reads
     __syncthreads();
     if (sm->err) ok = false;
@@ -402,6 +407,7 @@ __device__ bool gemm_bf16x3_sub(Smem *sm, uint8_t *stage_base, const uint8_t *a_
     if (tid == 0) {
         sm->chunks = base + nkc;
         sm->gemms = gnum + 1;
+        if (ph) ph[2] += (unsigned)(clock64() - c_start);
     }
     __syncthreads();
     return ok;
