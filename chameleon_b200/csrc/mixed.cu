@@ -249,28 +249,58 @@ __global__ void colmax_kernel(TileMapD x, int M, int N, unsigned long long *out)
     }
 }
 
-// Infinity norm of the symmetric matrix (= one norm): per lower tile, row sums
-// (thread per row, coalesced) feed the columns of the mirrored part and column
-// sums (thread per column) feed the tile's own columns.
-__global__ void sym_absnorm_kernel(SymTiles a, double *colsum) {
+// Infinity norm (= one norm) of the symmetric matrix stored in its `uplo`
+// triangle and, when a32.base is set, the FP32 copy of that triangle's tiles,
+// in one pass over the referenced tiles only.  One CTA per stored tile (p, q)
+// of the triangle, read in its stored orientation: warp w takes stored rows
+// w*32 + lane (+256, ...) and walks the columns, so every read is one
+// coalesced 256-byte row segment.  Row sums stay in registers, column sums are
+// warp-reduced into shared memory; each goes to the row it belongs to by
+// symmetry (stored row i of tile p -> row p*NB + i, stored column j of tile q
+// -> row q*NB + j).  On a diagonal tile only the referenced triangle counts:
+// row sums without the diagonal, column sums with it.  overflow is set when a
+// referenced value does not fit FP32.  Dynamic shared memory: NB doubles.
+__global__ void __launch_bounds__(256) sym_cast_norm_kernel(SymTiles a, TileMapD a32, double *colsum,
+                                                            int *overflow) {
+    extern __shared__ double s_col[];
     int t = blockIdx.x;
     int m = 0;
-    while (t > m) { t -= m + 1; ++m; }   // t-th lower tile in row-major order
+    while (t > m) { t -= m + 1; ++m; }   // t-th lower tile (m, n) in row-major order
     const int n = t;
-    const View L = a.L(m, n);
-    const int rm = a.tm(m), cn = a.tm(n);
-    const bool diag = (m == n);
-    for (int i = threadIdx.x; i < rm; i += blockDim.x) {
-        double s = 0.0;
-        const int jmax = diag ? i : cn;          // strictly lower part of the row
-        for (int j = 0; j < jmax; ++j) s += fabs(*L.at(i, j));
-        if (s != 0.0) atomicAdd(&colsum[m * a.NB + i], s);
+    const int p = a.upper ? n : m, q = a.upper ? m : n;   // stored tile
+    const double *src = a.A + a.off[p + (int64_t)a.NT * q];
+    const int lds = a.ld[p];
+    const int rows = a.tm(p), cols = a.tm(q);
+    const bool diag = (p == q);
+    float *dst = a32.base ? static_cast<float *>(a32.base) + a32.off[p + (int64_t)a32.mt * q] : nullptr;
+    const int ldd = a32.base ? a32.ld[p] : 0;
+    for (int j = threadIdx.x; j < cols; j += blockDim.x) s_col[j] = 0.0;
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int ovf = 0;
+    for (int r0 = warp * 32; r0 < rows; r0 += 256) {
+        const int i = r0 + lane;
+        const bool rv = i < rows;
+        double rs = 0.0;
+#pragma unroll 4
+        for (int j = 0; j < cols; ++j) {
+            const double v = rv ? src[i + (int64_t)j * lds] : 0.0;
+            if (dst && rv) dst[i + (int64_t)j * ldd] = __double2float_rn(v);
+            const bool ref = rv && (!diag || (a.upper ? i <= j : i >= j));
+            const double av = ref ? fabs(v) : 0.0;
+            ovf |= av > 3.4028234663852886e38;
+            if (!diag || i != j) rs += av;
+            double cs = av;
+#pragma unroll
+            for (int o = 16; o; o >>= 1) cs += __shfl_xor_sync(0xffffffffu, cs, o);
+            if (lane == 0 && cs != 0.0) atomicAdd(&s_col[j], cs);
+        }
+        if (rv && rs != 0.0) atomicAdd(&colsum[(int64_t)p * a.NB + i], rs);
     }
-    for (int j = threadIdx.x; j < cn; j += blockDim.x) {
-        double s = 0.0;
-        for (int i = diag ? j : 0; i < rm; ++i) s += fabs(*L.at(i, j));
-        atomicAdd(&colsum[n * a.NB + j], s);
-    }
+    __syncthreads();
+    for (int j = threadIdx.x; j < cols; j += blockDim.x)
+        if (s_col[j] != 0.0) atomicAdd(&colsum[(int64_t)q * a.NB + j], s_col[j]);
+    if (ovf && overflow) *overflow = 1;
 }
 
 static int ew_grid(int64_t total) {
@@ -342,11 +372,17 @@ static SymTiles symtiles(CHAM_desc_t *A, cham_uplo_t uplo, double *diag = nullpt
                     diag};
 }
 
-double sym_norm_inf(CHAM_desc_t *A, cham_uplo_t uplo, cudaStream_t s, MixedWs &m) {
+// ||A||_inf of the symmetric A (its `uplo` triangle); with a32 (same tiling as
+// A) the referenced tiles are cast into it in the same pass, overflow flagged
+// in *ovf.  Also makes the symmetric diagonal-tile copies for the residuals.
+double sym_norm_inf(CHAM_desc_t *A, cham_uplo_t uplo, cudaStream_t s, MixedWs &m, CHAM_desc_t *a32, int *ovf) {
     if (desc_upload(A) || mixed_reserve(m, A->n, A->nb, std::max(1, m.nrhs))) return -1.0;
+    if (a32 && (desc_upload(a32) || a32->nb != A->nb || a32->mb != A->mb || a32->mt != A->nt)) return -1.0;
     const int NT = A->nt;
     cudaMemsetAsync(m.colsum, 0, A->n * sizeof(double), s);
-    sym_absnorm_kernel<<<NT * (NT + 1) / 2, 256, 0, s>>>(symtiles(A, uplo), m.colsum);
+    const TileMapD t32 = a32 ? tmap(a32) : TileMapD{nullptr, nullptr, nullptr, 0, 0, 0};
+    sym_cast_norm_kernel<<<NT * (NT + 1) / 2, 256, A->nb * sizeof(double), s>>>(symtiles(A, uplo), t32, m.colsum,
+                                                                              ovf);
     // symmetric copies of the diagonal tiles for the residuals of this solve
     sym_diag_kernel<<<dim3(std::max(1, std::min(64, (A->nb * A->nb + 255) / 256)), NT), 256, 0, s>>>(
         symtiles(A, uplo, m.diag));
@@ -514,12 +550,14 @@ int mixed_posv_ws(cham_uplo_t uplo, int precision, CHAM_desc_t *A, CHAM_desc_t *
     if (!fallback) {
         if ((rc = desc_upload(A)) || (rc = desc_upload(B)) || (rc = desc_upload(X))) return rc;
         clk.tic();
-        const double anrm = sym_norm_inf(A, uplo, s, m);
+        CHB_CUDA(cudaMemsetAsync(m.flag, 0, sizeof(int), s));
+        if ((rc = cast_desc(B, m.B32, s, m.flag))) return rc;
+        // the norm pass also casts A's referenced tiles to FP32 (unless the
+        // FP32 factor is kept from an earlier call)
+        const double anrm = sym_norm_inf(A, uplo, s, m, factored ? nullptr : m.A32, m.flag);
+        if (anrm < 0) return CHAMELEON_ERR_UNEXPECTED;
         const double cte = anrm * 1.1102230246251565e-16 * sqrt((double)N);
         const int split = (precision == CHAM_B200_PREC_FP32) ? SPLIT_TF32X3 : SPLIT_BF16X3;
-        CHB_CUDA(cudaMemsetAsync(m.flag, 0, sizeof(int), s));
-        if (!factored && (rc = cast_desc(A, m.A32, s, m.flag))) return rc;
-        if ((rc = cast_desc(B, m.B32, s, m.flag))) return rc;
         int ovf = 0;
         CHB_CUDA(cudaMemcpyAsync(&ovf, m.flag, sizeof(int), cudaMemcpyDeviceToHost, s));
         clk.toc(st.cast_ms);

@@ -89,6 +89,22 @@ def test_mixed_overflow_in_cast_falls_back(cb):
     assert np.allclose(X, 1.0)
 
 
+@pytest.mark.parametrize("uplo", [121, 122])
+def test_mixed_huge_values_outside_the_triangle_are_not_read(cb, orc, uplo):
+    """Only the uplo triangle is referenced: values that do not fit FP32 in the
+    other one neither trigger the overflow fallback nor change the norm."""
+    N, NB = 700, 256
+    A0 = orc.dplgsy(float(N), N, 61)
+    B0 = orc.dplrnt(N, 3, 62)
+    Ain = np.array(A0, order="F")
+    other = np.triu_indices(N, 1) if uplo == 122 else np.tril_indices(N, -1)
+    Ain[other] = 1e39
+    rc, info, X, _ = solve_mixed(cb, uplo, 2, Ain, B0, NB)
+    assert rc == 0
+    assert 0 <= info.iterations <= 6 and info.fallback == 0
+    assert np_check_solve(A0, X, B0) < 60
+
+
 def test_mixed_not_spd_reports_info(cb, orc):
     N, NB = 300, 128
     A0 = orc.dplgsy(float(N), N, 2)
