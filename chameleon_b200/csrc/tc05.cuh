@@ -311,7 +311,7 @@ __device__ bool gemm_bf16x3(Smem *sm, uint8_t *stage_base, const uint8_t *a_chun
 // operands and roles as in gemm_bf16x3 (thread 0 copies, thread 32 MMAs,
 // idle() on thread 64).  The old values of C are staged in TMEM (columns
 // 128-255) by warps 4-7 while the copies and MMAs run: each of those warps
-// owns one TMEM lane quarter (32 rows), reads its 128 columns 64 at a time
+// owns one TMEM lane quarter (32 rows), reads its 128 columns 32 at a time
 // and stores them with tcgen05.st, so no value stays in registers across the
 // roles and the producer and MMA threads never wait on C.  The epilogue (all
 // 8 warps, 64 columns each) then reads accumulator and old value from TMEM.
@@ -371,12 +371,12 @@ __device__ bool gemm_bf16x3_sub(Smem *sm, uint8_t *stage_base, const uint8_t *a_
         const int q = warp & 3, row = q * 32 + lane;
         const uint32_t tc = sm->tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)BN;
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            float v[64];
+        for (int h = 0; h < 4; ++h) {
+            float v[32];
 #pragma unroll
-            for (int i = 0; i < 64; ++i) v[i] = load(row, h * 64 + i);
+            for (int i = 0; i < 32; ++i) v[i] = load(row, h * 32 + i);
 #pragma unroll
-            for (int j = 0; j < 4; ++j) tmem_st16(tc + (uint32_t)(h * 64 + j * 16), v + j * 16);
+            for (int j = 0; j < 2; ++j) tmem_st16(tc + (uint32_t)(h * 32 + j * 16), v + j * 16);
         }
         tmem_wait_st();
         if (ph && tid == 128) ph[0] += (unsigned)(clock64() - c_start);
