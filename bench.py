@@ -622,13 +622,13 @@ def b200_arm(args, world, rank, local):
         peak, peak_src = pk.get("fp64_tflops"), "fp64"
     achieved = mult * fact_flops / (fact_ms * 1e-3) / 1e12 if fact_ms > 0 else None
     # DRAM bytes of the factor+solve launch from 1-pass ncu captures of the whole
-    # launch (profiles/launches_dposv_mixed_N32768.md: 91.0 GB read + 27.4 GB
+    # launch (profiles/launches_dposv_mixed_N32768.md: 89.95 GB read + 26.10 GB
     # written at N = 32768; profiles/cholesky_dag_f32_bf16x3_tcgen05_N8192.md:
     # 1.52 GB at N = 8192); other sizes scale the nearer capture by the update
     # work (N/N0)^3, the traffic being dominated by the trailing updates
     traffic, traffic_src = None, None
     if args.precision == "bf16x3":
-        n0, b0 = (32768, 1.1841e11) if N >= 16384 else (8192, 1.5234e9)
+        n0, b0 = (32768, 1.1605e11) if N >= 16384 else (8192, 1.5234e9)
         traffic = b0 * (N / float(n0)) ** 3
         traffic_src = "ncu dram__bytes_read.sum + dram__bytes_write.sum of the launch at N=%d%s" % (
             n0, "" if N == n0 else " scaled by (N/%d)^3" % n0)
