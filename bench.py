@@ -179,8 +179,9 @@ def reference_arm(args, world, rank):
     return line
 
 
-def cpu_baseline_sample():
-    """The reference's dposv on the host cores on a bounded sample (N=8192)."""
+def cpu_baseline_sample(N, NB, nrhs):
+    """The reference's dposv on the host cores, on the bench's own problem
+    (one or more complete solves, stopping once 30 s of CPU time are spent)."""
     try:
         from oracle import oracle as O
         if not O.reference_available():
@@ -188,7 +189,6 @@ def cpu_baseline_sample():
         cores = os.cpu_count() or 1
         os.environ["OPENBLAS_NUM_THREADS"] = "1"
         L = O.reference(cores)
-        N, NB, nrhs = 8192, NB_DEF, NRHS_DEF
         A0 = np.zeros((N, N), order="F")
         B0 = np.zeros((N, nrhs), order="F")
         L.chamref_dplgsy(float(N), 123, N, O._ptr(A0), N, NB, SEED_A)
@@ -202,12 +202,13 @@ def cpu_baseline_sample():
             L.chamref_dposv(122, N, nrhs, NB, O._ptr(A), N, O._ptr(B), N, ctypes.byref(t))
             best = t.value if best is None else min(best, t.value)
             t_total += t.value
-            if t_total > 30:
+            if t_total + t.value > 30:   # the next solve would pass the 30 s bound
                 break
         val = dposv_flops(N, nrhs) / best / 1e12
         return {"value": val, "unit": "TFLOP/s", "cores": cores, "kind": "reference",
-                "sample": "reference dposv N=%d NB=%d nrhs=%d (best of <=3, %.1f s CPU); reference OpenMP runtime "
-                          "+ OpenBLAS, all host cores" % (N, NB, nrhs, t_total)}
+                "sample": "reference dposv N=%d NB=%d nrhs=%d, the bench's workload (best of <=3 solves, stopped "
+                          "after 30 s: %.1f s CPU); reference OpenMP runtime + OpenBLAS, all host cores"
+                          % (N, NB, nrhs, t_total)}
     except Exception as e:   # the baseline is reported, not required
         return {"value": None, "unit": "TFLOP/s", "cores": os.cpu_count(), "kind": "reference",
                 "sample": "failed: %s" % e}
@@ -622,10 +623,10 @@ def b200_arm(args, world, rank, local):
         peak, peak_src = pk.get("fp64_tflops"), "fp64"
     achieved = mult * fact_flops / (fact_ms * 1e-3) / 1e12 if fact_ms > 0 else None
     # DRAM bytes of the factor+solve launch from 1-pass ncu captures of the whole
-    # launch (profiles/launches_dposv_mixed_N32768.md: 89.95 GB read + 26.10 GB
-    # written at N = 32768; profiles/cholesky_dag_f32_bf16x3_tcgen05_N8192.md:
-    # 1.52 GB at N = 8192); other sizes scale the nearer capture by the update
-    # work (N/N0)^3, the traffic being dominated by the trailing updates
+    # launch (dram__bytes_read.sum + dram__bytes_write.sum: 89.95 GB + 26.10 GB
+    # at N = 32768, 1.52 GB at N = 8192); other sizes scale the nearer capture
+    # by the update work (N/N0)^3, the traffic being dominated by the trailing
+    # updates
     traffic, traffic_src = None, None
     if args.precision == "bf16x3":
         n0, b0 = (32768, 1.1605e11) if N >= 16384 else (8192, 1.5234e9)
@@ -641,6 +642,7 @@ def b200_arm(args, world, rank, local):
 
     # plain FP64 path on the same problem (reported beside the mixed number)
     fp64 = None
+    ferr = None
     if args.compare_fp64 and rank == 0:
         dA2 = cb.Desc.create(N, N, NB)
         dB2 = cb.Desc.create(N, nrhs, NB)
@@ -651,6 +653,11 @@ def b200_arm(args, world, rank, local):
         L.CHAM_B200_Event_Record(3)
         fms = L.CHAM_B200_Event_Elapsed(2, 3)
         fp64 = {"tflops": flops / (fms * 1e-3) / 1e12, "ms": fms}
+        # forward error of the mixed solution against the plain FP64 one (same
+        # inputs on rank 0)
+        X64 = dB2.to_numpy()
+        Xm = dX.to_numpy()
+        ferr = float(np.abs(Xm - X64).max() / np.abs(X64).max())
         dA2.destroy()
         dB2.destroy()
 
@@ -687,7 +694,7 @@ def b200_arm(args, world, rank, local):
     cond = conditioning_section(args, cb, rank) if args.cond else None
     batch = batch_section(args, cb, world, rank) if args.batch else None
     serving = serve_section(args, cb, rank) if args.serve else None
-    cpu = cpu_baseline_sample() if (rank == 0 and not args.no_cpu) else None
+    cpu = cpu_baseline_sample(N, NB, nrhs) if (rank == 0 and not args.no_cpu) else None
     line = {
         "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -699,6 +706,8 @@ def b200_arm(args, world, rank, local):
                    "l2": "inputs larger than L2 (A is %.1f GB FP64)" % (8 * N * N / 1e9),
                    "parallelism": "replicas x%d" % world},
         "refine": {"iterations": iters, "backward_error_max": max(berrs) if berrs else None,
+                   "backward_error_def": "max_j ||b_j - A x_j||_inf / (||A||_inf ||x_j||_inf) of the returned x",
+                   "forward_error_vs_fp64": ferr,
                    "phases_ms": {"factor+solve": stats[0], "refine_solves": stats[1], "residuals": stats[2],
                                  "casts+norm": stats[3], "total": stats[4]}},
         "fp64_plain": fp64,
@@ -727,7 +736,8 @@ def main():
     ap.add_argument("--nb", type=int, default=NB_DEF)
     ap.add_argument("--nrhs", type=int, default=NRHS_DEF)
     ap.add_argument("--precision", default="bf16x3", choices=["bf16x3", "fp32", "fp64"])
-    ap.add_argument("--ref-n", type=int, default=16384, help="order of the reference arm's per-step sample")
+    ap.add_argument("--ref-n", type=int, default=None,
+                    help="order of the reference arm's per-step solve (default: --n, the same workload)")
     ap.add_argument("--no-e2e", dest="e2e", action="store_false")
     ap.add_argument("--no-fp64", dest="compare_fp64", action="store_false")
     ap.add_argument("--no-cpu", action="store_true")
@@ -745,6 +755,8 @@ def main():
     ap.add_argument("--serve-cap-requests", type=int, default=300)
     ap.add_argument("--serve-plain", type=int, default=100, help="requests timed through CHAMELEON_dsposv")
     args = ap.parse_args()
+    if args.ref_n is None:
+        args.ref_n = args.n
     world, rank, local = dist_setup(args.gpus)
     try:
         if args.impl == "reference":

@@ -34,6 +34,10 @@ CHAMELEON_B200_TCGEN05 = 105
 CHAMELEON_B200_REC_TILE = 106
 CHAMELEON_B200_XINV_SOLVE = 107
 CHAMELEON_B200_POTRF_CTA = 108
+CHAMELEON_B200_UPD_GROUP_F64 = 109
+CHAMELEON_B200_UPD_GROUP_F32 = 110
+CHAMELEON_B200_UPD_GROUP_TC = 111
+CHAMELEON_B200_FACTOR_NB = 112
 PREC_FP64, PREC_FP32, PREC_BF16X3 = 0, 1, 2
 CHAMELEON_SUCCESS = 0
 CHAMELEON_ERR_NOT_INITIALIZED = -101
@@ -76,7 +80,7 @@ class RefineInfo(ctypes.Structure):
 
 class Task(ctypes.Structure):
     _fields_ = [("kind", ctypes.c_int16), ("sub", ctypes.c_int16), ("m", ctypes.c_int16),
-                ("n", ctypes.c_int16), ("k", ctypes.c_int16), ("bn", ctypes.c_int16), ("pad", ctypes.c_int32)]
+                ("n", ctypes.c_int16), ("k", ctypes.c_int16), ("bn", ctypes.c_int16), ("grp", ctypes.c_int32)]
 
 
 class Request(ctypes.Structure):
@@ -151,6 +155,7 @@ PROTOS = {
     "CUDA_dsyrk": (_i, [_i, _i, _i, _i, _dp, _vp, _i, _dp, _vp, _i, _vp]),
     "CUDA_dtrsm": (_i, [_i, _i, _i, _i, _i, _i, _dp, _vp, _i, _vp, _i, _vp]),
     "CUDA_dpotrf": (_i, [_i, _i, _vp, _i, _vp, _i, _vp, _vp]),
+    "CUDA_spotrf": (_i, [_i, _i, _vp, _i, _vp, _i, _vp, _vp]),
     "CUDA_dpotrf_noalloc": (_i, [_i, _i, _vp, _i, _vp, _vp]),
     "CUDA_dplgsy": (_i, [_dp, _i, _i, _vp, _i, _i, _i, _i, _ull, _vp]),
     "CUDA_dplrnt": (_i, [_i, _i, _vp, _i, _i, _i, _i, _ull, _vp]),
@@ -170,8 +175,8 @@ EXTRAS = {
     "CHAM_B200_Handle_Overflow": (_i, [_vp]),
     "CHAM_B200_Trace_Enable": (_i, [_i]),
     "CHAM_B200_Trace_Read": (_i, [_vp, _i]),
-    "CHAM_B200_Schedule_Size": (_i, [_i, _i, _i, _i, _i, _i, _i]),
-    "CHAM_B200_Schedule_Build": (_i, [_i, _i, _i, _i, _i, _i, _i, ctypes.POINTER(Task), _i]),
+    "CHAM_B200_Schedule_Size": (_i, [_i, _i, _i, _i, _i, _i, _i, _i]),
+    "CHAM_B200_Schedule_Build": (_i, [_i, _i, _i, _i, _i, _i, _i, _i, ctypes.POINTER(Task), _i]),
     "CHAM_B200_dposv_timed": (_i, [_i, _i, _i, _vp, _i, _vp, _i, ctypes.POINTER(ctypes.c_float)]),
     "CHAM_B200_Event_Record": (_i, [_i]),
     "CHAM_B200_Event_Elapsed": (ctypes.c_float, [_i, _i]),
@@ -375,17 +380,19 @@ def dsposv(uplo, N, NRHS, A, LDA, B, LDB, X, LDX):
 PROF_FP64, PROF_F32_MMA, PROF_F32_TC05 = 0, 1, 2
 
 
-def schedule(mode, N, NB, nrhs=0, NBB=None, workers=148, prof=PROF_FP64):
-    """The executor's task list for a shape and cost profile (host-only; no GPU needed)."""
+def schedule(mode, N, NB, nrhs=0, NBB=None, workers=148, prof=PROF_FP64, kgroup=1):
+    """The executor's task list for a shape, cost profile and update group
+    size (host-only; no GPU needed): rows (kind, sub, m, n, k, bn, grp)."""
     L = lib()
     NBB = NB if NBB is None else NBB
-    n = L.CHAM_B200_Schedule_Size(mode, N, NB, nrhs, NBB, workers, prof)
+    n = L.CHAM_B200_Schedule_Size(mode, N, NB, nrhs, NBB, workers, prof, kgroup)
     buf = (Task * max(n, 1))()
-    got = L.CHAM_B200_Schedule_Build(mode, N, NB, nrhs, NBB, workers, prof, buf, n)
+    got = L.CHAM_B200_Schedule_Build(mode, N, NB, nrhs, NBB, workers, prof, kgroup, buf, n)
     if got != n:
         raise ChameleonError("schedule build returned %d of %d" % (got, n))
-    arr = np.frombuffer(buf, dtype=np.int16).reshape(-1, 8)[:n]
-    return arr[:, :6].copy()   # kind, sub, m, n, k, bn
+    raw = np.frombuffer(buf, dtype=np.int16).reshape(-1, 8)[:n]
+    grp = raw[:, 6:8].copy().view(np.int32)
+    return np.concatenate([raw[:, :6].astype(np.int32), grp], axis=1)
 
 
 class Server:

@@ -38,6 +38,17 @@ int ensure_init() {
         fprintf(stderr, "CHAMELEON_B200 ERROR: CHAMELEON not initialized\n");
         return CHAMELEON_ERR_NOT_INITIALIZED;
     }
+    // The entry points compute on the library's own non-blocking stream, which
+    // the legacy default stream does not order.  A caller that filled its
+    // device matrix with work on the default stream (an asynchronous copy, a
+    // kernel of its own) must see that work finish before the call reads the
+    // matrix, as with a synchronous library: make the stream wait for
+    // everything the default stream holds at the time of the call.
+    if (c.order_event && (cudaEventRecord(c.order_event, cudaStreamLegacy) != cudaSuccess ||
+                          cudaStreamWaitEvent(c.stream, c.order_event, 0) != cudaSuccess)) {
+        cudaGetLastError();
+        return CHAMELEON_ERR_UNEXPECTED;
+    }
     return 0;
 }
 
@@ -364,6 +375,7 @@ int __chameleon_init(int nworkers, int ncudas) {
     CHB_CUDA(cudaGetDevice(&c.device));
     CHB_CUDA(cudaDeviceGetAttribute(&c.num_sms, cudaDevAttrMultiProcessorCount, c.device));
     CHB_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
+    CHB_CUDA(cudaEventCreateWithFlags(&c.order_event, cudaEventDisableTiming));
     if (const char *s = getenv("CHAMELEON_TILE_SIZE")) c.tile_size = std::max(1, atoi(s));
     if (const char *s = getenv("CHAMELEON_B200_PRECISION")) {
         if (!strcmp(s, "fp64")) c.precision = CHAM_B200_PREC_FP64;
@@ -425,6 +437,18 @@ int CHAMELEON_Set(int param, int value) {
     case CHAMELEON_B200_POTRF_CTA:
         c.potrf_cta = (value != 0);
         return 0;
+    case CHAMELEON_B200_UPD_GROUP_F64:
+    case CHAMELEON_B200_UPD_GROUP_F32:
+    case CHAMELEON_B200_UPD_GROUP_TC:
+        if (value < 1 || value > 64) return CHAMELEON_ERR_ILLEGAL_VALUE;
+        (param == CHAMELEON_B200_UPD_GROUP_F64 ? c.kgroup_f64
+                                               : param == CHAMELEON_B200_UPD_GROUP_F32 ? c.kgroup_f32 : c.kgroup_tc) =
+            value;
+        return 0;
+    case CHAMELEON_B200_FACTOR_NB:
+        if (value < 0 || (value > 0 && value % 64 != 0)) return CHAMELEON_ERR_ILLEGAL_VALUE;
+        c.factor_nb = value;
+        return 0;
     case CHAMELEON_TRANSLATION_MODE:
     case CHAMELEON_LOOKAHEAD:
     case CHAMELEON_CONCURRENCY:
@@ -447,6 +471,10 @@ int CHAMELEON_Get(int param, int *value) {
     case CHAMELEON_B200_REC_TILE: *value = c.rec_tile ? 1 : 0; return 0;
     case CHAMELEON_B200_XINV_SOLVE: *value = c.xinv_solve ? 1 : 0; return 0;
     case CHAMELEON_B200_POTRF_CTA: *value = c.potrf_cta ? 1 : 0; return 0;
+    case CHAMELEON_B200_UPD_GROUP_F64: *value = c.kgroup_f64; return 0;
+    case CHAMELEON_B200_UPD_GROUP_F32: *value = c.kgroup_f32; return 0;
+    case CHAMELEON_B200_UPD_GROUP_TC: *value = c.kgroup_tc; return 0;
+    case CHAMELEON_B200_FACTOR_NB: *value = c.factor_nb; return 0;
     }
     return CHAMELEON_ERR_ILLEGAL_VALUE;
 }

@@ -34,32 +34,36 @@ namespace {
 // panel tasks).  Multipliers of the flop model, calibrated from per-task
 // device traces at NB = 512 (POTRF, TRSM, UPD, FWD/BWD TRSM, FWD/BWD UPD).
 enum CostProfile : int { PROF_FP64 = 0, PROF_F32_MMA = 1, PROF_F32_TC05 = 2 };
+// upd_fix: the fixed cost of one update task (C read and write, dispatch) in
+// units of one panel's product, so that a group of cnt panels costs
+// upd * (cnt + upd_fix) / (1 + upd_fix).
 struct Calib {
-    double potrf, trsm, upd, strsm, supd;
+    double potrf, trsm, upd, strsm, supd, upd_fix;
 };
 static const Calib kCalib[3] = {
-    {4.9, 4.7, 5.8, 3.9, 7.1},   // FP64 DMMA
-    {4.0, 4.7, 2.1, 2.4, 3.3},   // FP32, split products on mma.sync
-    {4.2, 2.7, 0.92, 1.9, 4.0},  // FP32, tcgen05 updates, full-inverse substitutions (row-block sub-tasks)
+    {4.9, 4.7, 5.8, 3.9, 7.1, 0.05},   // FP64 DMMA
+    {4.0, 4.7, 2.1, 2.4, 3.3, 0.2},    // FP32, split products on mma.sync
+    {4.2, 2.7, 0.92, 1.9, 4.0, 0.6},   // FP32, tcgen05 updates, full-inverse substitutions (row-block sub-tasks)
 };
 
 struct Shape {
-    int mode, N, NB, nrhs, NBB, P, prof;
+    int mode, N, NB, nrhs, NBB, P, prof, G;   // G: update group size (upd_group_of)
     bool operator==(const Shape &o) const {
         return mode == o.mode && N == o.N && NB == o.NB && nrhs == o.nrhs && NBB == o.NBB && P == o.P &&
-               prof == o.prof;
+               prof == o.prof && G == o.G;
     }
 };
 struct ShapeHash {
     size_t operator()(const Shape &s) const {
         size_t h = 1469598103934665603ull;
-        for (int v : {s.mode, s.N, s.NB, s.nrhs, s.NBB, s.P, s.prof}) h = (h ^ (size_t)v) * 1099511628211ull;
+        for (int v : {s.mode, s.N, s.NB, s.nrhs, s.NBB, s.P, s.prof, s.G}) h = (h ^ (size_t)v) * 1099511628211ull;
         return h;
     }
 };
 
 struct Coarse {
-    int16_t kind, m, n, k, bn;
+    int16_t kind, m, n, k, bn;   // TK_UPD: k = first panel of the group, bn = panel count
+    int grp;                     // TK_UPD: index of the group in tile column n
     int nsub;
     double dur;               // duration of one sub-task (model units)
     std::vector<int> succ;
@@ -86,7 +90,7 @@ std::vector<Task> build_order(const Shape &s) {
     ct.reserve(fact ? (size_t)NT * NT * NT / 6 + 4 * NT * NT : 4 * NT * NT + 8);
     auto add = [&](int kind, int m, int n, int k, int bn, int nsub, double dur) {
         Coarse c;
-        c.kind = kind; c.m = m; c.n = n; c.k = k; c.bn = bn; c.nsub = nsub; c.dur = dur;
+        c.kind = kind; c.m = m; c.n = n; c.k = k; c.bn = bn; c.grp = 0; c.nsub = nsub; c.dur = dur;
         ct.push_back(c);
         return (int)ct.size() - 1;
     };
@@ -115,10 +119,17 @@ std::vector<Task> build_order(const Shape &s) {
                 edge(lastU[m + (size_t)NT * k], id);
                 Tr[m + (size_t)NT * k] = id;
             }
+            // the update groups of each later tile column whose last panel is k
+            // (upd_group_of): they become ready with this step's panel solves
             for (int n = k + 1; n < NT; ++n) {
+                int k0, cnt, gi;
+                upd_group_of(n, k, s.G, &k0, &cnt, &gi);
+                if (k0 + cnt - 1 != k) continue;
                 for (int m = n; m < NT; ++m) {
                     const int sub = (m == n) ? nbi(m) * (nbi(m) + 1) / 2 : nbi(m) * nbi(n);
-                    const int id = add(TK_UPD, m, n, k, 0, sub, cal.upd * 1.0 * SUBB * SUBB * nb * 2.0);
+                    const double dur = cal.upd * SUBB * SUBB * nb * 2.0 * (cnt + cal.upd_fix) / (1.0 + cal.upd_fix);
+                    const int id = add(TK_UPD, m, n, k0, cnt, sub, dur);
+                    ct[id].grp = gi;
                     edge(Tr[m + (size_t)NT * k], id);
                     if (m != n) edge(Tr[n + (size_t)NT * k], id);
                     edge(lastU[m + (size_t)NT * n], id);
@@ -195,7 +206,7 @@ std::vector<Task> build_order(const Shape &s) {
     double now = 0;
     auto emit = [&](const Coarse &c, int j) {
         Task t{};
-        t.kind = c.kind; t.m = c.m; t.n = c.n; t.k = c.k; t.bn = c.bn; t.sub = 0;
+        t.kind = c.kind; t.m = c.m; t.n = c.n; t.k = c.k; t.bn = c.bn; t.sub = 0; t.grp = c.grp;
         if (c.kind == TK_UPD) {
             const int a = nbi(c.m);
             int bi = 0, bj = 0;
@@ -359,7 +370,10 @@ int run_cholesky_dag(int mode, cham_uplo_t uplo, CHAM_desc_t *A, CHAM_desc_t *B,
     // block's width rounded up to 16, so that the costs stay close and the
     // number of distinct schedules stays small
     const int canonR = nrhs ? (NTB - 1) * NBB + std::min(NBB, ((nrhs - (NTB - 1) * NBB + 15) / 16) * 16) : 0;
-    Shape sh{mode, canonN, NB, canonR, NBB, grid, prof};
+    // update group size: fused k steps amortize the C round trip and the
+    // dispatch of an update over G panels (CHAMELEON_B200_UPD_GROUP per path)
+    const int G = std::max(1, prof == PROF_FP64 ? c.kgroup_f64 : (tc ? c.kgroup_tc : c.kgroup_f32));
+    Shape sh{mode, canonN, NB, canonR, NBB, grid, prof, G};
     Schedule *sch = get_schedule(sh);
     if (!sch) return CHAMELEON_ERR_OUT_OF_RESOURCES;
     const int NIB = (NB + IB - 1) / IB;
@@ -429,6 +443,7 @@ int run_cholesky_dag(int mode, cham_uplo_t uplo, CHAM_desc_t *A, CHAM_desc_t *B,
     p.st = w.st;
     p.trace = (g_trace_buf && g_trace_cap >= p.ntasks) ? g_trace_buf : nullptr;
     p.wait_budget_ns = (unsigned long long)c.wait_budget_us * 1000ull;
+    p.kgroup = G;
     if (tc) {
         p.split_nrb = (NB + SUBB - 1) / SUBB;
         p.split_nkc = NB / tc05::BK;
@@ -503,16 +518,16 @@ extern "C" int CHAM_B200_Trace_Read(void *host_out, int count) {
 }
 // Copy the schedule of a shape into `out` (host only; used by the CPU tests of
 // the DAG logic and by the trace tooling).  Returns the task count written.
-extern "C" int CHAM_B200_Schedule_Build(int mode, int N, int NB, int nrhs, int NBB, int workers, int prof,
+extern "C" int CHAM_B200_Schedule_Build(int mode, int N, int NB, int nrhs, int NBB, int workers, int prof, int kgroup,
                                         void *out, int cap) {
     using namespace chb;
-    const std::vector<Task> t = build_order(Shape{mode, N, NB, nrhs, NBB, workers, prof});
+    const std::vector<Task> t = build_order(Shape{mode, N, NB, nrhs, NBB, workers, prof, std::max(1, kgroup)});
     const int n = std::min<int>((int)t.size(), cap);
     memcpy(out, t.data(), sizeof(Task) * (size_t)n);
     return n;
 }
 // Number of tasks of the schedule of a given shape (for tests and tracing).
-extern "C" int CHAM_B200_Schedule_Size(int mode, int N, int NB, int nrhs, int NBB, int workers, int prof) {
+extern "C" int CHAM_B200_Schedule_Size(int mode, int N, int NB, int nrhs, int NBB, int workers, int prof, int kgroup) {
     using namespace chb;
-    return (int)build_order(Shape{mode, N, NB, nrhs, NBB, workers, prof}).size();
+    return (int)build_order(Shape{mode, N, NB, nrhs, NBB, workers, prof, std::max(1, kgroup)}).size();
 }

@@ -17,7 +17,7 @@ namespace chb {
 enum TaskKind : int16_t {
     TK_POTRF = 1,     // factor diagonal tile k, invert its inner diagonal blocks
     TK_TRSM = 2,      // panel row block: A(m,k) <- A(m,k) L(k,k)^{-T}
-    TK_UPD = 3,       // trailing sub-block: A(m,n) -= A(m,k) A(n,k)^T (SYRK when m == n)
+    TK_UPD = 3,       // trailing sub-block: A(m,n) -= sum_{k in group} A(m,k) A(n,k)^T (SYRK when m == n)
     TK_FWD_TRSM = 4,  // B(k) <- L(k,k)^{-1} B(k)
     TK_FWD_UPD = 5,   // B(m) -= L(m,k) B(k)            (m > k)
     TK_BWD_TRSM = 6,  // B(k) <- L(k,k)^{-T} B(k)
@@ -26,11 +26,37 @@ enum TaskKind : int16_t {
     TK_XINV = 9,      // full inverse of diagonal tile k (FP32 substitution steps)
 };
 
+// TK_UPD applies the panels k .. k + bn - 1 of one k group (one accumulator,
+// one write of the sub-block); `grp` is the group's position among the update
+// groups of tile column n (upd_group_of), i.e. how many groups precede it.
 struct Task {
     int16_t kind, sub;   // sub: row block (TRSM / *_UPD on B) or (bi | bj << 8) (TK_UPD)
-    int16_t m, n, k, bn;
-    int32_t pad;
+    int16_t m, n, k, bn; // bn: right-hand-side tile column, or (TK_UPD) the group's panel count
+    int32_t grp;         // TK_UPD: index of the group in tile column n
 };
+
+// Update groups of tile column n (n >= 1): the panels k < n that update tile
+// (m, n), m >= n, are applied in groups.  The last one, k = n - 1, is a group
+// of its own (it is on the critical path of step n); the others form groups of
+// G consecutive panels aligned at multiples of G ([0, G), [G, 2G), ...), the
+// last of them ending at n - 1.  Number of groups of column n:
+__host__ __device__ __forceinline__ int upd_ngroups(int n, int G) {
+    return n <= 0 ? 0 : (n - 1 + G - 1) / G + 1;
+}
+// The group of column n (n > k) that panel k belongs to: first panel, panel
+// count and index.
+__host__ __device__ __forceinline__ void upd_group_of(int n, int k, int G, int *k0, int *cnt, int *idx) {
+    if (k == n - 1) {
+        *k0 = k;
+        *cnt = 1;
+        *idx = upd_ngroups(n, G) - 1;
+    } else {
+        const int g = k / G;
+        *k0 = g * G;
+        *cnt = ((g + 1) * G < n - 1 ? (g + 1) * G : n - 1) - *k0;
+        *idx = g;
+    }
+}
 static_assert(sizeof(Task) == 16, "Task is 16 bytes");
 
 // MODE_XINV: the substitution steps apply full inverses of the diagonal tiles
@@ -92,6 +118,7 @@ struct ExecParams {
     // split chunks of panel tile (m,k), m > k, at split + (m(m-1)/2 + k) * tile_split_bytes
     uint8_t *split;
     int split_nrb, split_nkc;   // 128-row blocks and 64-wide k chunks per panel tile
+    int kgroup;                 // update group size G (upd_ngroups / upd_group_of)
     unsigned long long wait_budget_ns;
 };
 

@@ -11,6 +11,7 @@
 
 #include "core.cuh"
 #include "internal.h"
+#include "potrf_smem.cuh"
 #include "rec.cuh"
 #include "tc05.cuh"
 
@@ -73,17 +74,21 @@ __device__ Deps task_deps(const Task &t, const ExecParams &p, const Dims<T> &d) 
     };
     switch (t.kind) {
     case TK_POTRF:
-        need(0, &p.updA[t.k + p.NT * t.k], t.k * d.S(t.k, t.k));
+        need(0, &p.updA[t.k + p.NT * t.k], upd_ngroups(t.k, p.kgroup) * d.S(t.k, t.k));
         break;
     case TK_TRSM:
         need(0, &p.panA[t.k + p.NT * t.k], 1);
-        need(1, &p.updA[t.m + p.NT * t.k], t.k * d.S(t.m, t.k));
+        need(1, &p.updA[t.m + p.NT * t.k], upd_ngroups(t.k, p.kgroup) * d.S(t.m, t.k));
         break;
-    case TK_UPD:
-        need(0, &p.panA[t.m + p.NT * t.k], d.nbi(t.m));
-        need(1, &p.panA[t.n + p.NT * t.k], d.nbi(t.n));
-        need(2, &p.updA[t.m + p.NT * t.n], t.k * d.S(t.m, t.n));
+    case TK_UPD: {
+        // the group's last panel being solved implies the earlier ones are
+        // (each panel solve waits for the previous panels' updates of its tile)
+        const int kl = t.k + t.bn - 1;
+        need(0, &p.panA[t.m + p.NT * kl], d.nbi(t.m));
+        need(1, &p.panA[t.n + p.NT * kl], d.nbi(t.n));
+        need(2, &p.updA[t.m + p.NT * t.n], t.grp * d.S(t.m, t.n));
         break;
+    }
     case TK_INV:
         break;
     case TK_XINV:
@@ -183,6 +188,7 @@ __device__ void run_task(const Task &t, const ExecParams &p, const Dims<T> &d, T
         int info;
         if constexpr (std::is_same<T, float>::value) {
             if (p.full_inv) info = rec::tile_potrf_inv<T, SP>(d.A(t.k, t.k), d.X(t.k), d.tm(t.k), smem);
+            else if (d.tm(t.k) <= psm::MAXN) info = psm::potrf(d.A(t.k, t.k), d.tm(t.k), d.inv(t.k), smem);
             else info = rec::tile_potrf_blk<T, SP>(d.A(t.k, t.k), d.tm(t.k), d.inv(t.k), smem, ph);
         } else {
             info = rec::tile_potrf_blk<T, SP>(d.A(t.k, t.k), d.tm(t.k), d.inv(t.k), smem, ph);
@@ -237,14 +243,17 @@ __device__ void run_task(const Task &t, const ExecParams &p, const Dims<T> &d, T
         const VT C = d.A(t.m, t.n).sub(bi * SUBB, bj * SUBB);
         const bool diag = (t.m == t.n) && (bi == bj);
         if constexpr (TC) {
+            // the split tiles of panels k .. k + bn - 1 of one tile row are
+            // consecutive in the split buffer (index m(m-1)/2 + k)
             const size_t rbytes = (size_t)p.split_nkc * 2 * tc05::CHUNK_BYTES;
+            const size_t tstride = (size_t)p.split_nrb * rbytes;
             const uint8_t *a = split_tile(p, t.m, t.k) + bi * rbytes;
             const uint8_t *b = split_tile(p, t.n, t.k) + bj * rbytes;
             // warps 4-7 stage the old C block in TMEM while the MMAs run; the
             // epilogue subtracts the accumulator from it
             auto owned = [&](int r, int c) { return r < rows && c < cols && (!diag || r >= c); };
             const bool ok = tc05::gemm_bf16x3_sub(
-                tsm, stage, a, b, p.split_nkc,
+                tsm, stage, a, b, p.split_nkc, t.bn, tstride,
                 [&](int r, int c) { return owned(r, c) ? __ldcg(C.at(r, c)) : 0.f; },
                 [&](int r, int c, float v) {
                     if (owned(r, c)) *C.at(r, c) = v;
@@ -279,8 +288,9 @@ __device__ void run_task(const Task &t, const ExecParams &p, const Dims<T> &d, T
         }
         Acc<Cfg128<T, SP>> acc;
         acc.zero();
-        cta_gemm(acc, d.A(t.m, t.k).sub(bi * SUBB, 0), d.A(t.n, t.k).sub(bj * SUBB, 0), rows, cols,
-                 d.tm(t.k), smem);
+        for (int k = t.k; k < t.k + t.bn; ++k)
+            cta_gemm(acc, d.A(t.m, k).sub(bi * SUBB, 0), d.A(t.n, k).sub(bj * SUBB, 0), rows, cols, d.tm(k),
+                     smem);
         acc.sub_from(C, rows, cols, diag);
         break;
     }
@@ -441,8 +451,12 @@ __global__ void __launch_bounds__(NT_CTA, 1) cholesky_dag_kernel(ExecParams p) {
 
 template <class T, int SP, bool TC>
 constexpr size_t dag_smem_bytes() {
-    return (TC && (size_t)tc05::SMEM_BYTES > tile_smem_bytes<T, SP>() + 1024) ? (size_t)tc05::SMEM_BYTES
-                                                                           : tile_smem_bytes<T, SP>() + 1024;
+    // one CTA per SM: every variant may use the shared memory its largest task needs
+    // (the tcgen05 stages; FP32: the shared-memory diagonal-tile factorization)
+    size_t b = tile_smem_bytes<T, SP>() + 1024;
+    if (TC && (size_t)tc05::SMEM_BYTES > b) b = tc05::SMEM_BYTES;
+    if (std::is_same<T, float>::value && psm::SMEM_BYTES + 1024 > b) b = psm::SMEM_BYTES + 1024;
+    return b;
 }
 
 // Launch one persistent executor kernel of a variant (its shared-memory size

@@ -22,6 +22,7 @@ struct Context {
     int device = 0;
     int num_sms = 0;
     cudaStream_t stream = nullptr;
+    cudaEvent_t order_event = nullptr;   // orders `stream` after the caller's default stream
     int tile_size = 384;          // CHAMELEON_TILE_SIZE default (control/context.c:162)
     int inner_block = 48;
     int warnings = 1;
@@ -32,6 +33,12 @@ struct Context {
     bool rec_tile = false;        // FP32 factorization: recursive tile POTRF with full tile inverses
     bool xinv_solve = true;       // FP32 substitutions with full diagonal-tile inverses
     bool potrf_cta = false;        // one executor CTA dedicated to the diagonal-tile factorizations
+    // update group sizes (panels applied per trailing-update task) per path:
+    // FP64 DMMA, FP32 split products on mma.sync, FP32 on tcgen05
+    int kgroup_f64 = 1, kgroup_f32 = 1, kgroup_tc = 4;
+    // tile size of the mixed solver's FP32 copy of A (0: A's own tile size);
+    // used when it divides A's tile size
+    int factor_nb = 256;
     int desc_ids = 0;
     std::mutex mu;
 };
@@ -123,7 +130,7 @@ struct MixedWs {
     CHAM_desc_t *A32 = nullptr, *B32 = nullptr, *R = nullptr;   // views on the buffers below
     void *a32_buf = nullptr, *b32_buf = nullptr, *r_buf = nullptr;   // grow-only (dev_alloc)
     size_t a32_cap = 0, b32_cap = 0, r_cap = 0;
-    int N = -1, NB = -1, nrhs = -1;
+    int N = -1, NB = -1, NBf = -1, nrhs = -1;   // NBf: tile size of A32 / B32 (factor_tile(NB))
     unsigned long long *rmax = nullptr, *xmax = nullptr;
     double *colsum = nullptr;
     double *diag = nullptr;       // symmetric copies of the diagonal tiles (residuals)
@@ -180,6 +187,9 @@ struct ExecResult {
 enum ExecFlags : int { EXEC_REUSE_INV = 1 };
 int run_cholesky_dag(int mode, cham_uplo_t uplo, CHAM_desc_t *A, CHAM_desc_t *B, cudaStream_t s,
                      ExecResult *res, int split = 0, ExecWs *ws = nullptr, int grid = 0, int flags = 0);
+
+// Tile size of the mixed solver's FP32 factorization for FP64 tile size NB (mixed.cu).
+int factor_tile(int NB);
 
 // Mixed-precision solve on an explicit stream and workspaces (mixed.cu).
 // factored = true: m.A32 already holds the low-precision factor of A (resident

@@ -272,8 +272,10 @@ __global__ void __launch_bounds__(256) sym_cast_norm_kernel(SymTiles a, TileMapD
     const int lds = a.ld[p];
     const int rows = a.tm(p), cols = a.tm(q);
     const bool diag = (p == q);
-    float *dst = a32.base ? static_cast<float *>(a32.base) + a32.off[p + (int64_t)a32.mt * q] : nullptr;
-    const int ldd = a32.base ? a32.ld[p] : 0;
+    // the FP32 copy may use a finer tiling (tile size a32.mb dividing NB):
+    // stored tile (p, q) covers sub-tiles (p r + i / mb, q r + j / mb)
+    const int fb = a32.base ? a32.mb : a.NB;
+    const int rsub = a.NB / fb;
     for (int j = threadIdx.x; j < cols; j += blockDim.x) s_col[j] = 0.0;
     __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -281,19 +283,28 @@ __global__ void __launch_bounds__(256) sym_cast_norm_kernel(SymTiles a, TileMapD
     for (int r0 = warp * 32; r0 < rows; r0 += 256) {
         const int i = r0 + lane;
         const bool rv = i < rows;
+        const int rt = p * rsub + i / fb;   // sub-tile row of the FP32 copy
+        const int ldd = (a32.base && rv) ? a32.ld[rt] : 0;
         double rs = 0.0;
+        for (int jb = 0; jb < cols; jb += fb) {
+            float *dst = (a32.base && rv)
+                             ? static_cast<float *>(a32.base) + a32.off[rt + (int64_t)a32.mt * (q * rsub + jb / fb)] +
+                                   (i % fb)
+                             : nullptr;
+            const int je = min(cols, jb + fb);
 #pragma unroll 4
-        for (int j = 0; j < cols; ++j) {
-            const double v = rv ? src[i + (int64_t)j * lds] : 0.0;
-            if (dst && rv) dst[i + (int64_t)j * ldd] = __double2float_rn(v);
-            const bool ref = rv && (!diag || (a.upper ? i <= j : i >= j));
-            const double av = ref ? fabs(v) : 0.0;
-            ovf |= av > 3.4028234663852886e38;
-            if (!diag || i != j) rs += av;
-            double cs = av;
+            for (int j = jb; j < je; ++j) {
+                const double v = rv ? src[i + (int64_t)j * lds] : 0.0;
+                if (dst) dst[(int64_t)(j - jb) * ldd] = __double2float_rn(v);
+                const bool ref = rv && (!diag || (a.upper ? i <= j : i >= j));
+                const double av = ref ? fabs(v) : 0.0;
+                ovf |= av > 3.4028234663852886e38;
+                if (!diag || i != j) rs += av;
+                double cs = av;
 #pragma unroll
-            for (int o = 16; o; o >>= 1) cs += __shfl_xor_sync(0xffffffffu, cs, o);
-            if (lane == 0 && cs != 0.0) atomicAdd(&s_col[j], cs);
+                for (int o = 16; o; o >>= 1) cs += __shfl_xor_sync(0xffffffffu, cs, o);
+                if (lane == 0 && cs != 0.0) atomicAdd(&s_col[j], cs);
+            }
         }
         if (rv && rs != 0.0) atomicAdd(&colsum[(int64_t)p * a.NB + i], rs);
     }
@@ -322,13 +333,26 @@ static bool grow(void **buf, size_t *cap, size_t bytes) {
     return true;
 }
 
+}  // namespace
+
+// Tile size of the FP32 factorization for an FP64 tile size NB: the
+// configured factor tile size when it divides NB (a finer tiling shortens the
+// chain of diagonal-tile steps, the factorization's critical path), else NB.
+int factor_tile(int NB) {
+    const int f = ctx().factor_nb;
+    return (f > 0 && f < NB && NB % f == 0) ? f : NB;
+}
+
+namespace {
 int mixed_reserve(MixedWs &m, int N, int NB, int nrhs) {
-    if (m.N != N || m.NB != NB) {
+    const int NBf = factor_tile(NB);
+    if (m.N != N || m.NB != NB || m.NBf != NBf) {
         if (m.A32) CHAMELEON_Desc_Destroy(&m.A32);
         if (!grow(&m.a32_buf, &m.a32_cap, (size_t)N * N * sizeof(float))) return CHAMELEON_ERR_OUT_OF_RESOURCES;
-        if (int rc = desc_create_tiled_on(&m.A32, ChamRealFloat, m.a32_buf, NB, N, N)) return rc;
+        if (int rc = desc_create_tiled_on(&m.A32, ChamRealFloat, m.a32_buf, NBf, N, N)) return rc;
         m.N = N;
         m.NB = NB;
+        m.NBf = NBf;
         m.nrhs = -1;
     }
     if (m.nrhs != nrhs) {
@@ -337,7 +361,8 @@ int mixed_reserve(MixedWs &m, int N, int NB, int nrhs) {
         if (!grow(&m.b32_buf, &m.b32_cap, (size_t)N * nrhs * sizeof(float)) ||
             !grow(&m.r_buf, &m.r_cap, (size_t)N * nrhs * sizeof(double)))
             return CHAMELEON_ERR_OUT_OF_RESOURCES;
-        if (int rc = desc_create_tiled_on(&m.B32, ChamRealFloat, m.b32_buf, NB, N, nrhs)) return rc;
+        // B32 is tiled like the FP32 factor's tile rows; R like B
+        if (int rc = desc_create_tiled_on(&m.B32, ChamRealFloat, m.b32_buf, NBf, N, nrhs)) return rc;
         if (int rc = desc_create_tiled_on(&m.R, ChamRealDouble, m.r_buf, NB, N, nrhs)) return rc;
         m.nrhs = nrhs;
     }
@@ -377,7 +402,7 @@ static SymTiles symtiles(CHAM_desc_t *A, cham_uplo_t uplo, double *diag = nullpt
 // in *ovf.  Also makes the symmetric diagonal-tile copies for the residuals.
 double sym_norm_inf(CHAM_desc_t *A, cham_uplo_t uplo, cudaStream_t s, MixedWs &m, CHAM_desc_t *a32, int *ovf) {
     if (desc_upload(A) || mixed_reserve(m, A->n, A->nb, std::max(1, m.nrhs))) return -1.0;
-    if (a32 && (desc_upload(a32) || a32->nb != A->nb || a32->mb != A->mb || a32->mt != A->nt)) return -1.0;
+    if (a32 && (desc_upload(a32) || a32->nb != a32->mb || A->nb % a32->nb != 0 || a32->n != A->n)) return -1.0;
     const int NT = A->nt;
     cudaMemsetAsync(m.colsum, 0, A->n * sizeof(double), s);
     const TileMapD t32 = a32 ? tmap(a32) : TileMapD{nullptr, nullptr, nullptr, 0, 0, 0};
@@ -456,12 +481,15 @@ static int residual(CHAM_desc_t *A, cham_uplo_t uplo, CHAM_desc_t *B, CHAM_desc_
     return 0;
 }
 
-static bool converged(const std::vector<double> &rn, const std::vector<double> &xn, double cte, double *berr) {
+// dsposv's stopping test on every column, and the normwise backward error
+// max_j ||r_j||_inf / (||A||_inf ||x_j||_inf) of the current iterate.
+static bool converged(const std::vector<double> &rn, const std::vector<double> &xn, double cte, double anrm,
+                      double *berr) {
     bool ok = true;
     double b = 0;
     for (size_t j = 0; j < rn.size(); ++j) {
         if (!(rn[j] <= xn[j] * cte)) ok = false;
-        if (xn[j] > 0) b = std::max(b, rn[j] / xn[j]);
+        if (xn[j] > 0 && anrm > 0) b = std::max(b, rn[j] / (anrm * xn[j]));
     }
     if (berr) *berr = b;
     return ok;
@@ -582,7 +610,7 @@ int mixed_posv_ws(cham_uplo_t uplo, int precision, CHAM_desc_t *A, CHAM_desc_t *
             clk.tic();
             if ((rc = residual(A, uplo, B, X, s, rn, xn, m))) return rc;
             clk.toc(st.residual_ms);
-            bool ok = converged(rn, xn, cte, &berr);
+            bool ok = converged(rn, xn, cte, anrm, &berr);
             int it = 0;
             while (!ok && it < c.refine_maxiter) {
                 ++it;
@@ -602,7 +630,7 @@ int mixed_posv_ws(cham_uplo_t uplo, int precision, CHAM_desc_t *A, CHAM_desc_t *
                 clk.tic();
                 if ((rc = residual(A, uplo, B, X, s, rn, xn, m))) return rc;
                 clk.toc(st.residual_ms);
-                ok = converged(rn, xn, cte, &berr);
+                ok = converged(rn, xn, cte, anrm, &berr);
             }
             if (ok) {
                 iter = it;

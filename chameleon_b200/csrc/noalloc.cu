@@ -30,6 +30,7 @@
 
 #include "core.cuh"
 #include "internal.h"
+#include "rec.cuh"
 
 #define CHAM_B200_NOALLOC_POTRF_MAXN 1024
 
@@ -37,9 +38,11 @@ namespace chb {
 
 static __device__ __align__(256) double g_potrf_scratch[(CHAM_B200_NOALLOC_POTRF_MAXN / IB) * IB * IB];
 
+// The same tile algorithm as CUDA_dpotrf's kernel (blocked left-looking with
+// the 64-wide leaf), so both entry points return the same factor and info.
 __global__ void __launch_bounds__(NT_CTA, 1) potrf_noalloc_kernel(View T, int n, double *invd, int *info) {
     extern __shared__ __align__(128) double smem[];
-    const int r = tile_potrf<double, SPLIT_BF16X3>(T, n, invd, smem);
+    const int r = rec::tile_potrf_blk<double, SPLIT_BF16X3>(T, n, invd, smem);
     if (threadIdx.x == 0 && info) *info = r;
 }
 
@@ -51,6 +54,7 @@ bool g_attr_set[MAX_DEVICES] = {};
 
 // Per-device set-up: device address of the scratch array, kernel attribute.
 int noalloc_setup(int dev, double **addr) {
+    if (dev < 0 || dev >= MAX_DEVICES) return CHAMELEON_ERR_UNEXPECTED;
     std::lock_guard<std::mutex> lk(g_mu);
     if (!g_scratch_addr[dev]) {
         void *p = nullptr;
@@ -96,10 +100,13 @@ extern "C" int CUDA_dpotrf_noalloc(cham_uplo_t uplo, int n, double *A, int lda, 
         return 0;
     }
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return CHAMELEON_ERR_UNEXPECTED;
+    if (cudaGetDevice(&dev) != cudaSuccess) return CHAMELEON_ERR_UNEXPECTED;
     double *scratch = nullptr;
     if (int rc = noalloc_setup(dev, &scratch)) return rc;
     const View T = (uplo == ChamLower) ? View{A, 1, lda} : View{A, lda, 1};
+    // a launch error left over from unrelated earlier work would otherwise be
+    // reported as this launch's failure
+    (void)cudaGetLastError();
     potrf_noalloc_kernel<<<1, NT_CTA, TILE_KERNEL_SMEM_BYTES, s>>>(T, n, scratch, d_info);
     CHB_LAUNCHED(1);
     return cudaGetLastError() == cudaSuccess ? CHAMELEON_SUCCESS : CHAMELEON_ERR_UNEXPECTED;

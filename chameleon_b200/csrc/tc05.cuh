@@ -307,9 +307,11 @@ __device__ bool gemm_bf16x3(Smem *sm, uint8_t *stage_base, const uint8_t *a_chun
     return ok;
 }
 
-// C -= A * B^T for one 128 x 128 block of the executor's trailing update,
-// operands and roles as in gemm_bf16x3 (thread 0 copies, thread 32 MMAs,
-// idle() on thread 64).  The old values of C are staged in TMEM (columns
+// C -= A * B^T for one 128 x 128 block of the executor's trailing update over
+// the k chunks of `ntiles` panels (nkc_tile chunks each; the panels' chunks
+// are tile_stride bytes apart), accumulated in one TMEM accumulator; operands
+// and roles as in gemm_bf16x3 (thread 0 copies, thread 32 MMAs, idle() on
+// thread 64).  The old values of C are staged in TMEM (columns
 // 128-255) by warps 4-7 while the copies and MMAs run: each of those warps
 // owns one TMEM lane quarter (32 rows), reads its 128 columns 32 at a time
 // and stores them with tcgen05.st, so no value stays in registers across the
@@ -322,14 +324,17 @@ __device__ bool gemm_bf16x3(Smem *sm, uint8_t *stage_base, const uint8_t *a_chun
 // threads.  Returns false on a wait timeout.
 template <class L, class S, class I>
 __device__ bool gemm_bf16x3_sub(Smem *sm, uint8_t *stage_base, const uint8_t *a_chunks, const uint8_t *b_chunks,
-                                int nkc, L &&load, S &&store, I &&idle, unsigned *ph = nullptr) {
+                                int nkc_tile, int ntiles, size_t tile_stride, L &&load, S &&store, I &&idle,
+                                unsigned *ph = nullptr) {
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const uint32_t base = sm->chunks;   // k chunks issued by this CTA before this GEMM
     const uint32_t gnum = sm->gemms;    // GEMMs finished by this CTA before this one
+    const int nkc = nkc_tile * ntiles;  // k chunks of the whole group
     __syncthreads();
     const long long c_start = ph ? clock64() : 0;
     if (tid == 0) {
         fence_proxy_async();   // generic-proxy writes of the operands (other SMs) -> async-proxy reads
+        int kt = 0, kk = 0;    // panel of the group, chunk within the panel
         for (int kc = 0; kc < nkc; ++kc) {
             const uint32_t g = base + kc;
             const int s = g % STAGES;
@@ -338,9 +343,14 @@ __device__ bool gemm_bf16x3_sub(Smem *sm, uint8_t *stage_base, const uint8_t *a_
                 break;
             }
             uint8_t *st = stage_base + s * STAGE_BYTES;
+            const size_t off = (size_t)kt * tile_stride + (size_t)kk * 2 * CHUNK_BYTES;
             mbar_expect_tx(&sm->full[s], STAGE_BYTES);
-            bulk_g2s(st, a_chunks + (size_t)kc * 2 * CHUNK_BYTES, 2 * CHUNK_BYTES, &sm->full[s]);
-            bulk_g2s(st + 2 * CHUNK_BYTES, b_chunks + (size_t)kc * 2 * CHUNK_BYTES, 2 * CHUNK_BYTES, &sm->full[s]);
+            bulk_g2s(st, a_chunks + off, 2 * CHUNK_BYTES, &sm->full[s]);
+            bulk_g2s(st + 2 * CHUNK_BYTES, b_chunks + off, 2 * CHUNK_BYTES, &sm->full[s]);
+            if (++kk == nkc_tile) {
+                kk = 0;
+                ++kt;
+            }
         }
     } else if (tid == 32) {
         for (int kc = 0; kc < nkc; ++kc) {

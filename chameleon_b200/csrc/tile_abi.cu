@@ -11,6 +11,7 @@
 #include <algorithm>
 
 #include "core.cuh"
+#include "potrf_smem.cuh"
 #include "rec.cuh"
 #include "gen.cuh"
 #include "internal.h"
@@ -96,6 +97,17 @@ __global__ void __launch_bounds__(NT_CTA, 1) potrf_kernel(View T, int n, double 
     if (threadIdx.x == 0 && info) *info = r;
 }
 
+// FP32 tile Cholesky: the shared-memory kernel of the executor's diagonal
+// tiles for n <= 256, the blocked one (BF16x3 GEMMs) above.
+constexpr size_t SPOTRF_SMEM_BYTES =
+    psm::SMEM_BYTES > tile_smem_bytes<float>() ? psm::SMEM_BYTES : tile_smem_bytes<float>();
+__global__ void __launch_bounds__(NT_CTA, 1) spotrf_kernel(ViewF T, int n, float *invd, int *info) {
+    extern __shared__ __align__(128) float fsm[];
+    const int r = (n <= psm::MAXN) ? psm::potrf(T, n, invd, fsm)
+                                   : rec::tile_potrf_blk<float, SPLIT_BF16X3>(T, n, invd, fsm);
+    if (threadIdx.x == 0 && info) *info = r;
+}
+
 __global__ void plgsy_tile_kernel(double *A, int lda, int M, int N, double bump, int bigM, int m0, int n0,
                                   unsigned long long seed) {
     const int64_t total = (int64_t)M * N;
@@ -160,6 +172,8 @@ static int set_smem_attrs() {
     CHB_CUDA(cudaFuncSetAttribute(trsm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg64<double>::SMEM_BYTES));
     CHB_CUDA(cudaFuncSetAttribute(potrf_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)TILE_KERNEL_SMEM_BYTES));
+    CHB_CUDA(cudaFuncSetAttribute(spotrf_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)SPOTRF_SMEM_BYTES));
     CHB_CUDA(cudaFuncSetAttribute(inv_diag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)(2 * IB * LDD * sizeof(double))));
     smem_attr_done = true;
@@ -290,6 +304,28 @@ int CUDA_dpotrf(cham_uplo_t uplo, int n, double *A, int lda, double *WORK, int l
     if (int rc = handle_ws(handle, (size_t)nblk * IB * IB * sizeof(double))) return rc;
     const View T = (uplo == ChamLower) ? View{A, 1, lda} : View{A, lda, 1};
     potrf_kernel<<<1, NT_CTA, TILE_KERNEL_SMEM_BYTES, handle->stream>>>(T, n, handle->ws, d_info);
+    CHB_LAUNCHED(1);
+    return cudaGetLastError() == cudaSuccess ? CHAMELEON_SUCCESS : CHAMELEON_ERR_UNEXPECTED;
+}
+
+int CUDA_spotrf(cham_uplo_t uplo, int n, float *A, int lda, float *WORK, int lwork, int *d_info,
+                cusolverDnHandle_t handle) {
+    (void)WORK;
+    (void)lwork;
+    if (!handle) return CHAMELEON_ERR_ILLEGAL_VALUE;
+    if (uplo != ChamUpper && uplo != ChamLower) return -1;
+    if (n < 0) return -2;
+    if (lda < std::max(1, n)) return -4;
+    if (n == 0) {
+        if (d_info) cudaMemsetAsync(d_info, 0, sizeof(int), handle->stream);
+        return 0;
+    }
+    if (int rc = set_smem_attrs()) return rc;
+    const int nblk = (n + IB - 1) / IB;
+    if (int rc = handle_ws(handle, (size_t)nblk * IB * IB * sizeof(float))) return rc;
+    const ViewF T = (uplo == ChamLower) ? ViewF{A, 1, lda} : ViewF{A, lda, 1};
+    spotrf_kernel<<<1, NT_CTA, SPOTRF_SMEM_BYTES, handle->stream>>>(T, n, reinterpret_cast<float *>(handle->ws),
+                                                                    d_info);
     CHB_LAUNCHED(1);
     return cudaGetLastError() == cudaSuccess ? CHAMELEON_SUCCESS : CHAMELEON_ERR_UNEXPECTED;
 }

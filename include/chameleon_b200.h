@@ -69,6 +69,11 @@ typedef enum {
                                              diagonal tiles, kept across refinement solves (default) */
 #define CHAMELEON_B200_POTRF_CTA      108 /* 1: one executor CTA runs all diagonal-tile
                                              factorizations; 0: any CTA (default) */
+#define CHAMELEON_B200_UPD_GROUP_F64  109 /* panels applied per trailing-update task, FP64 path (default 1) */
+#define CHAMELEON_B200_UPD_GROUP_F32  110 /* the same, FP32 split products on mma.sync (default 1) */
+#define CHAMELEON_B200_UPD_GROUP_TC   111 /* the same, FP32 BF16x3 on tcgen05 (default 4) */
+#define CHAMELEON_B200_FACTOR_NB      112 /* tile size of the mixed solver's FP32 factorization;
+                                             0: the tile size of A (default 256 when it divides A's) */
 
 /* Factorization precisions for CHAMELEON_B200_PRECISION */
 #define CHAM_B200_PREC_FP64   0
@@ -253,6 +258,10 @@ int CUDA_dtrsm(cham_side_t side, cham_uplo_t uplo, cham_trans_t transa, cham_dia
                cublasHandle_t handle);
 /* d_info: device int receiving LAPACK's info; WORK/lwork are accepted and unused */
 int CUDA_dpotrf(cham_uplo_t uplo, int n, double *A, int lda, double *WORK, int lwork,
+                int *d_info, cusolverDnHandle_t handle);
+/* gpucublas_z.h:54 after z->s generation: FP32 tile Cholesky (the mixed
+ * solver's diagonal-tile kernel); d_info as CUDA_dpotrf */
+int CUDA_spotrf(cham_uplo_t uplo, int n, float *A, int lda, float *WORK, int lwork,
                 int *d_info, cusolverDnHandle_t handle);
 /* No counterpart in the reference.  CUDA_dpotrf without any device
  * allocation, for callers that cannot allocate: a task runtime that owns the

@@ -37,6 +37,12 @@ def build_port(force=False):
     return PORT_SO
 
 
+def reference_source_dir():
+    """Where oracle/build_ref.sh reads the reference sources: $CHAMREF_SRC, else
+    the recipe's default location."""
+    return os.environ.get("CHAMREF_SRC", "/root/reference")
+
+
 def build_ref(force=False):
     """Build the reference library (needs the reference sources; not on the GPU host)."""
     if not force and os.path.exists(REF_SO):

@@ -17,6 +17,13 @@ SUBB = 128
 FACT, SOLVE, XINV, NOINV = 1, 2, 4, 8
 
 
+def ngroups(n, G):
+    """Update groups of tile column n (upd_ngroups in executor.cuh): the last
+    panel n-1 alone, the panels before it in groups of G aligned at multiples
+    of G."""
+    return 0 if n <= 0 else -(-(n - 1) // G) + 1
+
+
 def geometry(N, NB, nrhs, NBB):
     NT = -(-N // NB)
     NTB = -(-nrhs // NBB) if nrhs else 0
@@ -26,7 +33,7 @@ def geometry(N, NB, nrhs, NBB):
     return NT, NTB, tm, nbi, S
 
 
-def check_waits(tasks, mode, N, NB, nrhs, NBB):
+def check_waits(tasks, mode, N, NB, nrhs, NBB, G=1):
     NT, NTB, tm, nbi, S = geometry(N, NB, nrhs, NBB)
     upd = np.zeros((NT, NT), int); pan = np.zeros((NT, NT), int)
     fwdB = np.zeros((NT, max(NTB, 1)), int); fwdD = np.zeros_like(fwdB)
@@ -35,17 +42,24 @@ def check_waits(tasks, mode, N, NB, nrhs, NBB):
     fact = bool(mode & FACT)
     # with full tile inverses (XINV) each substitution is split into row blocks
     ns = (lambda k: nbi(k)) if mode & XINV else (lambda k: 1)
-    for kind, sub, m, n, k, bn in tasks:
+    applied = {}   # (m, n, bi, bj) -> panels applied so far, in order
+    for kind, sub, m, n, k, bn, grp in tasks:
         if kind == TK_POTRF:
-            ok = upd[k, k] >= k * S(k, k); pan[k, k] += 1
+            ok = upd[k, k] >= ngroups(k, G) * S(k, k); pan[k, k] += 1
         elif kind == TK_INV:
             ok = True; pan[k, k] += 1
         elif kind == TK_XINV:
             ok = (not fact) or pan[k, k] >= 1; xinv[k] += 1
         elif kind == TK_TRSM:
-            ok = pan[k, k] >= 1 and upd[m, k] >= k * S(m, k); pan[m, k] += 1
+            ok = pan[k, k] >= 1 and upd[m, k] >= ngroups(k, G) * S(m, k); pan[m, k] += 1
         elif kind == TK_UPD:
-            ok = pan[m, k] >= nbi(m) and pan[n, k] >= nbi(n) and upd[m, n] >= k * S(m, n); upd[m, n] += 1
+            kl = k + bn - 1
+            ok = pan[m, kl] >= nbi(m) and pan[n, kl] >= nbi(n) and upd[m, n] >= grp * S(m, n)
+            upd[m, n] += 1
+            # every sub-block sees each panel k < n exactly once, in order
+            key = (m, n, sub)
+            assert applied.get(key, 0) == k, (key, applied.get(key, 0), k)
+            applied[key] = k + bn
         elif kind == TK_FWD_TRSM:
             if mode & XINV:
                 inv_ok = bool(mode & NOINV) or xinv[k] >= 1
@@ -66,7 +80,8 @@ def check_waits(tasks, mode, N, NB, nrhs, NBB):
     if fact:
         for m in range(NT):
             for n in range(m + 1):
-                assert upd[m, n] == n * S(m, n)
+                assert upd[m, n] == ngroups(n, G) * S(m, n)
+        assert all(v == key[1] for key, v in applied.items())
     if mode & SOLVE:
         want = np.array([ns(k) for k in range(NT)])[:, None]
         assert (fwdD[:, :NTB] == want).all() and (bwdD[:, :NTB] == want).all()
@@ -86,7 +101,7 @@ def emulate(tasks, A, B, uplo, N, NB, NBB, xinv=False):
     Bt = lambda m, bn: B[m * NB:m * NB + tm(m), bn * NBB:min((bn + 1) * NBB, B.shape[1])]
     Y = np.full_like(B, np.nan) if B is not None else None
     Yt = lambda m, bn: Y[m * NB:m * NB + tm(m), bn * NBB:min((bn + 1) * NBB, B.shape[1])]
-    for kind, sub, m, n, k, bn in tasks:
+    for kind, sub, m, n, k, bn, grp in tasks:
         if kind == TK_POTRF:
             T = L(k, k)
             T[np.tril_indices(T.shape[0])] = np.linalg.cholesky(np.tril(T) + np.tril(T, -1).T)[
@@ -97,7 +112,8 @@ def emulate(tasks, A, B, uplo, N, NB, NBB, xinv=False):
         elif kind == TK_UPD:
             bi, bj = sub & 0xFF, (sub >> 8) & 0xFF
             C = L(m, n)[bi * SUBB:(bi + 1) * SUBB, bj * SUBB:(bj + 1) * SUBB]
-            upd = L(m, k)[bi * SUBB:(bi + 1) * SUBB] @ L(n, k)[bj * SUBB:(bj + 1) * SUBB].T
+            upd = sum(L(m, kk)[bi * SUBB:(bi + 1) * SUBB] @ L(n, kk)[bj * SUBB:(bj + 1) * SUBB].T
+                      for kk in range(k, k + bn))
             if m == n and bi == bj:
                 upd = np.tril(upd)
             C -= upd
@@ -122,16 +138,17 @@ def emulate(tasks, A, B, uplo, N, NB, NBB, xinv=False):
 
 
 SHAPES = [(15, 16, 1, 16), (37, 17, 22, 17), (300, 128, 5, 128), (700, 256, 70, 64), (1000, 384, 3, 384),
-          (1100, 512, 64, 512), (513, 512, 1, 512)]
+          (1100, 512, 64, 512), (513, 512, 1, 512), (2000, 128, 7, 128), (1500, 100, 3, 100)]
 
 
 @pytest.mark.parametrize("N,NB,nrhs,NBB", SHAPES)
 @pytest.mark.parametrize("workers", [1, 7, 148])
 @pytest.mark.parametrize("prof", [0, 1, 2])
-def test_schedule_is_deadlock_free(cb_host, N, NB, nrhs, NBB, workers, prof):
+@pytest.mark.parametrize("G", [1, 3, 4])
+def test_schedule_is_deadlock_free(cb_host, N, NB, nrhs, NBB, workers, prof, G):
     for mode in (FACT, SOLVE, FACT | SOLVE):
-        t = cb_host.schedule(mode, N, NB, nrhs if mode & SOLVE else 0, NBB, workers, prof)
-        check_waits(t, mode, N, NB, nrhs if mode & SOLVE else 0, NBB)
+        t = cb_host.schedule(mode, N, NB, nrhs if mode & SOLVE else 0, NBB, workers, prof, G)
+        check_waits(t, mode, N, NB, nrhs if mode & SOLVE else 0, NBB, G)
 
 
 @pytest.mark.parametrize("N,NB,nrhs,NBB", SHAPES)
@@ -141,20 +158,21 @@ def test_schedule_with_full_tile_inverses_is_deadlock_free(cb_host, N, NB, nrhs,
     POTRF in a factor+solve launch, instead of TK_INV in a solve launch, and no
     inversion task at all when the inverses are reused (NOINV)."""
     for mode in (FACT | SOLVE | XINV, SOLVE | XINV, SOLVE | XINV | NOINV):
-        t = cb_host.schedule(mode, N, NB, nrhs, NBB, workers, 2)
-        check_waits(t, mode, N, NB, nrhs, NBB)
+        t = cb_host.schedule(mode, N, NB, nrhs, NBB, workers, 2, 4)
+        check_waits(t, mode, N, NB, nrhs, NBB, 4)
         kinds = set(int(x) for x in t[:, 0])
         assert (TK_XINV in kinds) == (not mode & NOINV)
         assert TK_INV not in kinds
 
 
 @pytest.mark.parametrize("uplo", [121, 122])
-@pytest.mark.parametrize("N,NB,nrhs,NBB", SHAPES[:6])
-def test_schedule_dataflow_reproduces_cholesky(cb_host, orc, uplo, N, NB, nrhs, NBB):
+@pytest.mark.parametrize("N,NB,nrhs,NBB", SHAPES[:6] + SHAPES[7:])
+@pytest.mark.parametrize("G", [1, 4])
+def test_schedule_dataflow_reproduces_cholesky(cb_host, orc, uplo, N, NB, nrhs, NBB, G):
     A0 = orc.dplgsy(float(N), N, 51)
     B0 = orc.dplrnt(N, nrhs, 5673)
     A = A0.copy(); B = B0.copy()
-    emulate(cb_host.schedule(FACT | SOLVE, N, NB, nrhs, NBB, 13), A, B, uplo, N, NB, NBB)
+    emulate(cb_host.schedule(FACT | SOLVE, N, NB, nrhs, NBB, 13, 0, G), A, B, uplo, N, NB, NBB)
     F = np.tril(A) if uplo == 122 else np.triu(A)
     assert orc.check_factorization(uplo, A0, F) < 60
     assert orc.check_solve(A0, B, B0) < 60
@@ -176,14 +194,14 @@ def test_schedule_dataflow_with_full_tile_inverses(cb_host, orc, uplo, N, NB, nr
     A0 = orc.dplgsy(float(N), N, 52)
     B0 = orc.dplrnt(N, nrhs, 5674)
     A = A0.copy(); B = B0.copy()
-    emulate(cb_host.schedule(FACT | SOLVE | XINV, N, NB, nrhs, NBB, 13, 2), A, B, uplo, N, NB, NBB, xinv=True)
+    emulate(cb_host.schedule(FACT | SOLVE | XINV, N, NB, nrhs, NBB, 13, 2, 4), A, B, uplo, N, NB, NBB, xinv=True)
     assert orc.check_solve(A0, B, B0) < 60
     B2 = B0.copy()
-    emulate(cb_host.schedule(SOLVE | XINV | NOINV, N, NB, nrhs, NBB, 13, 2), A, B2, uplo, N, NB, NBB, xinv=True)
+    emulate(cb_host.schedule(SOLVE | XINV | NOINV, N, NB, nrhs, NBB, 13, 2, 4), A, B2, uplo, N, NB, NBB, xinv=True)
     assert np.allclose(B2, B, rtol=1e-12, atol=1e-14)
 
 
-def replay_two_lists(tasks, mode, N, NB, nrhs, NBB):
+def replay_two_lists(tasks, mode, N, NB, nrhs, NBB, G=1):
     """The executor's dedicated-CTA scheme: one worker runs the POTRF tasks in
     list order, the others run the remaining tasks in list order.  Replays the
     two sequences greedily (whichever head's wait predicate holds goes next)
@@ -198,7 +216,7 @@ def replay_two_lists(tasks, mode, N, NB, nrhs, NBB):
             if idx < len(head_list):
                 cand = order + [head_list[idx]]
                 try:
-                    check_waits_prefix(cand, mode, N, NB, nrhs, NBB)
+                    check_waits_prefix(cand, mode, N, NB, nrhs, NBB, G)
                 except AssertionError:
                     continue
                 order = cand
@@ -212,7 +230,7 @@ def replay_two_lists(tasks, mode, N, NB, nrhs, NBB):
     return order
 
 
-def check_waits_prefix(prefix, mode, N, NB, nrhs, NBB):
+def check_waits_prefix(prefix, mode, N, NB, nrhs, NBB, G=1):
     """check_waits on a prefix of a run (no completeness checks)."""
     NT, NTB, tm, nbi, S = geometry(N, NB, nrhs, NBB)
     upd = np.zeros((NT, NT), int); pan = np.zeros((NT, NT), int)
@@ -221,17 +239,18 @@ def check_waits_prefix(prefix, mode, N, NB, nrhs, NBB):
     xinv = np.zeros(NT, int)
     fact = bool(mode & FACT)
     ns = (lambda k: nbi(k)) if mode & XINV else (lambda k: 1)
-    for kind, sub, m, n, k, bn in prefix:
+    for kind, sub, m, n, k, bn, grp in prefix:
         if kind == TK_POTRF:
-            ok = upd[k, k] >= k * S(k, k); pan[k, k] += 1
+            ok = upd[k, k] >= ngroups(k, G) * S(k, k); pan[k, k] += 1
         elif kind == TK_INV:
             ok = True; pan[k, k] += 1
         elif kind == TK_XINV:
             ok = (not fact) or pan[k, k] >= 1; xinv[k] += 1
         elif kind == TK_TRSM:
-            ok = pan[k, k] >= 1 and upd[m, k] >= k * S(m, k); pan[m, k] += 1
+            ok = pan[k, k] >= 1 and upd[m, k] >= ngroups(k, G) * S(m, k); pan[m, k] += 1
         elif kind == TK_UPD:
-            ok = pan[m, k] >= nbi(m) and pan[n, k] >= nbi(n) and upd[m, n] >= k * S(m, n); upd[m, n] += 1
+            kl = k + bn - 1
+            ok = pan[m, kl] >= nbi(m) and pan[n, kl] >= nbi(n) and upd[m, n] >= grp * S(m, n); upd[m, n] += 1
         elif kind == TK_FWD_TRSM:
             inv_ok = (bool(mode & NOINV) or xinv[k] >= 1) if mode & XINV else pan[k, k] >= 1
             ok = inv_ok and fwdB[k, bn] >= k * nbi(k); fwdD[k, bn] += 1
@@ -247,8 +266,8 @@ def check_waits_prefix(prefix, mode, N, NB, nrhs, NBB):
 
 @pytest.mark.parametrize("N,NB,nrhs,NBB", [(1000, 256, 3, 256), (1100, 512, 64, 512), (300, 128, 5, 128)])
 def test_dedicated_potrf_worker_never_stalls(cb_host, N, NB, nrhs, NBB):
-    for mode, prof in ((FACT, 0), (FACT | SOLVE, 0), (FACT | SOLVE | XINV, 2)):
-        t = cb_host.schedule(mode, N, NB, nrhs if mode & SOLVE else 0, NBB, 148, prof)
+    for mode, prof, G in ((FACT, 0, 1), (FACT | SOLVE, 0, 1), (FACT | SOLVE | XINV, 2, 4)):
+        t = cb_host.schedule(mode, N, NB, nrhs if mode & SOLVE else 0, NBB, 148, prof, G)
         order = replay_two_lists([tuple(int(v) for v in r) for r in t], mode, N, NB,
-                                 nrhs if mode & SOLVE else 0, NBB)
-        check_waits(np.array(order), mode, N, NB, nrhs if mode & SOLVE else 0, NBB)
+                                 nrhs if mode & SOLVE else 0, NBB, G)
+        check_waits(np.array(order), mode, N, NB, nrhs if mode & SOLVE else 0, NBB, G)

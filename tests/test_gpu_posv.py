@@ -274,6 +274,38 @@ def test_cuda_dpotrf(cb, orc, handle, uplo, n):
     assert np.array_equal(F - tri(F), A - tri(A))   # other triangle untouched
 
 
+@pytest.mark.parametrize("uplo", [121, 122])
+@pytest.mark.parametrize("n", [1, 37, 64, 100, 200, 255, 256, 300, 512])
+def test_cuda_spotrf(cb, orc, handle, uplo, n):
+    """FP32 tile Cholesky (the mixed solver's diagonal-tile kernel: on chip for
+    n <= 256, blocked above) against the FP64 factor, to FP32 accuracy, with
+    the other triangle untouched; a non-positive pivot gives LAPACK's info."""
+    import torch
+    A = orc.dplgsy(float(n), n, 23)
+    dA = torch.from_numpy(np.asfortranarray(A).T.astype(np.float32).copy()).cuda()
+    info = torch.full((1,), -7, dtype=torch.int32, device="cuda")
+    L = cb.lib()
+    assert L.CUDA_spotrf(uplo, n, ctypes.c_void_p(dA.data_ptr()), n, None, 0,
+                         ctypes.c_void_p(info.data_ptr()), handle) == 0
+    torch.cuda.synchronize()
+    assert int(info.item()) == 0
+    F = dA.cpu().numpy().T.astype(np.float64)
+    A32 = A.astype(np.float32).astype(np.float64)
+    Lref = np.linalg.cholesky(A32)
+    tri = np.triu if uplo == 121 else np.tril
+    Lg = tri(F) if uplo == 122 else tri(F).T
+    assert np.abs(Lg - Lref).max() <= 8 * n * 5.96e-8 * np.sqrt(np.abs(A32).max())
+    assert np.array_equal(F - tri(F), A32 - tri(A32))   # other triangle untouched
+    if n >= 100:
+        B = A.copy()
+        B[n - 30, n - 30] = -2.0 * n
+        dB = torch.from_numpy(np.asfortranarray(B).T.astype(np.float32).copy()).cuda()
+        assert L.CUDA_spotrf(uplo, n, ctypes.c_void_p(dB.data_ptr()), n, None, 0,
+                             ctypes.c_void_p(info.data_ptr()), handle) == 0
+        torch.cuda.synchronize()
+        assert int(info.item()) == n - 29
+
+
 def test_cuda_generators_match_oracle(cb, orc, handle):
     import torch
     m, n, bigM, m0, n0 = 50, 40, 300, 100, 60
@@ -326,3 +358,37 @@ def test_fp64_reads_only_uplo_triangle(cb, orc, uplo, N, NB):
     assert cb.dposv(uplo, N, nrhs, A, N, B, N) == 0
     assert np.isfinite(B).all()
     assert orc.check_solve(A0, B, B0) < 60
+
+
+@pytest.mark.parametrize("uplo", [121, 122])
+def test_default_stream_writes_are_ordered_before_the_call(cb, uplo):
+    """A caller that fills its device matrix on the default stream (here torch
+    copies into reused allocations, with no synchronization) and then calls
+    dposv_Tile must get the solution of that matrix: the library's stream
+    waits for the caller's default-stream work at every entry."""
+    import torch
+    N, NB, nrhs = 8192, 512, 16
+    A0 = torch.zeros((N, N), dtype=torch.float64, device="cuda")
+    B0 = torch.zeros((nrhs, N), dtype=torch.float64, device="cuda")
+    dA = cb.Desc.create(N, N, NB, mat=A0)
+    dB = cb.Desc.create(N, nrhs, NB, mat=B0)
+    assert cb.dplgsy_Tile(float(N), 123, dA, 51) == 0
+    assert cb.dplrnt_Tile(dB, 5673) == 0
+    dA.destroy()
+    dB.destroy()
+    A = torch.full_like(A0, float("nan"))
+    B = torch.full_like(B0, float("nan"))
+    for _ in range(3):
+        A.fill_(float("nan"))
+        B.fill_(float("nan"))
+        A.copy_(A0)          # queued on the default stream, not synchronized
+        B.copy_(B0)
+        dA = cb.Desc.create(N, N, NB, mat=A)
+        dB = cb.Desc.create(N, nrhs, NB, mat=B)
+        assert cb.dposv_Tile(uplo, dA, dB) == 0
+        torch.cuda.synchronize()
+        R = B0.T - A0 @ B.T
+        r = float(R.abs().sum(0).max() / (A0.abs().sum(0).max() * B.T.abs().sum(0).max() * N * EPS))
+        assert r < 60, r
+        dA.destroy()
+        dB.destroy()
