@@ -104,17 +104,34 @@ std::vector<Task> build_order(const Shape &s) {
     const bool xinv = s.mode & MODE_XINV;
     const double nb = s.NB;
     const Calib &cal = kCalib[(s.prof >= 0 && s.prof < 3) ? s.prof : 0];
+    // tcgen05 path: task durations in microseconds from per-task device traces
+    // at NB = 256 and 512 (N = 32768).  The diagonal and panel tasks there are
+    // latency-bound and grow linearly with the tile order, not with its flops,
+    // so a flop model misorders the list (tasks whose inputs are not ready are
+    // claimed first and their CTAs wait).
+    const bool lat = (s.prof == PROF_F32_TC05);
+    auto c_potrf = [&](double t) { return lat ? 1.6 * t : cal.potrf * 6.0 * t * t * t / 3.0; };
+    auto c_xinv = [&](double t) { return lat ? 1.5 * t : cal.potrf * 6.0 * t * t * t / 3.0; };
+    auto c_trsm = [&]() { return lat ? 0.34 * nb : cal.trsm * 2.0 * SUBB * nb * nb; };
+    auto c_upd = [&](int cnt) {
+        return lat ? 5.0 + 0.011 * nb * cnt
+                   : cal.upd * SUBB * SUBB * nb * 2.0 * (cnt + cal.upd_fix) / (1.0 + cal.upd_fix);
+    };
+    auto c_strsm = [&](double t, double w, int parts) {
+        return lat ? 13.0 + 0.01 * t : cal.strsm * 3.0 * t * t * w / parts;
+    };
+    auto c_supd = [&](double t, double w) { return lat ? 8.0 + 0.04 * t : cal.supd * 2.0 * SUBB * t * w; };
     if (fact) {
         for (int k = 0; k < NT; ++k) {
             const double tk = tm(k);
-            P[k] = add(TK_POTRF, k, k, k, 0, 1, cal.potrf * 6.0 * tk * tk * tk / 3.0);
+            P[k] = add(TK_POTRF, k, k, k, 0, 1, c_potrf(tk));
             edge(lastU[k + (size_t)NT * k], P[k]);
             if (xinv && solve) {
-                XI[k] = add(TK_XINV, k, k, k, 0, 1, cal.potrf * 6.0 * tk * tk * tk / 3.0);
+                XI[k] = add(TK_XINV, k, k, k, 0, 1, c_xinv(tk));
                 edge(P[k], XI[k]);
             }
             for (int m = k + 1; m < NT; ++m) {
-                const int id = add(TK_TRSM, m, k, k, 0, nbi(m), cal.trsm * 2.0 * SUBB * nb * nb);
+                const int id = add(TK_TRSM, m, k, k, 0, nbi(m), c_trsm());
                 edge(P[k], id);
                 edge(lastU[m + (size_t)NT * k], id);
                 Tr[m + (size_t)NT * k] = id;
@@ -127,7 +144,7 @@ std::vector<Task> build_order(const Shape &s) {
                 if (k0 + cnt - 1 != k) continue;
                 for (int m = n; m < NT; ++m) {
                     const int sub = (m == n) ? nbi(m) * (nbi(m) + 1) / 2 : nbi(m) * nbi(n);
-                    const double dur = cal.upd * SUBB * SUBB * nb * 2.0 * (cnt + cal.upd_fix) / (1.0 + cal.upd_fix);
+                    const double dur = c_upd(cnt);
                     const int id = add(TK_UPD, m, n, k0, cnt, sub, dur);
                     ct[id].grp = gi;
                     edge(Tr[m + (size_t)NT * k], id);
@@ -139,7 +156,7 @@ std::vector<Task> build_order(const Shape &s) {
         }
     } else if (solve && !(s.mode & MODE_NOINV)) {
         for (int k = 0; k < NT; ++k) {
-            if (xinv) XI[k] = add(TK_XINV, k, k, k, 0, 1, cal.potrf * 6.0 * tm(k) * tm(k) * tm(k) / 3.0);
+            if (xinv) XI[k] = add(TK_XINV, k, k, k, 0, 1, c_xinv(tm(k)));
             else P[k] = add(TK_INV, k, k, k, 0, 1, 1.0 * tm(k) * IB * IB);
         }
     }
@@ -151,12 +168,12 @@ std::vector<Task> build_order(const Shape &s) {
             for (int k = 0; k < NT; ++k) {
                 // MODE_XINV: one sub-task per row block (each applies its rows of the inverse)
                 const int f = add(TK_FWD_TRSM, k, k, k, bn, xinv ? nbi(k) : 1,
-                                  cal.strsm * 3.0 * tm(k) * tm(k) * w / (xinv ? nbi(k) : 1));
+                                  c_strsm(tm(k), w, xinv ? nbi(k) : 1));
                 edge(xinv ? XI[k] : P[k], f);
                 edge(lastFU[k + (size_t)NT * bn], f);
                 F[k + (size_t)NT * bn] = f;
                 for (int m = k + 1; m < NT; ++m) {
-                    const int u = add(TK_FWD_UPD, m, k, k, bn, nbi(m), cal.supd * 2.0 * SUBB * tm(k) * w);
+                    const int u = add(TK_FWD_UPD, m, k, k, bn, nbi(m), c_supd(tm(k), w));
                     edge(f, u);
                     if (fact) edge(Tr[m + (size_t)NT * k], u);
                     edge(lastFU[m + (size_t)NT * bn], u);
@@ -165,12 +182,12 @@ std::vector<Task> build_order(const Shape &s) {
             }
             for (int k = NT - 1; k >= 0; --k) {
                 const int b = add(TK_BWD_TRSM, k, k, k, bn, xinv ? nbi(k) : 1,
-                                  cal.strsm * 3.0 * tm(k) * tm(k) * w / (xinv ? nbi(k) : 1));
+                                  c_strsm(tm(k), w, xinv ? nbi(k) : 1));
                 edge(F[k + (size_t)NT * bn], b);
                 edge(lastBU[k + (size_t)NT * bn], b);
                 Bk[k + (size_t)NT * bn] = b;
                 for (int m = k - 1; m >= 0; --m) {
-                    const int u = add(TK_BWD_UPD, m, k, k, bn, nbi(m), cal.supd * 2.0 * SUBB * tm(k) * w);
+                    const int u = add(TK_BWD_UPD, m, k, k, bn, nbi(m), c_supd(tm(k), w));
                     edge(b, u);
                     edge(lastBU[m + (size_t)NT * bn], u);
                     lastBU[m + (size_t)NT * bn] = u;

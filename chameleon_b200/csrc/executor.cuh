@@ -35,26 +35,37 @@ struct Task {
     int32_t grp;         // TK_UPD: index of the group in tile column n
 };
 
-// Update groups of tile column n (n >= 1): the panels k < n that update tile
-// (m, n), m >= n, are applied in groups.  The last one, k = n - 1, is a group
-// of its own (it is on the critical path of step n); the others form groups of
-// G consecutive panels aligned at multiples of G ([0, G), [G, 2G), ...), the
-// last of them ending at n - 1.  Number of groups of column n:
+// Update groups of tile column n: the panels k < n that update tile (m, n),
+// m >= n, are applied in groups.  The last UPD_TAIL panels (n-2, n-1) are
+// groups of their own: they are on the critical path of steps n-1 and n.  The
+// panels before them form groups of G aligned at the end (the first group
+// takes the remainder), so that every step completes a group for 1/G of the
+// columns and the update work arrives evenly instead of in bursts.
+constexpr int UPD_TAIL = 2;
 __host__ __device__ __forceinline__ int upd_ngroups(int n, int G) {
-    return n <= 0 ? 0 : (n - 1 + G - 1) / G + 1;
+    if (n <= UPD_TAIL) return n > 0 ? n : 0;
+    return (n - UPD_TAIL + G - 1) / G + UPD_TAIL;
 }
 // The group of column n (n > k) that panel k belongs to: first panel, panel
 // count and index.
 __host__ __device__ __forceinline__ void upd_group_of(int n, int k, int G, int *k0, int *cnt, int *idx) {
-    if (k == n - 1) {
+    const int m = n > UPD_TAIL ? n - UPD_TAIL : 0;   // panels in groups of G
+    if (k >= m) {
         *k0 = k;
         *cnt = 1;
-        *idx = upd_ngroups(n, G) - 1;
+        *idx = (m + G - 1) / G + (k - m);
+        return;
+    }
+    const int r = m % G;   // size of the first (partial) group, 0 if none
+    if (r > 0 && k < r) {
+        *k0 = 0;
+        *cnt = r;
+        *idx = 0;
     } else {
-        const int g = k / G;
-        *k0 = g * G;
-        *cnt = ((g + 1) * G < n - 1 ? (g + 1) * G : n - 1) - *k0;
-        *idx = g;
+        const int g = (k - r) / G;
+        *k0 = r + g * G;
+        *cnt = G;
+        *idx = g + (r > 0 ? 1 : 0);
     }
 }
 static_assert(sizeof(Task) == 16, "Task is 16 bytes");

@@ -188,7 +188,7 @@ __device__ void run_task(const Task &t, const ExecParams &p, const Dims<T> &d, T
         int info;
         if constexpr (std::is_same<T, float>::value) {
             if (p.full_inv) info = rec::tile_potrf_inv<T, SP>(d.A(t.k, t.k), d.X(t.k), d.tm(t.k), smem);
-            else if (d.tm(t.k) <= psm::MAXN) info = psm::potrf(d.A(t.k, t.k), d.tm(t.k), d.inv(t.k), smem);
+            else if (d.tm(t.k) <= psm::MAXN) info = psm::potrf(d.A(t.k, t.k), d.tm(t.k), d.inv(t.k), smem, ph);
             else info = rec::tile_potrf_blk<T, SP>(d.A(t.k, t.k), d.tm(t.k), d.inv(t.k), smem, ph);
         } else {
             info = rec::tile_potrf_blk<T, SP>(d.A(t.k, t.k), d.tm(t.k), d.inv(t.k), smem, ph);

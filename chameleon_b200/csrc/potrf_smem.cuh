@@ -13,8 +13,8 @@
 // Layout: the lower triangle by 64-wide block columns; block column b holds
 // rows 64 b .. n-1, column-major with a leading dimension rounded up to a
 // multiple of 4 (float4 row loads).  Right-looking over block columns:
-//   leaf:     D_bb = L_bb L_bb^T and X_b = L_bb^-1 (64 x 64, registers: each
-//             thread owns a 4 x 4 block; one barrier per column)
+//   leaf:     D_bb = L_bb L_bb^T and X_b = L_bb^-1 (the warp-level 64 x 64
+//             leaf of rec.cuh on a staged copy of the block)
 //   panel:    L_ib = A_ib X_b^T                      (i > b)
 //   trailing: A_ij -= L_ib L_jb^T                    (i >= j > b)
 // Same contract as CORE_spotrf on a lower view (coreblas/compute/core_zpotrf.c
@@ -30,7 +30,8 @@ namespace psm {
 
 constexpr int MAXN = 256;   // largest tile order
 constexpr int BW = 64;      // block-column width (= IB)
-constexpr int LDI = 65;     // leading dimension of the block inverse in shared memory
+constexpr int LDI = 65;     // leading dimension of the staged block and its inverse
+static_assert(LDI == rec::LDS, "the staged leaf uses the leading dimension of rec.cuh");
 
 __host__ __device__ constexpr int blk_ld(int n, int b) { return ((n - BW * b) + 3) & ~3; }
 __host__ __device__ constexpr int blk_off(int n, int b) {
@@ -38,117 +39,35 @@ __host__ __device__ constexpr int blk_off(int n, int b) {
     for (int i = 0; i < b; ++i) o += BW * blk_ld(n, i);
     return o;
 }
-// Shared memory: the block columns, the block inverse, two 64-float broadcast
-// buffers, the info word (floats; 16-byte aligned base).
-constexpr int SMEM_FLOATS = blk_off(MAXN, MAXN / BW) + BW * LDI + 2 * BW + 8;
+// Shared memory: the block columns, the staged diagonal block and its inverse
+// (floats; 16-byte aligned base).
+constexpr int SMEM_FLOATS = blk_off(MAXN, MAXN / BW) + 2 * BW * LDI + 8;
 constexpr size_t SMEM_BYTES = (size_t)SMEM_FLOATS * sizeof(float);
 
 // Cholesky of the nbk x nbk block (nbk <= 64) at D (column-major, ld ldd,
-// lower triangle) in place, and its inverse into Xs (ld LDI, 64 x 64 written
-// in full: zeros above the diagonal and outside nbk).  cbuf: 128 floats.
-// Returns LAPACK info (1-based column of the first non-positive pivot).
-// All 256 threads; ends with a barrier.
-static __device__ __noinline__ int leaf(float *D, int ldd, int nbk, float *Xs, float *cbuf) {
-    const int tid = threadIdx.x;
-    const int r0 = 4 * (tid >> 4), c0 = 4 * (tid & 15);   // this thread's 4 x 4 block
-    float a[4][4];
-#pragma unroll
-    for (int e = 0; e < 4; ++e)
-#pragma unroll
-        for (int f = 0; f < 4; ++f) {
-            const int r = r0 + e, c = c0 + f;
-            a[e][f] = (r < nbk && c < nbk && r >= c) ? D[c * ldd + r] : 0.f;
-        }
-    if (c0 == 0) {
-#pragma unroll
-        for (int e = 0; e < 4; ++e) cbuf[r0 + e] = a[e][0];
+// lower triangle) in place, and its inverse into Xs (ld LDI, 64 x 64: zeros
+// above the diagonal and outside nbk).  The block is staged, identity-padded,
+// into sD (64 x LDI) for the warp-level 64 x 64 leaf of rec.cuh (32 x 32
+// Cholesky and inverse kernels in rolled form).  Returns LAPACK info.  All 256
+// threads; ends with a barrier.
+static __device__ __noinline__ int leaf(float *D, int ldd, int nbk, float *sD, float *Xs) {
+    for (int idx = threadIdx.x; idx < 64 * 64; idx += NT_CTA) {
+        const int r = idx & 63, c = idx >> 6;
+        float v = (r == c) ? 1.f : 0.f;
+        if (r < nbk && c < nbk) v = (r >= c) ? D[c * ldd + r] : 0.f;
+        sD[c * LDI + r] = v;
     }
     __syncthreads();
-    int info = 0;
-    for (int j = 0; j < nbk; ++j) {
-        const float *col = cbuf + (j & 1) * BW;   // column j after its j updates
-        const float d = col[j];
-        if (!(d > 0.f)) {   // uniform: every thread reads the same pivot (also catches NaN)
-            info = j + 1;
-            break;
-        }
-        const float rs = rec::rsqrt_wp(d);
-        float li[4], lc[4];
-#pragma unroll
-        for (int e = 0; e < 4; ++e) li[e] = col[r0 + e] * rs;
-#pragma unroll
-        for (int f = 0; f < 4; ++f) lc[f] = col[c0 + f] * rs;
-#pragma unroll
-        for (int e = 0; e < 4; ++e)
-#pragma unroll
-            for (int f = 0; f < 4; ++f) {
-                const int r = r0 + e, c = c0 + f;
-                if (c > j && r >= c && r < nbk) a[e][f] -= li[e] * lc[f];
-            }
-        // column j is final: L(i, j) = col[i] / sqrt(d), L(j, j) = sqrt(d)
-#pragma unroll
-        for (int f = 0; f < 4; ++f)
-            if (c0 + f == j) {
-#pragma unroll
-                for (int e = 0; e < 4; ++e)
-                    if (r0 + e >= j) a[e][f] = (r0 + e == j) ? d * rs : li[e];
-            }
-        // column j + 1 (now updated by all j + 1 columns) to the other buffer
-        if (j + 1 < nbk) {
-#pragma unroll
-            for (int f = 0; f < 4; ++f)
-                if (c0 + f == j + 1) {
-#pragma unroll
-                    for (int e = 0; e < 4; ++e) cbuf[((j + 1) & 1) * BW + r0 + e] = a[e][f];
-                }
-        }
-        __syncthreads();
-    }
+    const int info = rec::leaf64_core<float, true>(sD, Xs);
     if (info) return info;
-#pragma unroll
-    for (int e = 0; e < 4; ++e)
-#pragma unroll
-        for (int f = 0; f < 4; ++f) {
-            const int r = r0 + e, c = c0 + f;
-            if (r < nbk && c < nbk && r >= c) D[c * ldd + r] = a[e][f];
+    for (int idx = threadIdx.x; idx < 64 * 64; idx += NT_CTA) {
+        const int r = idx & 63, c = idx >> 6;
+        if (r < nbk && c < nbk) {
+            if (r >= c) D[c * ldd + r] = sD[c * LDI + r];
+        } else {
+            Xs[c * LDI + r] = 0.f;   // the identity padding's inverse
         }
-    __syncthreads();
-    // X = L^-1 by rows: row i is final once divided by L(i, i); it then
-    // updates the rows below (x(r, c) -= L(r, i) x(i, c)).
-    float x[4][4];
-#pragma unroll
-    for (int e = 0; e < 4; ++e)
-#pragma unroll
-        for (int f = 0; f < 4; ++f) x[e][f] = (r0 + e == c0 + f && r0 + e < nbk) ? 1.f : 0.f;
-    for (int i = 0; i < nbk; ++i) {
-        float *row = cbuf + (i & 1) * BW;
-        if (i >= r0 && i < r0 + 4) {
-            const float inv = 1.f / D[i * ldd + i];
-#pragma unroll
-            for (int e = 0; e < 4; ++e)
-                if (r0 + e == i) {
-#pragma unroll
-                    for (int f = 0; f < 4; ++f) {
-                        x[e][f] *= inv;   // zero for c > i
-                        row[c0 + f] = x[e][f];
-                    }
-                }
-        }
-        __syncthreads();
-        float lr[4], xr[4];
-#pragma unroll
-        for (int e = 0; e < 4; ++e) lr[e] = (r0 + e > i && r0 + e < nbk) ? D[i * ldd + r0 + e] : 0.f;
-#pragma unroll
-        for (int f = 0; f < 4; ++f) xr[f] = row[c0 + f];
-#pragma unroll
-        for (int e = 0; e < 4; ++e)
-#pragma unroll
-            for (int f = 0; f < 4; ++f) x[e][f] -= lr[e] * xr[f];
     }
-#pragma unroll
-    for (int e = 0; e < 4; ++e)
-#pragma unroll
-        for (int f = 0; f < 4; ++f) Xs[(c0 + f) * LDI + r0 + e] = x[e][f];
     __syncthreads();
     return 0;
 }
@@ -191,26 +110,69 @@ static __device__ __forceinline__ void gemm64(Frag &acc, const float *Xm, int ld
 // Factor the n x n lower view T (n <= MAXN) through shared memory `sm`
 // (SMEM_BYTES, 16-byte aligned); inverted blocks to invd.  Returns info.
 // All 256 threads.
-static __device__ int potrf(const ViewF &T, int n, float *invd, float *sm) {
+static __device__ int potrf(const ViewF &T, int n, float *invd, float *sm, unsigned *ph = nullptr) {
     const int tid = threadIdx.x;
     const int nb = (n + BW - 1) / BW;
     float *Xs = sm + blk_off(n, nb);
-    float *cbuf = Xs + BW * LDI;
-    // load the lower triangle (coalesced along the contiguous direction of T)
+    // tracing (ph != null): thread 0 adds the clock cycles of the leaves, the
+    // panel products and the trailing updates (with the load and the
+    // write-back) to ph[0..2]
+    long long c0 = (ph && tid == 0) ? clock64() : 0;
+    auto lap = [&](int i) {
+        if (ph && tid == 0) {
+            const long long c1 = clock64();
+            ph[i] += (unsigned)(c1 - c0);
+            c0 = c1;
+        }
+    };
+    // Load block column b (rows 64 b .. n-1, all 64 columns; the part above
+    // the diagonal is never read).  A column-major tile with 16-byte aligned
+    // columns is copied with 16-byte cp.async, every copy of the tile in
+    // flight at once; otherwise element by element, coalesced along the
+    // contiguous direction, eight loads in flight per thread.
     const bool colmajor = (T.rs == 1);
-    for (int idx = tid; idx < n * n; idx += NT_CTA) {
-        const int i = colmajor ? idx % n : idx / n, j = colmajor ? idx / n : idx % n;
-        if (i >= j) {
-            const int b = j / BW;
-            sm[blk_off(n, b) + (j - BW * b) * blk_ld(n, b) + (i - BW * b)] = *T.at(i, j);
+    const bool vec = colmajor && ((reinterpret_cast<uintptr_t>(T.p) & 15) == 0) && (T.cs % 4 == 0);
+    if (vec) {
+        for (int b = 0; b < nb; ++b) {
+            const int rows = n - BW * b, ld = blk_ld(n, b), nq = ld / 4, wb = min(BW, n - BW * b);
+            float *Sb = sm + blk_off(n, b);
+            for (int idx = tid; idx < nq * wb; idx += NT_CTA) {
+                const int q = idx % nq, c = idx / nq, r = 4 * q;
+                const int nv = max(0, min(4, rows - r));
+                const float *src = T.at(BW * b + r, BW * b + c);
+                cp_async16(Sb + c * ld + r, nv ? src : T.p, nv * 4);
+            }
+        }
+        cp_async_commit();
+        cp_async_wait<0>();
+    } else {
+        for (int idx0 = tid; idx0 < n * n; idx0 += 8 * NT_CTA) {
+            float v[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const int idx = idx0 + u * NT_CTA;
+                const int i = colmajor ? idx % n : idx / n, j = colmajor ? idx / n : idx % n;
+                v[u] = (idx < n * n && i >= j) ? *T.at(i, j) : 0.f;
+            }
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const int idx = idx0 + u * NT_CTA;
+                const int i = colmajor ? idx % n : idx / n, j = colmajor ? idx / n : idx % n;
+                if (idx < n * n && i >= j) {
+                    const int b = j / BW;
+                    sm[blk_off(n, b) + (j - BW * b) * blk_ld(n, b) + (i - BW * b)] = v[u];
+                }
+            }
         }
     }
     __syncthreads();
+    lap(2);
     int info = 0;
     for (int b = 0; b < nb; ++b) {
         float *Sb = sm + blk_off(n, b);
         const int ldb = blk_ld(n, b), nbk = min(BW, n - BW * b);
-        const int linfo = leaf(Sb, ldb, nbk, Xs, cbuf);
+        const int linfo = leaf(Sb, ldb, nbk, Xs + BW * LDI, Xs);
+        lap(0);
         if (linfo) {
             info = BW * b + linfo;
             break;
@@ -236,6 +198,7 @@ static __device__ int potrf(const ViewF &T, int n, float *invd, float *sm) {
                     }
             __syncthreads();
         }
+        lap(1);
         // trailing: block columns c > b
         for (int cb = b + 1; cb < nb; ++cb) {
             float *Sc = sm + blk_off(n, cb);
@@ -255,16 +218,29 @@ static __device__ int potrf(const ViewF &T, int n, float *invd, float *sm) {
                     }
         }
         __syncthreads();
+        lap(2);
     }
-    // write back the lower triangle
-    for (int idx = tid; idx < n * n; idx += NT_CTA) {
-        const int i = colmajor ? idx % n : idx / n, j = colmajor ? idx / n : idx % n;
-        if (i >= j) {
-            const int b = j / BW;
-            *T.at(i, j) = sm[blk_off(n, b) + (j - BW * b) * blk_ld(n, b) + (i - BW * b)];
+    // write back the lower triangle, block column by block column: groups of
+    // four rows entirely below the diagonal as one 16-byte store when the tile
+    // allows it, the rest element by element (the upper triangle is never
+    // written)
+    for (int b = 0; b < nb; ++b) {
+        const int rows = n - BW * b, ld = blk_ld(n, b), nq = ld / 4, wb = min(BW, n - BW * b);
+        const float *Sb = sm + blk_off(n, b);
+        for (int idx = tid; idx < nq * wb; idx += NT_CTA) {
+            const int q = colmajor ? idx % nq : idx / wb, c = colmajor ? idx / nq : idx % wb, r = 4 * q;
+            if (vec && r >= c + 3 && r + 4 <= rows) {
+                *reinterpret_cast<float4 *>(T.at(BW * b + r, BW * b + c)) =
+                    *reinterpret_cast<const float4 *>(Sb + c * ld + r);
+            } else {
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+                    if (r + u < rows && r + u >= c) *T.at(BW * b + r + u, BW * b + c) = Sb[c * ld + r + u];
+            }
         }
     }
     __syncthreads();
+    lap(2);
     return info;
 }
 

@@ -102,6 +102,56 @@ __device__ __noinline__ void warp_trinv32(const T *S, T *Xs) {
     __syncwarp();
 }
 
+// Rolled forms of the two warp kernels above: the same arithmetic per entry,
+// in a loop of 32 identical steps whose code (~1-2 KB) stays in the
+// instruction cache.  Register indices stay static by shifting: at step j,
+// slot k of a lane holds the entry of column (row) j + k, and the update of
+// slot k writes slot k - 1, so slot 0 is always the current column (row) and
+// the shift costs no moves.
+template <class T>
+__device__ __noinline__ int warp_chol32r(T *S) {
+    const int lane = threadIdx.x & 31;
+    T a[32];   // a[k]: entry (lane, j + k)
+#pragma unroll
+    for (int c = 0; c < 32; ++c) a[c] = (c <= lane) ? S[lane + c * LDS] : T(0);
+    int info = 0;
+#pragma unroll 1
+    for (int j = 0; j < 32; ++j) {
+        T d = __shfl_sync(FULL, a[0], j);
+        if (!(d > T(0))) {   // also catches NaN
+            if (info == 0) info = j + 1;
+            d = T(1);
+        }
+        const T r = rsqrt_wp(d);
+        const T l = (lane == j) ? d * r : a[0] * r;
+        if (lane >= j) S[lane + j * LDS] = l;
+#pragma unroll
+        for (int k = 1; k < 32; ++k) a[k - 1] = a[k] - l * __shfl_sync(FULL, l, (j + k) & 31);
+        a[31] = T(0);
+    }
+    __syncwarp();
+    return info;
+}
+
+// X = L^-1 for the 32 x 32 lower block at S, lane c = column c of X, slot k =
+// row i + k at step i (the entries of columns of L are broadcast loads).
+template <class T>
+__device__ __noinline__ void warp_trinv32r(const T *S, T *Xs) {
+    const int lane = threadIdx.x & 31;
+    T x[32];
+#pragma unroll
+    for (int k = 0; k < 32; ++k) x[k] = (k == lane) ? T(1) : T(0);
+#pragma unroll 1
+    for (int i = 0; i < 32; ++i) {
+        const T xi = x[0] * (T(1) / S[i + i * LDS]);   // X(i, lane), final (zero above the diagonal)
+        Xs[i + lane * LDS] = xi;
+#pragma unroll
+        for (int k = 1; k < 32; ++k) x[k - 1] = x[k] - S[((i + k) & 31) + i * LDS] * xi;
+        x[31] = T(0);
+    }
+    __syncwarp();
+}
+
 // out(i, c) = sum_{k<32} P[i + k*LDS] * Q[c + k*LDS] (ROWS_Q: Q read as
 // rows) or Q[k + c*LDS] (Q read as columns), 32 x 32 outputs spread over the
 // CTA: thread (i = tid & 31, cg = tid >> 5) owns columns 4cg .. 4cg+3.
@@ -134,13 +184,13 @@ __device__ __noinline__ int leaf64_core(T *sD, T *sX) {
     __syncthreads();
     if (FACT) {
         if (warp == 0) {
-            const int info = warp_chol32(sD);
+            const int info = warp_chol32r(sD);
             if (tid == 0) s_info = info;
         }
         __syncthreads();
         if (s_info) return s_info;
     }
-    if (warp == 0) warp_trinv32(sD, sX);
+    if (warp == 0) warp_trinv32r(sD, sX);
     __syncthreads();
     T o[4];
     const int i = tid & 31, cg = tid >> 5;
@@ -160,13 +210,13 @@ __device__ __noinline__ int leaf64_core(T *sD, T *sX) {
         }
         __syncthreads();
         if (warp == 0) {
-            const int info = warp_chol32(sD + 32 + 32 * LDS);
+            const int info = warp_chol32r(sD + 32 + 32 * LDS);
             if (tid == 0) s_info = info ? 32 + info : 0;
         }
         __syncthreads();
         if (s_info) return s_info;
     }
-    if (warp == 1) warp_trinv32(sD + 32 + 32 * LDS, sX + 32 + 32 * LDS);
+    if (warp == 1) warp_trinv32r(sD + 32 + 32 * LDS, sX + 32 + 32 * LDS);
     __syncthreads();
     // W = L21 X11 into the upper-right block of sX (zero in the inverse)
     small_mm32<T, false>(sD + 32, sX, o);

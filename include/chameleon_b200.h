@@ -71,7 +71,7 @@ typedef enum {
                                              factorizations; 0: any CTA (default) */
 #define CHAMELEON_B200_UPD_GROUP_F64  109 /* panels applied per trailing-update task, FP64 path (default 1) */
 #define CHAMELEON_B200_UPD_GROUP_F32  110 /* the same, FP32 split products on mma.sync (default 1) */
-#define CHAMELEON_B200_UPD_GROUP_TC   111 /* the same, FP32 BF16x3 on tcgen05 (default 4) */
+#define CHAMELEON_B200_UPD_GROUP_TC   111 /* the same, FP32 BF16x3 on tcgen05 (default 8) */
 #define CHAMELEON_B200_FACTOR_NB      112 /* tile size of the mixed solver's FP32 factorization;
                                              0: the tile size of A (default 256 when it divides A's) */
 

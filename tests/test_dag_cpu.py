@@ -17,11 +17,13 @@ SUBB = 128
 FACT, SOLVE, XINV, NOINV = 1, 2, 4, 8
 
 
-def ngroups(n, G):
+def ngroups(n, G, tail=2):
     """Update groups of tile column n (upd_ngroups in executor.cuh): the last
-    panel n-1 alone, the panels before it in groups of G aligned at multiples
-    of G."""
-    return 0 if n <= 0 else -(-(n - 1) // G) + 1
+    `tail` panels alone, the panels before them in groups of G aligned at the
+    end (the first group takes the remainder)."""
+    if n <= tail:
+        return max(n, 0)
+    return -(-(n - tail) // G) + tail
 
 
 def geometry(N, NB, nrhs, NBB):
