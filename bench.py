@@ -686,9 +686,16 @@ def b200_arm(args, world, rank, local):
             e2e_step()
         L.CHAM_B200_Event_Record(5)
         ems = L.CHAM_B200_Event_Elapsed(4, 5) / ne
-        e2e = {"value": flops / (ems * 1e-3) / 1e12, "unit": "TFLOP/s", "h2d_bytes_per_step": 8 * N * N + 8 * N * nrhs,
+        # the referenced triangle of A moves, one tile column of the FP32
+        # factor's tiling at a time, while the factorization runs
+        fnb = cb.get_param(cb.CHAMELEON_B200_FACTOR_NB)
+        fnb = fnb if (0 < fnb < NB and NB % fnb == 0) else NB
+        tri_bytes = sum(8 * (N - q * fnb) * min(fnb, N - q * fnb) for q in range((N + fnb - 1) // fnb))
+        e2e = {"value": flops / (ems * 1e-3) / 1e12, "unit": "TFLOP/s", "h2d_bytes_per_step": tri_bytes + 8 * N * nrhs,
                "d2h_bytes_per_step": 8 * N * nrhs, "ms_per_step": ems,
-               "api": "CHAMELEON_dsposv (LAPACK layout, pinned host A/B/X)"}
+               "api": "CHAMELEON_dsposv (LAPACK layout, pinned host A/B/X; the lower triangle of A streams in "
+                      "tile column by tile column while the factorization casts and factors the columns that "
+                      "have landed)"}
         del hA
 
     cond = conditioning_section(args, cb, rank) if args.cond else None

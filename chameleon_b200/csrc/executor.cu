@@ -48,22 +48,27 @@ static const Calib kCalib[3] = {
 
 struct Shape {
     int mode, N, NB, nrhs, NBB, P, prof, G;   // G: update group size (upd_group_of)
+    int h2d_gbs;                              // MODE_CAST: host-to-device bandwidth of the model (GB/s)
     bool operator==(const Shape &o) const {
         return mode == o.mode && N == o.N && NB == o.NB && nrhs == o.nrhs && NBB == o.NBB && P == o.P &&
-               prof == o.prof && G == o.G;
+               prof == o.prof && G == o.G && h2d_gbs == o.h2d_gbs;
     }
 };
 struct ShapeHash {
     size_t operator()(const Shape &s) const {
         size_t h = 1469598103934665603ull;
-        for (int v : {s.mode, s.N, s.NB, s.nrhs, s.NBB, s.P, s.prof, s.G}) h = (h ^ (size_t)v) * 1099511628211ull;
+        for (int v : {s.mode, s.N, s.NB, s.nrhs, s.NBB, s.P, s.prof, s.G, s.h2d_gbs})
+            h = (h ^ (size_t)v) * 1099511628211ull;
         return h;
     }
 };
 
+constexpr int TK_COPY = 100;   // model only: the host-to-device copy of one tile column (not emitted)
+
 struct Coarse {
     int16_t kind, m, n, k, bn;   // TK_UPD: k = first panel of the group, bn = panel count
     int grp;                     // TK_UPD: index of the group in tile column n
+    bool virt = false;           // model-only task: runs on the copy engine, not on a CTA
     int nsub;
     double dur;               // duration of one sub-task (model units)
     std::vector<int> succ;
@@ -101,6 +106,8 @@ std::vector<Task> build_order(const Shape &s) {
     };
     // ids: potrf[k], trsm[m,k], upd[m,n,k] (last update of tile (m,n) so far)
     std::vector<int> P(NT, -1), XI(NT, -1), Tr((size_t)NT * NT, -1), lastU((size_t)NT * NT, -1);
+    std::vector<int> Cst((size_t)NT * NT, -1);   // MODE_CAST: cast task of tile (m, n)
+    const bool cast = fact && (s.mode & MODE_CAST);
     const bool xinv = s.mode & MODE_XINV;
     const double nb = s.NB;
     const Calib &cal = kCalib[(s.prof >= 0 && s.prof < 3) ? s.prof : 0];
@@ -121,11 +128,33 @@ std::vector<Task> build_order(const Shape &s) {
         return lat ? 13.0 + 0.01 * t : cal.strsm * 3.0 * t * t * w / parts;
     };
     auto c_supd = [&](double t, double w) { return lat ? 8.0 + 0.04 * t : cal.supd * 2.0 * SUBB * t * w; };
+    if (cast) {
+        // the copy engine delivers the stored triangle one tile column after
+        // the other (model-only tasks, in order); each tile's cast waits for
+        // its column
+        const double gbs = std::max(1, s.h2d_gbs);
+        int prev = -1;
+        for (int q = 0; q < NT; ++q) {
+            const double rows = (s.mode & MODE_CAST) ? (double)(s.N - q * s.NB) : 0.0;
+            const double us = lat ? rows * tm(q) * 8.0 / (gbs * 1e3) : 0.0;
+            const int cp = add(TK_COPY, q, q, q, 0, 1, us);
+            ct[cp].virt = true;
+            edge(prev, cp);
+            prev = cp;
+            // a column's copy covers tile column q of the lower triangle, or
+            // tile row q's stored tiles of the upper one: the same tiles by symmetry
+            for (int m = q; m < NT; ++m) {
+                Cst[m + (size_t)NT * q] = add(TK_CAST, m, q, q, 0, 1, lat ? 8.0 * tm(m) * tm(q) / 65536.0 : 1.0);
+                edge(cp, Cst[m + (size_t)NT * q]);
+            }
+        }
+    }
     if (fact) {
         for (int k = 0; k < NT; ++k) {
             const double tk = tm(k);
             P[k] = add(TK_POTRF, k, k, k, 0, 1, c_potrf(tk));
             edge(lastU[k + (size_t)NT * k], P[k]);
+            if (k == 0) edge(Cst[0], P[k]);
             if (xinv && solve) {
                 XI[k] = add(TK_XINV, k, k, k, 0, 1, c_xinv(tk));
                 edge(P[k], XI[k]);
@@ -134,6 +163,7 @@ std::vector<Task> build_order(const Shape &s) {
                 const int id = add(TK_TRSM, m, k, k, 0, nbi(m), c_trsm());
                 edge(P[k], id);
                 edge(lastU[m + (size_t)NT * k], id);
+                if (k == 0) edge(Cst[m], id);
                 Tr[m + (size_t)NT * k] = id;
             }
             // the update groups of each later tile column whose last panel is k
@@ -147,6 +177,7 @@ std::vector<Task> build_order(const Shape &s) {
                     const double dur = c_upd(cnt);
                     const int id = add(TK_UPD, m, n, k0, cnt, sub, dur);
                     ct[id].grp = gi;
+                    if (gi == 0) edge(Cst[m + (size_t)NT * n], id);
                     edge(Tr[m + (size_t)NT * k], id);
                     if (m != n) edge(Tr[n + (size_t)NT * k], id);
                     edge(lastU[m + (size_t)NT * n], id);
@@ -213,14 +244,20 @@ std::vector<Task> build_order(const Shape &s) {
     std::priority_queue<Ready> ready;
     std::priority_queue<Fin> running;
     std::vector<int> started(ct.size(), 0), finished(ct.size(), 0);
+    double now = 0;
+    // model-only tasks start as soon as they are ready, without a worker
+    auto make_ready = [&](int i) {
+        if (ct[i].virt) running.push({now + ct[i].dur, i});
+        else ready.push({ct[i].blevel, i});
+    };
     for (int i = 0; i < (int)ct.size(); ++i)
-        if (ct[i].npred == 0) ready.push({ct[i].blevel, i});
+        if (ct[i].npred == 0) make_ready(i);
     std::vector<Task> out;
     size_t total = 0;
-    for (auto &c : ct) total += c.nsub;
+    for (auto &c : ct)
+        if (!c.virt) total += c.nsub;
     out.reserve(total);
     int free_w = s.P;
-    double now = 0;
     auto emit = [&](const Coarse &c, int j) {
         Task t{};
         t.kind = c.kind; t.m = c.m; t.n = c.n; t.k = c.k; t.bn = c.bn; t.sub = 0; t.grp = c.grp;
@@ -258,10 +295,10 @@ std::vector<Task> build_order(const Shape &s) {
         const Fin f = running.top();
         running.pop();
         now = f.t;
-        ++free_w;
+        if (!ct[f.id].virt) ++free_w;
         if (++finished[f.id] == ct[f.id].nsub) {
             for (int sidx : ct[f.id].succ)
-                if (--ct[sidx].npred == 0) ready.push({ct[sidx].blevel, sidx});
+                if (--ct[sidx].npred == 0) make_ready(sidx);
         }
     }
     return out;
@@ -345,7 +382,7 @@ void free_exec_ws(ExecWs &w) {
 }
 
 int run_cholesky_dag(int mode, cham_uplo_t uplo, CHAM_desc_t *A, CHAM_desc_t *B, cudaStream_t s,
-                     ExecResult *res, int split, ExecWs *wsp, int grid_req, int flags) {
+                     ExecResult *res, int split, ExecWs *wsp, int grid_req, int flags, const CastIn *cin) {
     Context &c = ctx();
     ExecWs &w = wsp ? *wsp : g_ws;
     const int N = A->n;
@@ -358,6 +395,10 @@ int run_cholesky_dag(int mode, cham_uplo_t uplo, CHAM_desc_t *A, CHAM_desc_t *B,
     res->info = 0; res->error = 0; res->ms = 0.f;
     if (N == 0) return 0;
     if (nrhs && B->dtyp != A->dtyp) return CHAMELEON_ERR_ILLEGAL_VALUE;
+    if (cin) {
+        if (!f32 || !(mode & MODE_FACT)) return CHAMELEON_ERR_ILLEGAL_VALUE;
+        mode |= MODE_CAST;
+    }
     // tcgen05 trailing updates: FP32 factorization with BF16x3 products and
     // 64-aligned tiles (the split chunks are 64 wide in k).
     const bool tc = f32 && split == SPLIT_BF16X3 && (mode & MODE_FACT) && (NB % tc05::BK == 0) && NT > 1 &&
@@ -390,11 +431,11 @@ int run_cholesky_dag(int mode, cham_uplo_t uplo, CHAM_desc_t *A, CHAM_desc_t *B,
     // update group size: fused k steps amortize the C round trip and the
     // dispatch of an update over G panels (CHAMELEON_B200_UPD_GROUP per path)
     const int G = std::max(1, prof == PROF_FP64 ? c.kgroup_f64 : (tc ? c.kgroup_tc : c.kgroup_f32));
-    Shape sh{mode, canonN, NB, canonR, NBB, grid, prof, G};
+    Shape sh{mode, canonN, NB, canonR, NBB, grid, prof, G, cin ? std::max(1, cin->h2d_gbs) : 0};
     Schedule *sch = get_schedule(sh);
     if (!sch) return CHAMELEON_ERR_OUT_OF_RESOURCES;
     const int NIB = (NB + IB - 1) / IB;
-    const size_t nctr = (size_t)2 * NT * NT + (size_t)4 * NT * std::max(NTB, 1) + NT;
+    const size_t nctr = (size_t)(cin ? 3 : 2) * NT * NT + (size_t)4 * NT * std::max(NTB, 1) + NT;
     const size_t esz = f32 ? sizeof(float) : sizeof(double);
     const size_t inv_elems = full_inv ? (size_t)NT * NB * NB : (size_t)NT * NIB * IB * IB;
     rc = ensure_ws(w, nctr * sizeof(int), inv_elems * esz);
@@ -435,6 +476,15 @@ int run_cholesky_dag(int mode, cham_uplo_t uplo, CHAM_desc_t *A, CHAM_desc_t *B,
     p.NIB = NIB;
     p.full_inv = full_inv ? 1 : 0;
     p.xinvDone = p.bwdDone + nb4;
+    if (cin) {
+        p.castDone = p.xinvDone + NT;
+        p.csrc = cin->src;
+        p.csrc_ld = cin->ld;
+        p.carrive = cin->arrive;
+        p.cepoch = cin->epoch;
+        p.colsum = cin->colsum;
+        p.covf = cin->ovf;
+    }
     p.xinv = nullptr;
     if (xinv) {
         const size_t xbytes = (size_t)NT * NB * NB * sizeof(float);
@@ -538,7 +588,8 @@ extern "C" int CHAM_B200_Trace_Read(void *host_out, int count) {
 extern "C" int CHAM_B200_Schedule_Build(int mode, int N, int NB, int nrhs, int NBB, int workers, int prof, int kgroup,
                                         void *out, int cap) {
     using namespace chb;
-    const std::vector<Task> t = build_order(Shape{mode, N, NB, nrhs, NBB, workers, prof, std::max(1, kgroup)});
+    const std::vector<Task> t =
+        build_order(Shape{mode, N, NB, nrhs, NBB, workers, prof, std::max(1, kgroup), (mode & MODE_CAST) ? 50 : 0});
     const int n = std::min<int>((int)t.size(), cap);
     memcpy(out, t.data(), sizeof(Task) * (size_t)n);
     return n;
@@ -546,5 +597,6 @@ extern "C" int CHAM_B200_Schedule_Build(int mode, int N, int NB, int nrhs, int N
 // Number of tasks of the schedule of a given shape (for tests and tracing).
 extern "C" int CHAM_B200_Schedule_Size(int mode, int N, int NB, int nrhs, int NBB, int workers, int prof, int kgroup) {
     using namespace chb;
-    return (int)build_order(Shape{mode, N, NB, nrhs, NBB, workers, prof, std::max(1, kgroup)}).size();
+    return (int)build_order(Shape{mode, N, NB, nrhs, NBB, workers, prof, std::max(1, kgroup), (mode & MODE_CAST) ? 50 : 0})
+        .size();
 }

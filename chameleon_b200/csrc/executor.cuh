@@ -24,6 +24,8 @@ enum TaskKind : int16_t {
     TK_BWD_UPD = 7,   // B(m) -= L(k,m)^T B(k)          (m < k)
     TK_INV = 8,       // invert inner diagonal blocks of an existing factor (potrs alone)
     TK_XINV = 9,      // full inverse of diagonal tile k (FP32 substitution steps)
+    TK_CAST = 10,     // (MODE_CAST) FP64 -> FP32 copy of tile (m,n) once its columns have
+                      // arrived from the host, with its share of ||A||_inf
 };
 
 // TK_UPD applies the panels k .. k + bn - 1 of one k group (one accumulator,
@@ -73,7 +75,10 @@ static_assert(sizeof(Task) == 16, "Task is 16 bytes");
 // MODE_XINV: the substitution steps apply full inverses of the diagonal tiles
 // (one GEMM per tile), computed by TK_XINV tasks; with MODE_NOINV (solve only)
 // the inverses are already in place from an earlier launch on the same factor.
-enum ExecMode : int { MODE_FACT = 1, MODE_SOLVE = 2, MODE_XINV = 4, MODE_NOINV = 8 };
+// MODE_CAST: the FP32 tiles of A are produced inside the launch by TK_CAST
+// tasks from an FP64 column-major copy of A that is still arriving from the
+// host: each tile's first consumer waits for its cast.
+enum ExecMode : int { MODE_FACT = 1, MODE_SOLVE = 2, MODE_XINV = 4, MODE_NOINV = 8, MODE_CAST = 16 };
 
 constexpr int SUBB = 128;      // sub-block edge of trailing updates / row blocks
 
@@ -130,6 +135,18 @@ struct ExecParams {
     uint8_t *split;
     int split_nrb, split_nkc;   // 128-row blocks and 64-wide k chunks per panel tile
     int kgroup;                 // update group size G (upd_ngroups / upd_group_of)
+    // MODE_CAST: the FP64 source (column-major, ld csrc_ld) of the stored
+    // triangle; tile column q of it has arrived once carrive[q] >= cepoch
+    // (written by the copy engine after the column's data); castDone counts
+    // the casts per tile; colsum receives the absolute row sums of the
+    // symmetric matrix (its infinity norm), covf is set on a value beyond FP32
+    const double *csrc;
+    int64_t csrc_ld;
+    const int *carrive;
+    int cepoch;
+    int *castDone;
+    double *colsum;
+    int *covf;
     unsigned long long wait_budget_ns;
 };
 

@@ -75,10 +75,18 @@ __device__ Deps task_deps(const Task &t, const ExecParams &p, const Dims<T> &d) 
     switch (t.kind) {
     case TK_POTRF:
         need(0, &p.updA[t.k + p.NT * t.k], upd_ngroups(t.k, p.kgroup) * d.S(t.k, t.k));
+        if ((p.mode & MODE_CAST) && t.k == 0) need(1, &p.castDone[0], 1);
         break;
     case TK_TRSM:
         need(0, &p.panA[t.k + p.NT * t.k], 1);
         need(1, &p.updA[t.m + p.NT * t.k], upd_ngroups(t.k, p.kgroup) * d.S(t.m, t.k));
+        // tile column 0 has no update before its panel solve: wait for its cast
+        if ((p.mode & MODE_CAST) && t.k == 0) need(1, &p.castDone[t.m], 1);
+        break;
+    case TK_CAST:
+        // copy q delivers tile column q of the logical lower triangle (for
+        // Upper storage: block row q of the stored upper triangle)
+        need(0, &p.carrive[t.n], p.cepoch);
         break;
     case TK_UPD: {
         // the group's last panel being solved implies the earlier ones are
@@ -87,6 +95,8 @@ __device__ Deps task_deps(const Task &t, const ExecParams &p, const Dims<T> &d) 
         need(0, &p.panA[t.m + p.NT * kl], d.nbi(t.m));
         need(1, &p.panA[t.n + p.NT * kl], d.nbi(t.n));
         need(2, &p.updA[t.m + p.NT * t.n], t.grp * d.S(t.m, t.n));
+        // the first update of a tile is its first reader: wait for its cast
+        if ((p.mode & MODE_CAST) && t.grp == 0) need(2, &p.castDone[t.m + p.NT * t.n], 1);
         break;
     }
     case TK_INV:
@@ -160,6 +170,50 @@ __device__ inline bool wait_deps(const Deps &dp, const ExecParams &p, int task) 
 __device__ __forceinline__ uint8_t *split_tile(const ExecParams &p, int m, int k) {
     const size_t tile_bytes = (size_t)p.split_nrb * p.split_nkc * 2 * tc05::CHUNK_BYTES;
     return p.split + ((size_t)m * (m - 1) / 2 + k) * tile_bytes;
+}
+
+// TK_CAST: stored tile (p, q) of the FP64 source -> the same tile of the FP32
+// A (its stored orientation), plus the tile's share of the symmetric
+// infinity norm: absolute row sums go to colsum[p NB + i], column sums to
+// colsum[q NB + j] (on a diagonal tile only the referenced triangle counts,
+// its diagonal once).  Warp w takes stored rows w*32 + lane (+256, ...) and
+// walks the columns: every load is one coalesced 256-byte row segment, read
+// through L2 (the copy engine wrote it during this launch).  s_col: NB doubles.
+template <class T>
+__device__ void cast_tile(const Task &t, const ExecParams &p, const Dims<T> &d, double *s_col) {
+    const int P = p.upper ? t.n : t.m, Q = p.upper ? t.m : t.n;   // stored tile
+    const int rows = d.tm(P), cols = d.tm(Q);
+    const bool diag = (P == Q);
+    const double *src = p.csrc + (int64_t)P * p.NB + (int64_t)Q * p.NB * p.csrc_ld;
+    T *dst = static_cast<T *>(p.A) + p.a_off[P + p.NT * Q];
+    const int ldd = p.a_ld[P];
+    for (int j = threadIdx.x; j < cols; j += NT_CTA) s_col[j] = 0.0;
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int ovf = 0;
+    for (int r0 = warp * 32; r0 < rows; r0 += NT_CTA) {
+        const int i = r0 + lane;
+        const bool rv = i < rows;
+        double rs = 0.0;
+#pragma unroll 4
+        for (int j = 0; j < cols; ++j) {
+            const double v = rv ? __ldcg(src + i + (int64_t)j * p.csrc_ld) : 0.0;
+            if (rv) dst[i + (int64_t)j * ldd] = (T)v;
+            const bool ref = rv && (!diag || (p.upper ? i <= j : i >= j));
+            const double av = ref ? fabs(v) : 0.0;
+            ovf |= av > 3.4028234663852886e38;
+            if (!diag || i != j) rs += av;
+            double cs = av;
+#pragma unroll
+            for (int o = 16; o; o >>= 1) cs += __shfl_xor_sync(0xffffffffu, cs, o);
+            if (lane == 0 && cs != 0.0) atomicAdd(&s_col[j], cs);
+        }
+        if (rv && rs != 0.0) atomicAdd(&p.colsum[(int64_t)P * p.NB + i], rs);
+    }
+    __syncthreads();
+    for (int j = threadIdx.x; j < cols; j += NT_CTA)
+        if (s_col[j] != 0.0) atomicAdd(&p.colsum[(int64_t)Q * p.NB + j], s_col[j]);
+    if (ovf) atomicOr(p.covf, 1);
 }
 
 // Look-ahead of the dispatch loop, in shared memory.  A tcgen05 update task
@@ -297,6 +351,9 @@ __device__ void run_task(const Task &t, const ExecParams &p, const Dims<T> &d, T
     case TK_XINV:
         if constexpr (std::is_same<T, float>::value) rec::tile_trtri<T, SP>(d.A(t.k, t.k), d.XI(t.k), d.tm(t.k), smem);
         break;
+    case TK_CAST:
+        if constexpr (std::is_same<T, float>::value) cast_tile(t, p, d, reinterpret_cast<double *>(smem));
+        break;
     case TK_FWD_TRSM:
     case TK_BWD_TRSM: {
         const VT X = d.Bt(t.k, t.bn);
@@ -358,6 +415,7 @@ __device__ void run_task(const Task &t, const ExecParams &p, const Dims<T> &d, T
 
 __device__ inline int *task_counter(const Task &t, const ExecParams &p) {
     switch (t.kind) {
+    case TK_CAST: return &p.castDone[t.m + p.NT * t.n];
     case TK_POTRF:
     case TK_INV: return &p.panA[t.k + p.NT * t.k];
     case TK_XINV: return &p.xinvDone[t.k];

@@ -39,6 +39,9 @@ struct Context {
     // tile size of the mixed solver's FP32 copy of A (0: A's own tile size);
     // used when it divides A's tile size
     int factor_nb = 256;
+    // expected host-to-device copy bandwidth (GB/s): orders the tasks of a
+    // factorization that starts while its matrix is still arriving
+    int h2d_gbs = 50;
     int desc_ids = 0;
     std::mutex mu;
 };
@@ -172,6 +175,22 @@ int launch_posv_batch(std::vector<BatchItem> &items, double *A, double *B, int u
 void free_mixed_ws(MixedWs &m);
 void free_exec_ws(ExecWs &w);
 
+// A factorization whose FP32 tiles are cast inside the launch from an FP64
+// column-major copy of A that the copy engine is still writing (MODE_CAST):
+// tile column q has arrived once arrive[q] >= epoch.  colsum (N doubles,
+// zeroed by the caller) receives the row sums of |A| (symmetric), ovf is set
+// when a referenced value does not fit FP32.  h2d_gbs: expected copy
+// bandwidth, for the order of the task list.
+struct CastIn {
+    const double *src;
+    int64_t ld;
+    const int *arrive;
+    int epoch;
+    double *colsum;
+    int *ovf;
+    int h2d_gbs;
+};
+
 // Executor entry (executor.cu).
 struct ExecResult {
     int info = 0;     // >0: LAPACK-style order of the failing minor
@@ -186,15 +205,42 @@ struct ExecResult {
 // inverses a previous launch on the same workspace computed for this factor.
 enum ExecFlags : int { EXEC_REUSE_INV = 1 };
 int run_cholesky_dag(int mode, cham_uplo_t uplo, CHAM_desc_t *A, CHAM_desc_t *B, cudaStream_t s,
-                     ExecResult *res, int split = 0, ExecWs *ws = nullptr, int grid = 0, int flags = 0);
+                     ExecResult *res, int split = 0, ExecWs *ws = nullptr, int grid = 0, int flags = 0,
+                     const CastIn *cin = nullptr);
 
 // Tile size of the mixed solver's FP32 factorization for FP64 tile size NB (mixed.cu).
 int factor_tile(int NB);
 
+// A host matrix whose referenced triangle is being copied to dA (column-major,
+// ld) one tile column at a time; column q has landed once arrive[q] >= epoch
+// (tri_stream_start, mixed.cu); `done` is recorded after the last copy.
+struct TriStream {
+    double *dA;
+    int64_t ld;
+    const int *arrive;
+    int epoch;
+    cudaEvent_t done;
+    int h2d_gbs;
+};
+// Copy stream, flags and pinned epoch word of the triangle streaming.
+struct TriStreamState {
+    cudaStream_t cs = nullptr;
+    cudaEvent_t done = nullptr;
+    int *d_arrive = nullptr;
+    int cap = 0;
+    int *h_epoch = nullptr;
+    int epoch = 0;
+};
+int tri_stream_start(TriStreamState &ts, cham_uplo_t uplo, const double *hA, int lda, double *dA, int N, int nb,
+                     TriStream *out);
+
 // Mixed-precision solve on an explicit stream and workspaces (mixed.cu).
 // factored = true: m.A32 already holds the low-precision factor of A (resident
 // factor re-use); only the solve and refinement run.
+// tri: A (FP64, column-major view of tri->dA) is still arriving from the host;
+// its tiles are cast inside the factorization launch (MODE_CAST).
 int mixed_posv_ws(cham_uplo_t uplo, int precision, CHAM_desc_t *A, CHAM_desc_t *B, CHAM_desc_t *X, int *iter_out,
-                  CHAM_b200_refine_info_t *info, cudaStream_t s, MixedWs &m, ExecWs *ews, int grid, bool factored);
+                  CHAM_b200_refine_info_t *info, cudaStream_t s, MixedWs &m, ExecWs *ews, int grid, bool factored,
+                  const TriStream *tri = nullptr);
 
 }  // namespace chb

@@ -397,6 +397,13 @@ static SymTiles symtiles(CHAM_desc_t *A, cham_uplo_t uplo, double *diag = nullpt
                     diag};
 }
 
+// Symmetric copies of the diagonal tiles of A for the residuals of this solve.
+static void sym_diag(CHAM_desc_t *A, cham_uplo_t uplo, cudaStream_t s, MixedWs &m) {
+    sym_diag_kernel<<<dim3(std::max(1, std::min(64, (A->nb * A->nb + 255) / 256)), A->nt), 256, 0, s>>>(
+        symtiles(A, uplo, m.diag));
+    CHB_LAUNCHED(1);
+}
+
 // ||A||_inf of the symmetric A (its `uplo` triangle); with a32 (same tiling as
 // A) the referenced tiles are cast into it in the same pass, overflow flagged
 // in *ovf.  Also makes the symmetric diagonal-tile copies for the residuals.
@@ -408,10 +415,8 @@ double sym_norm_inf(CHAM_desc_t *A, cham_uplo_t uplo, cudaStream_t s, MixedWs &m
     const TileMapD t32 = a32 ? tmap(a32) : TileMapD{nullptr, nullptr, nullptr, 0, 0, 0};
     sym_cast_norm_kernel<<<NT * (NT + 1) / 2, 256, A->nb * sizeof(double), s>>>(symtiles(A, uplo), t32, m.colsum,
                                                                               ovf);
-    // symmetric copies of the diagonal tiles for the residuals of this solve
-    sym_diag_kernel<<<dim3(std::max(1, std::min(64, (A->nb * A->nb + 255) / 256)), NT), 256, 0, s>>>(
-        symtiles(A, uplo, m.diag));
-    CHB_LAUNCHED(2);
+    sym_diag(A, uplo, s, m);
+    CHB_LAUNCHED(1);
     std::vector<double> h(A->n);
     cudaMemcpyAsync(h.data(), m.colsum, A->n * sizeof(double), cudaMemcpyDeviceToHost, s);
     cudaStreamSynchronize(s);
@@ -560,7 +565,8 @@ void free_mixed_ws(MixedWs &m) {
 }
 
 int mixed_posv_ws(cham_uplo_t uplo, int precision, CHAM_desc_t *A, CHAM_desc_t *B, CHAM_desc_t *X, int *iter_out,
-                  CHAM_b200_refine_info_t *info, cudaStream_t s, MixedWs &m, ExecWs *ews, int grid, bool factored) {
+                  CHAM_b200_refine_info_t *info, cudaStream_t s, MixedWs &m, ExecWs *ews, int grid, bool factored,
+                  const TriStream *tri) {
     Context &c = ctx();
     const int N = A->n, nrhs = B->n, NB = A->nb;
     int iter = 0;
@@ -580,30 +586,59 @@ int mixed_posv_ws(cham_uplo_t uplo, int precision, CHAM_desc_t *A, CHAM_desc_t *
         clk.tic();
         CHB_CUDA(cudaMemsetAsync(m.flag, 0, sizeof(int), s));
         if ((rc = cast_desc(B, m.B32, s, m.flag))) return rc;
-        // the norm pass also casts A's referenced tiles to FP32 (unless the
-        // FP32 factor is kept from an earlier call)
-        const double anrm = sym_norm_inf(A, uplo, s, m, factored ? nullptr : m.A32, m.flag);
-        if (anrm < 0) return CHAMELEON_ERR_UNEXPECTED;
-        const double cte = anrm * 1.1102230246251565e-16 * sqrt((double)N);
         const int split = (precision == CHAM_B200_PREC_FP32) ? SPLIT_TF32X3 : SPLIT_BF16X3;
+        double anrm = 0;
         int ovf = 0;
-        CHB_CUDA(cudaMemcpyAsync(&ovf, m.flag, sizeof(int), cudaMemcpyDeviceToHost, s));
+        if (!tri) {
+            // the norm pass also casts A's referenced tiles to FP32 (unless the
+            // FP32 factor is kept from an earlier call)
+            anrm = sym_norm_inf(A, uplo, s, m, factored ? nullptr : m.A32, m.flag);
+            if (anrm < 0) return CHAMELEON_ERR_UNEXPECTED;
+            CHB_CUDA(cudaMemcpyAsync(&ovf, m.flag, sizeof(int), cudaMemcpyDeviceToHost, s));
+        } else {
+            // A is still arriving: the factorization launch casts its tiles as
+            // their columns land and accumulates the norm
+            CHB_CUDA(cudaMemsetAsync(m.colsum, 0, (size_t)N * sizeof(double), s));
+        }
         clk.toc(st.cast_ms);
         if (ovf) {
             iter = -2;
             fallback = true;
         }
         if (!fallback) {
-            if ((rc = run_cholesky_dag(factored ? MODE_SOLVE : (MODE_FACT | MODE_SOLVE), uplo, m.A32, m.B32, s, &res,
-                                       split, ews, grid, EXEC_REUSE_INV)))
-                return rc;
+            CastIn cin{};
+            if (tri) {
+                if (desc_upload(m.A32)) return CHAMELEON_ERR_UNEXPECTED;
+                cin = CastIn{tri->dA, tri->ld, tri->arrive, tri->epoch, m.colsum, m.flag, tri->h2d_gbs};
+            }
+            rc = run_cholesky_dag(factored ? MODE_SOLVE : (MODE_FACT | MODE_SOLVE), uplo, m.A32, m.B32, s, &res, split,
+                                  ews, grid, EXEC_REUSE_INV, tri ? &cin : nullptr);
+            if (tri) {
+                // every column has landed (each cast waited for its column); order
+                // the FP64 readers of A after the copies all the same
+                if (cudaStreamWaitEvent(s, tri->done, 0) != cudaSuccess) rc = rc ? rc : CHAMELEON_ERR_UNEXPECTED;
+            }
+            if (rc) return rc;
             st.factor_ms += res.ms;
             if (res.error) return res.error;
-            if (res.info) {
+            if (tri) {
+                sym_diag(A, uplo, s, m);
+                std::vector<double> h(N);
+                CHB_CUDA(cudaMemcpyAsync(h.data(), m.colsum, (size_t)N * sizeof(double), cudaMemcpyDeviceToHost, s));
+                CHB_CUDA(cudaMemcpyAsync(&ovf, m.flag, sizeof(int), cudaMemcpyDeviceToHost, s));
+                CHB_CUDA(cudaStreamSynchronize(s));
+                for (double v : h) anrm = std::max(anrm, v);
+                if (ovf) {
+                    iter = -2;
+                    fallback = true;
+                }
+            }
+            if (!fallback && res.info) {
                 iter = -3;
                 fallback = true;
             }
         }
+        const double cte = anrm * 1.1102230246251565e-16 * sqrt((double)N);
         if (!fallback) {
             if ((rc = cast_desc(m.B32, X, s, nullptr))) return rc;
             std::vector<double> rn, xn;
@@ -667,9 +702,56 @@ int mixed_posv_ws(cham_uplo_t uplo, int precision, CHAM_desc_t *A, CHAM_desc_t *
 }
 
 int mixed_posv(cham_uplo_t uplo, int precision, CHAM_desc_t *A, CHAM_desc_t *B, CHAM_desc_t *X, int *iter_out,
-               CHAM_b200_refine_info_t *info) {
-    return mixed_posv_ws(uplo, precision, A, B, X, iter_out, info, ctx().stream, g_mws, nullptr, 0, false);
+               CHAM_b200_refine_info_t *info, const TriStream *tri = nullptr) {
+    return mixed_posv_ws(uplo, precision, A, B, X, iter_out, info, ctx().stream, g_mws, nullptr, 0, false, tri);
 }
+
+// The referenced triangle of a host matrix is copied to the device one tile
+// column (of the FP32 factor's tiling) at a time on a copy stream, each
+// column followed by a 4-byte arrival flag from pinned host memory (the copy
+// engine executes the two in order), so that the factorization can start on
+// the first columns while the others are still on the way.  Column q of the
+// lower triangle is rows [q nb, N) of columns [q nb, q nb + w); for the upper
+// triangle, rows [q nb, q nb + w) of columns [q nb, N) (the same tiles of the
+// symmetric matrix).  Only the triangle moves: half the bytes of the matrix.
+int tri_stream_start(TriStreamState &ts, cham_uplo_t uplo, const double *hA, int lda, double *dA, int N, int nb,
+                     TriStream *out) {
+    const int NT = (N + nb - 1) / nb;
+    if (!ts.cs) {
+        CHB_CUDA(cudaStreamCreateWithFlags(&ts.cs, cudaStreamNonBlocking));
+        CHB_CUDA(cudaEventCreateWithFlags(&ts.done, cudaEventDisableTiming));
+        CHB_CUDA(cudaHostAlloc((void **)&ts.h_epoch, sizeof(int), cudaHostAllocDefault));
+    }
+    if (NT > ts.cap) {
+        // the flags keep counting up across calls (epochs), so a fresh array
+        // starts from zero once and is never reset
+        if (ts.d_arrive) cudaFree(ts.d_arrive);
+        ts.d_arrive = nullptr;
+        ts.cap = 0;
+        CHB_CUDA(cudaMalloc(&ts.d_arrive, (size_t)NT * sizeof(int)));
+        CHB_CUDA(cudaMemset(ts.d_arrive, 0, (size_t)NT * sizeof(int)));
+        ts.cap = NT;
+        ts.epoch = 0;
+    }
+    // the previous call's copies read *h_epoch; they are done (synchronous API)
+    CHB_CUDA(cudaStreamSynchronize(ts.cs));
+    *ts.h_epoch = ++ts.epoch;
+    for (int q = 0; q < NT; ++q) {
+        const int c0 = q * nb, w = std::min(nb, N - c0);
+        const size_t off_d = (size_t)c0 + (size_t)c0 * N, off_h = (size_t)c0 + (size_t)c0 * lda;
+        if (uplo == ChamLower)
+            CHB_CUDA(cudaMemcpy2DAsync(dA + off_d, (size_t)N * 8, hA + off_h, (size_t)lda * 8, (size_t)(N - c0) * 8, w,
+                                       cudaMemcpyHostToDevice, ts.cs));
+        else
+            CHB_CUDA(cudaMemcpy2DAsync(dA + off_d, (size_t)N * 8, hA + off_h, (size_t)lda * 8, (size_t)w * 8, N - c0,
+                                       cudaMemcpyHostToDevice, ts.cs));
+        CHB_CUDA(cudaMemcpyAsync(ts.d_arrive + q, ts.h_epoch, sizeof(int), cudaMemcpyHostToDevice, ts.cs));
+    }
+    CHB_CUDA(cudaEventRecord(ts.done, ts.cs));
+    *out = TriStream{dA, (int64_t)N, ts.d_arrive, ts.epoch, ts.done, ctx().h2d_gbs};
+    return 0;
+}
+TriStreamState g_tri;
 
 }  // namespace chb
 
@@ -737,11 +819,23 @@ int CHAMELEON_dsposv(cham_uplo_t uplo, int N, int NRHS, double *A, int LDA, doub
         return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
     };
     const bool ad = on_dev(A), bd = on_dev(B), xd = on_dev(X);
-    // host arrays are staged densely (ld = N): only the N x cols block moves
+    // host arrays are staged densely (ld = N): only the N x cols block moves;
+    // a host A streams its referenced triangle in while the factorization
+    // runs (tri_stream_start)
     double *dA = A, *dB = B, *dX = X;
     int lda = LDA, ldb = LDB, ldx = LDX;
+    TriStream tri{};
+    const int prec0 = c.precision == CHAM_B200_PREC_FP64 ? CHAM_B200_PREC_BF16X3 : c.precision;
+    const int nbf = factor_tile(c.tile_size);
+    const bool stream_a = !ad && prec0 == CHAM_B200_PREC_BF16X3 && c.use_tcgen05 && nbf % 64 == 0 && N > nbf;
     if (!ad) {
-        if (!(dA = stage_in(0, A, LDA, N, N, s))) return CHAMELEON_ERR_OUT_OF_RESOURCES;
+        if (stream_a) {
+            if (!(dA = staging(0, std::max<size_t>((size_t)N * N * sizeof(double), 16))))
+                return CHAMELEON_ERR_OUT_OF_RESOURCES;
+            if ((rc = tri_stream_start(g_tri, uplo, A, LDA, dA, N, nbf, &tri))) return rc;
+        } else if (!(dA = stage_in(0, A, LDA, N, N, s))) {
+            return CHAMELEON_ERR_OUT_OF_RESOURCES;
+        }
         lda = N;
     }
     if (!bd) {
@@ -756,9 +850,9 @@ int CHAMELEON_dsposv(cham_uplo_t uplo, int N, int NRHS, double *A, int LDA, doub
     desc_create_cm(&Ad, dA, lda, N, N, c.tile_size);
     desc_create_cm(&Bd, dB, ldb, N, NRHS, c.tile_size);
     desc_create_cm(&Xd, dX, ldx, N, NRHS, c.tile_size);
-    const int prec = c.precision == CHAM_B200_PREC_FP64 ? CHAM_B200_PREC_BF16X3 : c.precision;
     int iter = 0;
-    rc = mixed_posv(uplo, prec, Ad, Bd, Xd, &iter, nullptr);
+    rc = mixed_posv(uplo, prec0, Ad, Bd, Xd, &iter, nullptr, stream_a ? &tri : nullptr);
+    if (stream_a) cudaStreamSynchronize(g_tri.cs);   // the staging buffer is free again
     if (ITER) *ITER = iter;
     if (!xd) stage_out(X, LDX, dX, N, NRHS, s);
     if (!ad && iter < 0) stage_out(A, LDA, dA, N, N, s);

@@ -12,9 +12,9 @@ import numpy as np
 import pytest
 import scipy.linalg as sla
 
-TK_POTRF, TK_TRSM, TK_UPD, TK_FWD_TRSM, TK_FWD_UPD, TK_BWD_TRSM, TK_BWD_UPD, TK_INV, TK_XINV = range(1, 10)
+TK_POTRF, TK_TRSM, TK_UPD, TK_FWD_TRSM, TK_FWD_UPD, TK_BWD_TRSM, TK_BWD_UPD, TK_INV, TK_XINV, TK_CAST = range(1, 11)
 SUBB = 128
-FACT, SOLVE, XINV, NOINV = 1, 2, 4, 8
+FACT, SOLVE, XINV, NOINV, CAST = 1, 2, 4, 8, 16
 
 
 def ngroups(n, G, tail=2):
@@ -45,18 +45,24 @@ def check_waits(tasks, mode, N, NB, nrhs, NBB, G=1):
     # with full tile inverses (XINV) each substitution is split into row blocks
     ns = (lambda k: nbi(k)) if mode & XINV else (lambda k: 1)
     applied = {}   # (m, n, bi, bj) -> panels applied so far, in order
+    cast = np.zeros((NT, NT), int)
+    ccast = bool(mode & CAST)   # the host's arrival flags are external: assumed set
     for kind, sub, m, n, k, bn, grp in tasks:
-        if kind == TK_POTRF:
-            ok = upd[k, k] >= ngroups(k, G) * S(k, k); pan[k, k] += 1
+        if kind == TK_CAST:
+            ok = m >= n and cast[m, n] == 0; cast[m, n] += 1
+        elif kind == TK_POTRF:
+            ok = upd[k, k] >= ngroups(k, G) * S(k, k) and (not ccast or k > 0 or cast[0, 0] == 1); pan[k, k] += 1
         elif kind == TK_INV:
             ok = True; pan[k, k] += 1
         elif kind == TK_XINV:
             ok = (not fact) or pan[k, k] >= 1; xinv[k] += 1
         elif kind == TK_TRSM:
-            ok = pan[k, k] >= 1 and upd[m, k] >= ngroups(k, G) * S(m, k); pan[m, k] += 1
+            ok = pan[k, k] >= 1 and upd[m, k] >= ngroups(k, G) * S(m, k) and (not ccast or k > 0 or cast[m, 0] == 1)
+            pan[m, k] += 1
         elif kind == TK_UPD:
             kl = k + bn - 1
             ok = pan[m, kl] >= nbi(m) and pan[n, kl] >= nbi(n) and upd[m, n] >= grp * S(m, n)
+            ok = ok and (not ccast or grp > 0 or cast[m, n] == 1)
             upd[m, n] += 1
             # every sub-block sees each panel k < n exactly once, in order
             key = (m, n, sub)
@@ -84,6 +90,8 @@ def check_waits(tasks, mode, N, NB, nrhs, NBB, G=1):
             for n in range(m + 1):
                 assert upd[m, n] == ngroups(n, G) * S(m, n)
         assert all(v == key[1] for key, v in applied.items())
+        if ccast:
+            assert (cast[np.tril_indices(NT)] == 1).all() and not np.triu(cast, 1).any()
     if mode & SOLVE:
         want = np.array([ns(k) for k in range(NT)])[:, None]
         assert (fwdD[:, :NTB] == want).all() and (bwdD[:, :NTB] == want).all()
@@ -104,6 +112,8 @@ def emulate(tasks, A, B, uplo, N, NB, NBB, xinv=False):
     Y = np.full_like(B, np.nan) if B is not None else None
     Yt = lambda m, bn: Y[m * NB:m * NB + tm(m), bn * NBB:min((bn + 1) * NBB, B.shape[1])]
     for kind, sub, m, n, k, bn, grp in tasks:
+        if kind == TK_CAST:
+            continue
         if kind == TK_POTRF:
             T = L(k, k)
             T[np.tril_indices(T.shape[0])] = np.linalg.cholesky(np.tril(T) + np.tril(T, -1).T)[
@@ -151,6 +161,18 @@ def test_schedule_is_deadlock_free(cb_host, N, NB, nrhs, NBB, workers, prof, G):
     for mode in (FACT, SOLVE, FACT | SOLVE):
         t = cb_host.schedule(mode, N, NB, nrhs if mode & SOLVE else 0, NBB, workers, prof, G)
         check_waits(t, mode, N, NB, nrhs if mode & SOLVE else 0, NBB, G)
+
+
+@pytest.mark.parametrize("N,NB,nrhs,NBB", SHAPES)
+@pytest.mark.parametrize("workers", [1, 7, 148])
+def test_schedule_casting_arriving_tiles_is_deadlock_free(cb_host, N, NB, nrhs, NBB, workers):
+    """MODE_CAST: the FP32 tiles are cast inside the launch as their columns
+    arrive; every tile is cast once, before its first reader (the panel solve
+    of column 0 or the first update group), whatever the list order."""
+    for mode in (FACT | SOLVE | XINV | CAST, FACT | CAST):
+        t = cb_host.schedule(mode, N, NB, nrhs if mode & SOLVE else 0, NBB, workers, 2, 8)
+        check_waits(t, mode, N, NB, nrhs if mode & SOLVE else 0, NBB, 8)
+        assert (t[:, 0] == TK_CAST).sum() == (-(-N // NB)) * (-(-N // NB) + 1) // 2
 
 
 @pytest.mark.parametrize("N,NB,nrhs,NBB", SHAPES)
@@ -242,6 +264,8 @@ def check_waits_prefix(prefix, mode, N, NB, nrhs, NBB, G=1):
     fact = bool(mode & FACT)
     ns = (lambda k: nbi(k)) if mode & XINV else (lambda k: 1)
     for kind, sub, m, n, k, bn, grp in prefix:
+        if kind == TK_CAST:
+            continue
         if kind == TK_POTRF:
             ok = upd[k, k] >= ngroups(k, G) * S(k, k); pan[k, k] += 1
         elif kind == TK_INV:

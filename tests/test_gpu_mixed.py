@@ -219,3 +219,37 @@ def test_recursive_tile_not_spd_reports_info(cb):
         ms = ctypes.c_float()
         assert cb.lib().CHAM_B200_Mixed_Factor_Only(122, 2, dA.ptr, dB.ptr, ctypes.byref(ms)) == 301
     cb.lib().CHAMELEON_Set(cb.CHAMELEON_B200_REC_TILE, old)
+
+
+@pytest.mark.parametrize("uplo", [121, 122])
+@pytest.mark.parametrize("N,NB,nrhs", [(3000, 512, 7), (2100, 256, 3), (1025, 512, 64)])
+def test_dsposv_host_matrix_streams_while_factoring(cb, orc, uplo, N, NB, nrhs):
+    """A host matrix is copied to the device one tile column at a time while
+    the factorization casts the columns that have landed (only the referenced
+    triangle moves).  The result equals the one from the same matrix already
+    on the device (same FP32 factor; the norm is summed in another order, so
+    agreement to the refinement's stopping accuracy), and NaN in the other
+    triangle of the host matrix is never read."""
+    import torch
+    A0 = orc.dplgsy(float(N), N, 91)
+    B0 = orc.dplrnt(N, nrhs, 92)
+    cb.set_param(cb.CHAMELEON_TILE_SIZE, NB)
+    try:
+        A = poison_other_triangle(A0, uplo)
+        Ah = torch.from_numpy(A.T.copy()).pin_memory()          # column-major N x N in pinned memory
+        Bh = torch.from_numpy(np.asfortranarray(B0).T.copy()).pin_memory()
+        Xh = torch.zeros_like(Bh).pin_memory()
+        rc, it = cb.dsposv(uplo, N, nrhs, Ah, N, Bh, N, Xh, N)
+        assert rc == 0 and it >= 0
+        X = Xh.numpy().T
+        assert np_check_solve(A0, X, B0) < 60
+        Ad = torch.from_numpy(np.asfortranarray(A0).T.copy()).cuda()
+        Bd = torch.from_numpy(np.asfortranarray(B0).T.copy()).cuda()
+        Xd = torch.zeros_like(Bd)
+        rc2, it2 = cb.dsposv(uplo, N, nrhs, Ad, N, Bd, N, Xd, N)
+        assert rc2 == 0 and it2 >= 0
+        Xdev = Xd.cpu().numpy().T
+        assert np.abs(X - Xdev).max() / np.abs(Xdev).max() < 2 * np.sqrt(N) * EPS
+        assert np.array_equal(Ah.numpy(), A.T, equal_nan=True)   # the host matrix is not written
+    finally:
+        cb.set_param(cb.CHAMELEON_TILE_SIZE, 384)
