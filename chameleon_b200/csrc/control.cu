@@ -129,7 +129,8 @@ cudaStream_t meta_stream() {
 // Stream-ordered workspace memory: allocation and release go through the
 // meta stream, so neither waits for kernels running on other streams (a plain
 // cudaFree synchronizes the whole device).  dev_alloc returns memory usable on
-// any stream; dev_free requires that no queued work still uses the memory.
+// any stream (contents undefined); dev_free requires that no queued work still
+// uses the memory.
 // The library's own memory pool: freed blocks stay mapped for reuse (release
 // threshold = max), so workspace churn never returns memory to the driver and
 // re-maps it -- which can stall every stream of the device.  The pool is an
@@ -163,8 +164,10 @@ void *dev_alloc(size_t bytes) {
         cudaGetLastError();
         return nullptr;
     }
-    if (cudaMemsetAsync(p, 0, std::max<size_t>(bytes, 16), ms) != cudaSuccess ||
-        cudaStreamSynchronize(ms) != cudaSuccess) {
+    // no fill: a memset is a kernel, and on a device whose SMs are all held by
+    // other streams' persistent launches it would wait for them (callers
+    // write or clear their buffers on their own streams before reading them)
+    if (cudaStreamSynchronize(ms) != cudaSuccess) {
         cudaGetLastError();
         cudaFreeAsync(p, ms);
         return nullptr;
@@ -174,6 +177,27 @@ void *dev_alloc(size_t bytes) {
 
 void dev_free(void *p) {
     if (p) cudaFreeAsync(p, meta_stream());
+}
+
+// Maps `bytes` of device memory into the library pool ahead of use (one
+// allocation, freed at once: the pool keeps the memory), so that later
+// workspace growth is served from mapped memory.  Growing the pool maps new
+// physical memory, which took hundreds of milliseconds while persistent
+// launches occupied the device.
+int pool_reserve(size_t bytes) {
+    cudaMemPool_t pool = lib_pool();
+    if (!pool || bytes == 0) return 0;
+    size_t have = 0;
+    cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &have);
+    if (have >= bytes) return 0;
+    void *p = nullptr;
+    cudaStream_t ms = meta_stream();
+    if (cudaMallocFromPoolAsync(&p, bytes - have, pool, ms) != cudaSuccess) {
+        cudaGetLastError();
+        return CHAMELEON_ERR_OUT_OF_RESOURCES;
+    }
+    cudaFreeAsync(p, ms);
+    return cudaStreamSynchronize(ms) == cudaSuccess ? 0 : CHAMELEON_ERR_UNEXPECTED;
 }
 
 int desc_create_tiled_on(CHAM_desc_t **desc, cham_flttype_t dtyp, void *storage, int nb, int m, int n) {
@@ -846,13 +870,13 @@ static double *g_stage[3] = {nullptr, nullptr, nullptr};
 static size_t g_stage_bytes[3] = {0, 0, 0};
 double *staging(int slot, size_t bytes) {
     if (bytes > g_stage_bytes[slot]) {
-        if (g_stage[slot]) cudaFree(g_stage[slot]);
+        // the previous call that used the buffer is done (synchronous API);
+        // pool memory: no device-wide synchronization
+        cudaStreamSynchronize(ctx().stream);
+        dev_free(g_stage[slot]);
         g_stage[slot] = nullptr;
         g_stage_bytes[slot] = 0;
-        if (cudaMalloc(&g_stage[slot], bytes) != cudaSuccess) {
-            cudaGetLastError();
-            return nullptr;
-        }
+        if (!(g_stage[slot] = (double *)dev_alloc(bytes))) return nullptr;
         g_stage_bytes[slot] = bytes;
     }
     return g_stage[slot];

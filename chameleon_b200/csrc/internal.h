@@ -93,9 +93,11 @@ int desc_tile_ld(const CHAM_desc_t *d, int m);
 int desc_upload(CHAM_desc_t *d);
 cudaStream_t meta_stream();   // private stream of descriptor metadata uploads
 // Workspace memory allocated / released in stream order on the meta stream
-// (no device-wide synchronization); zero-filled.
+// (no device-wide synchronization, no kernel); contents undefined.
 void *dev_alloc(size_t bytes);
 void dev_free(void *p);
+// Map `bytes` of device memory into the library pool ahead of use.
+int pool_reserve(size_t bytes);
 // Tile-layout (CCRB) m x n descriptor on caller-owned device storage of at
 // least m * n elements (not freed by Desc_Destroy); uploaded.
 int desc_create_tiled_on(CHAM_desc_t **desc, cham_flttype_t dtyp, void *storage, int nb, int m, int n);
@@ -233,6 +235,7 @@ struct TriStreamState {
 };
 int tri_stream_start(TriStreamState &ts, cham_uplo_t uplo, const double *hA, int lda, double *dA, int N, int nb,
                      TriStream *out);
+void free_tri_stream(TriStreamState &ts);
 
 // Mixed-precision solve on an explicit stream and workspaces (mixed.cu).
 // factored = true: m.A32 already holds the low-precision factor of A (resident

@@ -728,9 +728,13 @@ int tri_stream_start(TriStreamState &ts, cham_uplo_t uplo, const double *hA, int
         if (ts.d_arrive) cudaFree(ts.d_arrive);
         ts.d_arrive = nullptr;
         ts.cap = 0;
-        CHB_CUDA(cudaMalloc(&ts.d_arrive, (size_t)NT * sizeof(int)));
-        CHB_CUDA(cudaMemset(ts.d_arrive, 0, (size_t)NT * sizeof(int)));
-        ts.cap = NT;
+        const int cap = std::max(NT, 256);
+        CHB_CUDA(cudaMalloc(&ts.d_arrive, (size_t)cap * sizeof(int)));
+        // zeros from host memory: a copy, not a memset kernel (which could wait
+        // for SMs that other streams' persistent launches hold)
+        std::vector<int> zeros(cap, 0);
+        CHB_CUDA(cudaMemcpy(ts.d_arrive, zeros.data(), (size_t)cap * sizeof(int), cudaMemcpyHostToDevice));
+        ts.cap = cap;
         ts.epoch = 0;
     }
     // the previous call's copies read *h_epoch; they are done (synchronous API)
@@ -752,6 +756,17 @@ int tri_stream_start(TriStreamState &ts, cham_uplo_t uplo, const double *hA, int
     return 0;
 }
 TriStreamState g_tri;
+
+void free_tri_stream(TriStreamState &ts) {
+    if (ts.cs) {
+        cudaStreamSynchronize(ts.cs);
+        cudaStreamDestroy(ts.cs);
+    }
+    if (ts.done) cudaEventDestroy(ts.done);
+    if (ts.d_arrive) cudaFree(ts.d_arrive);
+    if (ts.h_epoch) cudaFreeHost(ts.h_epoch);
+    ts = TriStreamState();
+}
 
 }  // namespace chb
 

@@ -18,11 +18,14 @@
 //
 // Admission: a request starts only when its device memory fits in the HBM
 // budget next to the running requests and the kept factors (unused kept
-// factors are released least recently used first); otherwise it waits, in
-// arrival order.  A request larger than the whole budget starts when nothing
-// else runs.  Times are CHAM_B200_Serve_Now() (CLOCK_MONOTONIC seconds).
+// factors are released least recently used first); among the queued large
+// requests the shortest goes first unless the oldest has waited 50 ms.  A
+// request larger than the whole budget starts when nothing else runs.  Each
+// slot's factorization launch holds at most its share of the SMs, and a new
+// matrix streams in (its referenced triangle) while it is being factored.  Times are CHAM_B200_Serve_Now() (CLOCK_MONOTONIC seconds).
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <stdlib.h>
 #include <string.h>
 #include <time.h>
 
@@ -87,6 +90,7 @@ struct Slot {
     ExecWs ews;
     MixedWs mws;
     DevBuf A, B, X;
+    TriStreamState tri;   // copy stream of the request matrices (streamed triangle)
 };
 
 struct Server {
@@ -112,6 +116,9 @@ struct Server {
 };
 
 int choose_nb(int N) { return N >= 4096 ? 512 : 256; }
+
+constexpr int kReserveSMs = 16;        // SMs left to short kernels next to the slots' launches
+constexpr double kAgeSeconds = 0.05;   // a queued request older than this is served next
 
 size_t kept_bytes(int N) {
     const size_t n = N, nb = choose_nb(N), nt = (n + nb - 1) / nb;
@@ -174,17 +181,56 @@ struct Descs {
     }
 };
 
+// Diagnostics (CHAMELEON_B200_SERVE_TRACE=1): the host-side phases of every
+// request whose service takes longer than 100 ms go to stderr.
+bool serve_trace() {
+    static const bool on = [] {
+        const char *e = getenv("CHAMELEON_B200_SERVE_TRACE");
+        return e && *e && *e != '0';
+    }();
+    return on;
+}
+struct PhaseLog {
+    double t[8] = {0};
+    const char *name[8] = {nullptr};
+    int n = 0;
+    void mark(const char *what) {
+        if (n < 8) {
+            t[n] = now_s();
+            name[n++] = what;
+        }
+    }
+    void report(const CHAM_b200_request_t *r, double t_start) const {
+        if (!serve_trace() || n == 0 || t[n - 1] - t_start < 0.1) return;
+        fprintf(stderr, "serve: N=%d nrhs=%d reuse=%d service %.1f ms:", r->N, r->nrhs, r->A ? 0 : 1,
+                (t[n - 1] - t_start) * 1e3);
+        double prev = t_start;
+        for (int i = 0; i < n; ++i) {
+            fprintf(stderr, " %s %.1f", name[i], (t[i] - prev) * 1e3);
+            prev = t[i];
+        }
+        fprintf(stderr, "\n");
+    }
+};
+
 // Mixed-precision solve of one request on slot `sl` (or on its kept factor).
 int solve_large(Server *sv, Slot &sl, CHAM_b200_request_t *r, int *iters) {
+    PhaseLog pl;
+    const double t_in = now_s();
     const int N = r->N, nrhs = r->nrhs, NB = choose_nb(N);
     const int NT = (N + NB - 1) / NB;
     const cham_uplo_t uplo = (r->uplo == ChamUpper) ? ChamUpper : ChamLower;
-    const int grid = std::min(ctx().num_sms, std::max(8, NT * (NT + 1) * 4));
+    // Each slot's persistent launch holds at most its share of the SMs minus a
+    // reserve: a CTA of it fills an SM's register file, so kernels of other
+    // slots and of the batch stream could otherwise start only when it ends
+    const int share = std::max(8, (ctx().num_sms - kReserveSMs) / (int)sv->slots.size());
+    const int grid = std::min(share, std::max(8, NT * (NT + 1) * 4));
     cudaStream_t s = sl.s;
     const size_t bb = (size_t)N * nrhs * 8;
     if (int rc = sl.B.reserve(bb)) return rc;
     if (int rc = sl.X.reserve(bb)) return rc;
     if (int rc = upload(sl.B.p, r->B, r->ldb, N, nrhs, s)) return rc;
+    pl.mark("B");
 
     std::shared_ptr<Kept> kp;
     if (!r->A) {   // solve with a kept factor
@@ -216,7 +262,17 @@ int solve_large(Server *sv, Slot &sl, CHAM_b200_request_t *r, int *iters) {
             rc = sl.A.reserve((size_t)N * N * 8);
             dA = (double *)sl.A.p;
         }
-        if (!rc && r->A) rc = upload(dA, r->A, r->lda, N, N, s);
+        // the referenced triangle of a new matrix streams in while the
+        // factorization casts the columns that have landed
+        const int nbf = factor_tile(NB);
+        const bool stream_a = r->A && nbf % 64 == 0 && N > nbf && ctx().use_tcgen05;
+        TriStream tri{};
+        pl.mark("lock+alloc");
+        if (!rc && r->A) {
+            if (stream_a) rc = tri_stream_start(sl.tri, uplo, r->A, r->lda, dA, N, nbf, &tri);
+            else rc = upload(dA, r->A, r->lda, N, N, s);
+        }
+        pl.mark("A");
         Descs d;
         if (!rc) rc = desc_create_cm(&d.A, dA, N, N, N, NB);
         if (!rc) rc = desc_create_cm(&d.B, (double *)sl.B.p, N, N, nrhs, NB);
@@ -231,12 +287,18 @@ int solve_large(Server *sv, Slot &sl, CHAM_b200_request_t *r, int *iters) {
         } else if (!rc) {
             MixedWs &m = kp ? kp->mws : sl.mws;
             ExecWs &e = kp ? kp->ews : sl.ews;
-            rc = mixed_posv_ws(uplo, CHAM_B200_PREC_BF16X3, d.A, d.B, d.X, &iter, nullptr, s, m, &e, grid, reuse);
+            rc = mixed_posv_ws(uplo, CHAM_B200_PREC_BF16X3, d.A, d.B, d.X, &iter, nullptr, s, m, &e, grid, reuse,
+                               stream_a ? &tri : nullptr);
             if (kp && iter < 0) kp->fp64 = true;   // the FP64 fallback factored the kept matrix in place
         }
+        pl.mark("solve");
         if (!rc) rc = download(r->X, r->ldx, sl.X.p, N, nrhs, s);
         if (cudaStreamSynchronize(s) != cudaSuccess && !rc) rc = CHAMELEON_ERR_UNEXPECTED;
+        // the request's host matrix is not read after it completes
+        if (stream_a && cudaStreamSynchronize(sl.tri.cs) != cudaSuccess && !rc) rc = CHAMELEON_ERR_UNEXPECTED;
+        pl.mark("X");
     }
+    pl.report(r, t_in);
     *iters = iter;
     std::shared_ptr<Kept> replaced;   // released after the lock
     std::lock_guard<std::mutex> lk(sv->mu);
@@ -264,14 +326,27 @@ void slot_worker(Server *sv, int idx) {
         size_t need = 0;
         {
             std::unique_lock<std::mutex> lk(sv->mu);
+            // Shortest first (a solve with a kept factor counts as a quarter of
+            // its order), so that small requests do not wait behind large
+            // ones; a request that has waited kAgeSeconds goes next whatever
+            // its size, so that large ones are not starved.
+            size_t pick = 0;
+            auto choose = [&]() {
+                pick = 0;
+                if (now_s() - sv->large_q.front()->t_submit > kAgeSeconds) return;
+                auto cost = [](const CHAM_b200_request_t *q) { return q->A ? (double)q->N : 0.25 * q->N; };
+                for (size_t i = 1; i < sv->large_q.size(); ++i)
+                    if (cost(sv->large_q[i]) < cost(sv->large_q[pick])) pick = i;
+            };
             sv->cv.wait(lk, [&] {
                 if (sv->large_q.empty()) return sv->stop;
-                const size_t nb = need_bytes(sv->large_q.front(), sv->small_n);
+                choose();
+                const size_t nb = need_bytes(sv->large_q[pick], sv->small_n);
                 return make_room(sv, nb) || sv->used == 0 || sv->stop;
             });
             if (sv->large_q.empty()) return;   // stop requested and nothing queued
-            r = sv->large_q.front();
-            sv->large_q.pop_front();
+            r = sv->large_q[pick];
+            sv->large_q.erase(sv->large_q.begin() + (std::ptrdiff_t)pick);
             need = need_bytes(r, sv->small_n);
             sv->used += need;
         }
@@ -377,6 +452,9 @@ int CHAM_B200_Serve_Create(CHAM_b200_server_t *out, int slots, double hbm_budget
     size_t fr = 0, tot = 0;
     cudaMemGetInfo(&fr, &tot);
     sv->budget = hbm_budget_bytes > 0 ? (size_t)hbm_budget_bytes : (size_t)(0.8 * (double)fr);
+    // the requests' buffers and workspaces come from memory mapped now, not
+    // on the request path (half the budget, at most 48 GB)
+    pool_reserve(std::min(sv->budget / 2, (size_t)48 << 30));
     if (cudaStreamCreateWithFlags(&sv->bs, cudaStreamNonBlocking) != cudaSuccess) {
         delete sv;
         return CHAMELEON_ERR_UNEXPECTED;
@@ -458,6 +536,7 @@ int CHAM_B200_Serve_Destroy(CHAM_b200_server_t srv) {
         free_mixed_ws(sl->mws);
         free_exec_ws(sl->ews);
         cudaStreamDestroy(sl->s);
+        free_tri_stream(sl->tri);
     }
     sv->slots.clear();
     cudaStreamSynchronize(sv->bs);
