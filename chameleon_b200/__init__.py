@@ -175,6 +175,15 @@ EXTRAS = {
     "CHAM_B200_Handle_Overflow": (_i, [_vp]),
     "CHAM_B200_Trace_Enable": (_i, [_i]),
     "CHAM_B200_Trace_Read": (_i, [_vp, _i]),
+    "CHAM_B200_Dag_Create": (_i, [ctypes.POINTER(_vp)]),
+    "CHAM_B200_Dag_Destroy": (_i, [_vp]),
+    "CHAM_B200_Dag_Clear": (_i, [_vp]),
+    "CHAM_B200_Dag_Record": (_i, [_vp, _i, _i, _i, _i, _i]),
+    "CHAM_B200_Dag_Size": (_i, [_vp]),
+    "CHAM_B200_Dag_Get": (_i, [_vp, _vp, _i]),
+    "CHAM_B200_Dag_Schedule": (_i, [_vp, _i, _i, _i, _i, _i, _vp, _i]),
+    "CHAM_B200_Dag_Run": (_i, [_vp, _i, _i, _i, _vp, _vp, _vp, _i, _i, _vp, _vp, _vp, _vp]),
+    "CHAM_B200_Init": (_i, []),
     "CHAM_B200_Schedule_Size": (_i, [_i, _i, _i, _i, _i, _i, _i, _i]),
     "CHAM_B200_Schedule_Build": (_i, [_i, _i, _i, _i, _i, _i, _i, _i, ctypes.POINTER(Task), _i]),
     "CHAM_B200_dposv_timed": (_i, [_i, _i, _i, _vp, _i, _vp, _i, ctypes.POINTER(ctypes.c_float)]),

@@ -212,6 +212,25 @@ int desc_create_tiled_on(CHAM_desc_t **desc, cham_flttype_t dtyp, void *storage,
     return desc_upload(d);
 }
 
+static int desc_upload_tables(CHAM_desc_t *d, const int64_t *off, const int *ld);
+
+// A descriptor over tiles addressed by caller tables: tile (m, n) at
+// base + off[m + mt n], leading dimension ld[m] (a runtime plugin's view of
+// another library's descriptor); uploaded, storage not owned.
+int desc_create_from_tables(CHAM_desc_t **desc, double *base, int mb, int m, int n, const int64_t *off,
+                            const int *ld, int nb) {
+    if (nb <= 0) nb = mb;
+    CHAM_desc_t *d = (CHAM_desc_t *)calloc(1, sizeof(CHAM_desc_t));
+    layout_init(d, ChamRealDouble, mb, nb, mb * nb, m, n, m, n);
+    d->mat = base;
+    d->alloc_mat = 0;
+    d->schedopt = new DescPriv();
+    d->id = ctx().desc_ids++;
+    fill_tiles(d);
+    *desc = d;
+    return desc_upload_tables(d, off, ld);
+}
+
 int desc_upload(CHAM_desc_t *d) {
     DescPriv *pv = priv(d);
     if (pv->dev.off) return 0;
@@ -221,6 +240,12 @@ int desc_upload(CHAM_desc_t *d) {
     for (int n = 0; n < d->nt; ++n)
         for (int m = 0; m < d->mt; ++m) off[m + (size_t)d->mt * n] = desc_tile_off(d, m, n);
     for (int m = 0; m < d->mt; ++m) ld[m] = desc_tile_ld(d, m);
+    return desc_upload_tables(d, off.data(), ld.data());
+}
+
+static int desc_upload_tables(CHAM_desc_t *d, const int64_t *off_h, const int *ld_h) {
+    DescPriv *pv = priv(d);
+    const size_t nt = (size_t)d->mt * d->nt;
     // Stream-ordered allocation on a private stream: creating and destroying
     // descriptors does not synchronize the device (cudaFree would), so
     // concurrent solvers on other streams keep running.
@@ -233,8 +258,8 @@ int desc_upload(CHAM_desc_t *d) {
         CHB_CUDA(cudaMallocAsync(&pv->dev.off, nt * sizeof(int64_t), ms));
         CHB_CUDA(cudaMallocAsync(&pv->dev.ld, d->mt * sizeof(int), ms));
     }
-    CHB_CUDA(cudaMemcpyAsync(pv->dev.off, off.data(), nt * sizeof(int64_t), cudaMemcpyHostToDevice, ms));
-    CHB_CUDA(cudaMemcpyAsync(pv->dev.ld, ld.data(), d->mt * sizeof(int), cudaMemcpyHostToDevice, ms));
+    CHB_CUDA(cudaMemcpyAsync(pv->dev.off, off_h, nt * sizeof(int64_t), cudaMemcpyHostToDevice, ms));
+    CHB_CUDA(cudaMemcpyAsync(pv->dev.ld, ld_h, d->mt * sizeof(int), cudaMemcpyHostToDevice, ms));
     CHB_CUDA(cudaStreamSynchronize(ms));
     return 0;
 }
@@ -420,6 +445,11 @@ int __chameleon_finalize(void) {
 }
 
 int CHAMELEON_Initialized(void) { return ctx().initialized ? 1 : 0; }
+
+int CHAM_B200_Init(void) {
+    if (ctx().initialized) return 0;
+    return __chameleon_init(0, 1);
+}
 
 int CHAMELEON_Set(int param, int value) {
     Context &c = ctx();

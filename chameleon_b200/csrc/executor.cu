@@ -9,6 +9,7 @@
 // Device side: dispatch by atomic cursor, bounded waits on per-tile counters,
 // tile operations from core.cuh, release by red.release.
 #include <algorithm>
+#include <array>
 #include <climits>
 #include <cmath>
 #include <memory>
@@ -82,6 +83,9 @@ struct Schedule {
     int npotrf = 0;              // POTRF tasks (for the dedicated CTA), their indices after the tasks
     const int *d_potrf = nullptr;
 };
+
+template <class NBI>
+std::vector<Task> list_schedule(std::vector<Coarse> &ct, int P, NBI nbi);
 
 std::vector<Task> build_order(const Shape &s) {
     const int NT = (s.N + s.NB - 1) / s.NB;
@@ -226,6 +230,13 @@ std::vector<Task> build_order(const Shape &s) {
             }
         }
     }
+    return list_schedule(ct, s.P, nbi);
+}
+
+// List scheduling of a coarse DAG (generation order topological) on P
+// workers with critical-path priorities; emits the sub-tasks in start order.
+template <class NBI>
+std::vector<Task> list_schedule(std::vector<Coarse> &ct, int P, NBI nbi) {
     // bottom levels (generation order is topological)
     for (int i = (int)ct.size() - 1; i >= 0; --i) {
         double b = 0;
@@ -257,7 +268,7 @@ std::vector<Task> build_order(const Shape &s) {
     for (auto &c : ct)
         if (!c.virt) total += c.nsub;
     out.reserve(total);
-    int free_w = s.P;
+    int free_w = P;
     auto emit = [&](const Coarse &c, int j) {
         Task t{};
         t.kind = c.kind; t.m = c.m; t.n = c.n; t.k = c.k; t.bn = c.bn; t.sub = 0; t.grp = c.grp;
@@ -307,19 +318,15 @@ std::vector<Task> build_order(const Shape &s) {
 std::mutex g_sched_mu;
 std::unordered_map<Shape, std::unique_ptr<Schedule>, ShapeHash> g_sched;
 
-Schedule *get_schedule(const Shape &s) {
-    std::lock_guard<std::mutex> lk(g_sched_mu);
-    auto it = g_sched.find(s);
-    if (it != g_sched.end()) return it->second.get();
-    auto sch = std::make_unique<Schedule>();
-    sch->tasks = build_order(s);
+// Device copy of a task list (and of its POTRF indices).
+int upload_schedule(Schedule *sch) {
     if (!sch->tasks.empty()) {
         std::vector<int> pidx;
         for (size_t i = 0; i < sch->tasks.size(); ++i)
             if (sch->tasks[i].kind == TK_POTRF) pidx.push_back((int)i);
         const size_t tbytes = sch->tasks.size() * sizeof(Task);
         const size_t bytes = tbytes + pidx.size() * sizeof(int);
-        if (!(sch->d_tasks = (Task *)dev_alloc(bytes))) return nullptr;
+        if (!(sch->d_tasks = (Task *)dev_alloc(bytes))) return CHAMELEON_ERR_OUT_OF_RESOURCES;
         sch->npotrf = (int)pidx.size();
         sch->d_potrf = reinterpret_cast<const int *>(reinterpret_cast<const uint8_t *>(sch->d_tasks) + tbytes);
         cudaStream_t ms = meta_stream();
@@ -327,8 +334,18 @@ Schedule *get_schedule(const Shape &s) {
             (!pidx.empty() && cudaMemcpyAsync((void *)sch->d_potrf, pidx.data(), pidx.size() * sizeof(int),
                                               cudaMemcpyHostToDevice, ms) != cudaSuccess) ||
             cudaStreamSynchronize(ms) != cudaSuccess)
-            return nullptr;
+            return CHAMELEON_ERR_UNEXPECTED;
     }
+    return 0;
+}
+
+Schedule *get_schedule(const Shape &s) {
+    std::lock_guard<std::mutex> lk(g_sched_mu);
+    auto it = g_sched.find(s);
+    if (it != g_sched.end()) return it->second.get();
+    auto sch = std::make_unique<Schedule>();
+    sch->tasks = build_order(s);
+    if (upload_schedule(sch.get())) return nullptr;
     Schedule *raw = sch.get();
     g_sched[s] = std::move(sch);
     return raw;
@@ -381,6 +398,10 @@ void free_exec_ws(ExecWs &w) {
     w = ExecWs();
 }
 
+// A task list recorded by a caller (CHAM_B200_Dag_*), already checked and on
+// the device; its update groups are single panels.
+static thread_local const Schedule *t_given = nullptr;
+
 int run_cholesky_dag(int mode, cham_uplo_t uplo, CHAM_desc_t *A, CHAM_desc_t *B, cudaStream_t s,
                      ExecResult *res, int split, ExecWs *wsp, int grid_req, int flags, const CastIn *cin) {
     Context &c = ctx();
@@ -430,9 +451,9 @@ int run_cholesky_dag(int mode, cham_uplo_t uplo, CHAM_desc_t *A, CHAM_desc_t *B,
     const int canonR = nrhs ? (NTB - 1) * NBB + std::min(NBB, ((nrhs - (NTB - 1) * NBB + 15) / 16) * 16) : 0;
     // update group size: fused k steps amortize the C round trip and the
     // dispatch of an update over G panels (CHAMELEON_B200_UPD_GROUP per path)
-    const int G = std::max(1, prof == PROF_FP64 ? c.kgroup_f64 : (tc ? c.kgroup_tc : c.kgroup_f32));
+    const int G = t_given ? 1 : std::max(1, prof == PROF_FP64 ? c.kgroup_f64 : (tc ? c.kgroup_tc : c.kgroup_f32));
     Shape sh{mode, canonN, NB, canonR, NBB, grid, prof, G, cin ? std::max(1, cin->h2d_gbs) : 0};
-    Schedule *sch = get_schedule(sh);
+    const Schedule *sch = t_given ? t_given : get_schedule(sh);
     if (!sch) return CHAMELEON_ERR_OUT_OF_RESOURCES;
     const int NIB = (NB + IB - 1) / IB;
     const size_t nctr = (size_t)(cin ? 3 : 2) * NT * NT + (size_t)4 * NT * std::max(NTB, 1) + NT;
@@ -600,3 +621,249 @@ extern "C" int CHAM_B200_Schedule_Size(int mode, int N, int NB, int nrhs, int NB
     return (int)build_order(Shape{mode, N, NB, nrhs, NBB, workers, prof, std::max(1, kgroup), (mode & MODE_CAST) ? 50 : 0})
         .size();
 }
+
+// ---------------------------------------------------------------------------
+// Recorded DAGs: tile tasks submitted by a caller (a Chameleon runtime plugin
+// whose INSERT_TASK_* calls append here; chameleon_pzpotrf / chameleon_pztrsm
+// run unchanged above it) and run by the persistent executor.
+// ---------------------------------------------------------------------------
+struct cham_b200_dag_s {
+    std::vector<std::array<int, 5>> rec;   // kind, m, n, k, bn in submission order
+};
+
+namespace chb {
+namespace {
+
+// The executor's counter predicates (executor_kernel.cuh task_deps, update
+// groups of one panel), replayed on a task list: true when every task's
+// inputs are complete once every task before it has run, i.e. the list is
+// deadlock-free for any number of CTAs.
+bool replay_ok(const std::vector<Task> &tl, int mode, int N, int NB, int NTB) {
+    const int NT = (N + NB - 1) / NB;
+    auto tm = [&](int m) { return (m == NT - 1) ? N - m * NB : NB; };
+    auto nbi = [&](int m) { return (tm(m) + SUBB - 1) / SUBB; };
+    auto S = [&](int m, int n) { return m == n ? nbi(m) * (nbi(m) + 1) / 2 : nbi(m) * nbi(n); };
+    const bool fact = mode & MODE_FACT;
+    const size_t nb4 = (size_t)NT * std::max(NTB, 1);
+    std::vector<int> upd((size_t)NT * NT, 0), pan((size_t)NT * NT, 0), fB(nb4, 0), fD(nb4, 0), bB(nb4, 0), bD(nb4, 0);
+    for (const Task &t : tl) {
+        bool ok = true;
+        const size_t kb = t.k + (size_t)NT * t.bn, mb = t.m + (size_t)NT * t.bn;
+        switch (t.kind) {
+        case TK_POTRF: ok = upd[t.k + (size_t)NT * t.k] >= t.k * S(t.k, t.k); pan[t.k + (size_t)NT * t.k]++; break;
+        case TK_INV: pan[t.k + (size_t)NT * t.k]++; break;
+        case TK_TRSM:
+            ok = pan[t.k + (size_t)NT * t.k] >= 1 && upd[t.m + (size_t)NT * t.k] >= t.k * S(t.m, t.k);
+            pan[t.m + (size_t)NT * t.k]++;
+            break;
+        case TK_UPD:
+            ok = t.bn == 1 && pan[t.m + (size_t)NT * t.k] >= nbi(t.m) && pan[t.n + (size_t)NT * t.k] >= nbi(t.n) &&
+                 upd[t.m + (size_t)NT * t.n] >= t.k * S(t.m, t.n);
+            upd[t.m + (size_t)NT * t.n]++;
+            break;
+        case TK_FWD_TRSM: ok = pan[t.k + (size_t)NT * t.k] >= 1 && fB[kb] >= t.k; fD[kb]++; break;
+        case TK_FWD_UPD: ok = fD[kb] >= 1 && (!fact || pan[t.m + (size_t)NT * t.k] >= nbi(t.m)) && fB[mb] >= t.k; fB[mb]++; break;
+        case TK_BWD_TRSM: ok = fD[kb] >= 1 && bB[kb] >= NT - 1 - t.k; bD[kb]++; break;
+        case TK_BWD_UPD: ok = bD[kb] >= 1 && bB[mb] >= NT - 1 - t.k; bB[mb]++; break;
+        default: ok = false;
+        }
+        if (!ok) return false;
+    }
+    return true;
+}
+
+}  // namespace
+}  // namespace chb
+
+extern "C" {
+
+int CHAM_B200_Dag_Create(CHAM_b200_dag_t *dag) {
+    if (!dag) return CHAMELEON_ERR_ILLEGAL_VALUE;
+    *dag = new cham_b200_dag_s();
+    return 0;
+}
+int CHAM_B200_Dag_Destroy(CHAM_b200_dag_t dag) {
+    delete dag;
+    return 0;
+}
+int CHAM_B200_Dag_Clear(CHAM_b200_dag_t dag) {
+    if (!dag) return CHAMELEON_ERR_ILLEGAL_VALUE;
+    dag->rec.clear();
+    return 0;
+}
+int CHAM_B200_Dag_Record(CHAM_b200_dag_t dag, int kind, int m, int n, int k, int bn) {
+    using namespace chb;
+    if (!dag || kind < CHAM_B200_DAG_POTRF || kind > CHAM_B200_DAG_BWD_UPDATE || m < 0 || n < 0 || k < 0 || bn < 0)
+        return CHAMELEON_ERR_ILLEGAL_VALUE;
+    dag->rec.push_back({kind, m, n, k, bn});
+    return 0;
+}
+int CHAM_B200_Dag_Size(CHAM_b200_dag_t dag) { return dag ? (int)dag->rec.size() : CHAMELEON_ERR_ILLEGAL_VALUE; }
+int CHAM_B200_Dag_Get(CHAM_b200_dag_t dag, int *out, int cap) {
+    if (!dag || !out) return CHAMELEON_ERR_ILLEGAL_VALUE;
+    const int n = std::min<int>(cap, (int)dag->rec.size());
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j < 5; ++j) out[5 * i + j] = dag->rec[i][j];
+    return n;
+}
+
+// The recorded tasks as the executor's coarse DAG: every record's tiles (A's
+// lower triangle, B's tile column bn) with read-after-write, write-after-read
+// and write-after-write edges in submission order, then the same list
+// scheduling as the built-in DAGs, and a replay of the device's wait
+// predicates on the result.  Returns the sub-task list (empty + error code on
+// a record the executor cannot run in that order).
+static int dag_to_tasks(const cham_b200_dag_s &dag, int N, int NB, int nrhs, int NBB, int workers,
+                        std::vector<chb::Task> *out, int *mode_out) {
+    using namespace chb;
+    const int NT = (N + NB - 1) / NB;
+    const int NTB = nrhs > 0 ? (nrhs + NBB - 1) / NBB : 0;
+    auto tm = [&](int m) { return (m == NT - 1) ? N - m * NB : NB; };
+    auto nbi = [&](int m) { return (tm(m) + SUBB - 1) / SUBB; };
+    int mode = 0;
+    for (auto &r : dag.rec) mode |= (r[0] <= TK_UPD) ? MODE_FACT : MODE_SOLVE;
+    std::vector<Coarse> ct;
+    // tile ids: A (m, n) -> m + NT n; B (m, bn) -> NT NT + m + NT bn
+    const size_t ntile = (size_t)NT * NT + (size_t)NT * std::max(NTB, 1);
+    std::vector<int> last_w(ntile, -1);
+    std::vector<std::vector<int>> readers(ntile);
+    auto add = [&](int kind, int m, int n, int k, int bn, int nsub, double dur) {
+        Coarse c;
+        c.kind = kind; c.m = m; c.n = n; c.k = k; c.bn = bn; c.grp = 0; c.nsub = nsub; c.dur = dur;
+        ct.push_back(c);
+        return (int)ct.size() - 1;
+    };
+    auto edge = [&](int a, int b) {
+        if (a < 0 || b < 0 || a == b) return;
+        ct[a].succ.push_back(b);
+        ct[b].npred++;
+    };
+    auto rd = [&](size_t tile, int id) {
+        edge(last_w[tile], id);
+        readers[tile].push_back(id);
+    };
+    auto wr = [&](size_t tile, int id) {
+        edge(last_w[tile], id);
+        for (int r : readers[tile]) edge(r, id);
+        readers[tile].clear();
+        last_w[tile] = id;
+    };
+    auto At = [&](int m, int n) { return (size_t)m + (size_t)NT * n; };
+    auto Bt = [&](int m, int bn) { return (size_t)NT * NT + m + (size_t)NT * bn; };
+    const double nb = NB;
+    // FP64 path costs (flop model), as in build_order
+    const Calib &cal = kCalib[PROF_FP64];
+    std::vector<int> inv_id(NT, -1);
+    if (!(mode & MODE_FACT)) {   // solve only: the executor inverts the diagonal blocks first
+        for (int k = 0; k < NT; ++k) {
+            inv_id[k] = add(TK_INV, k, k, k, 0, 1, 1.0 * tm(k) * IB * IB);
+            rd(At(k, k), inv_id[k]);
+        }
+    }
+    for (auto &r : dag.rec) {
+        const int kind = r[0], m = r[1], n = r[2], k = r[3], bn = r[4];
+        const bool inA = m < NT && n < NT && k < NT;
+        const bool inB = bn < std::max(NTB, 1);
+        if (!inA || !inB) return CHAMELEON_ERR_ILLEGAL_VALUE;
+        int id = -1;
+        const double w = NTB ? ((bn == NTB - 1) ? nrhs - bn * NBB : NBB) : 0;
+        switch (kind) {
+        case TK_POTRF:
+            if (m != k || n != k) return CHAMELEON_ERR_ILLEGAL_VALUE;
+            id = add(TK_POTRF, k, k, k, 0, 1, cal.potrf * 2.0 * tm(k) * tm(k) * tm(k));
+            wr(At(k, k), id);
+            break;
+        case TK_TRSM:
+            if (n != k || m <= k) return CHAMELEON_ERR_ILLEGAL_VALUE;
+            id = add(TK_TRSM, m, k, k, 0, nbi(m), cal.trsm * 2.0 * SUBB * nb * nb);
+            rd(At(k, k), id);
+            wr(At(m, k), id);
+            break;
+        case TK_UPD:
+            if (m < n || n <= k) return CHAMELEON_ERR_ILLEGAL_VALUE;
+            id = add(TK_UPD, m, n, k, 1, m == n ? nbi(m) * (nbi(m) + 1) / 2 : nbi(m) * nbi(n),
+                     cal.upd * SUBB * SUBB * nb * 2.0);
+            ct[id].grp = k;
+            rd(At(m, k), id);
+            if (m != n) rd(At(n, k), id);
+            wr(At(m, n), id);
+            break;
+        case TK_FWD_TRSM:
+        case TK_BWD_TRSM:
+            if (m != k || n != k || !NTB) return CHAMELEON_ERR_ILLEGAL_VALUE;
+            id = add(kind, k, k, k, bn, 1, cal.strsm * 3.0 * tm(k) * tm(k) * w);
+            rd(At(k, k), id);
+            if (inv_id[k] >= 0) edge(inv_id[k], id);
+            wr(Bt(k, bn), id);
+            break;
+        case TK_FWD_UPD:
+        case TK_BWD_UPD:
+            // forward: B(m) -= L(m,k) B(k), m > k; backward: B(m) -= L(k,m)^T B(k), m < k
+            if (!NTB || (kind == TK_FWD_UPD ? m <= k : m >= k)) return CHAMELEON_ERR_ILLEGAL_VALUE;
+            id = add(kind, m, k, k, bn, nbi(m), cal.supd * 2.0 * SUBB * tm(k) * w);
+            rd(kind == TK_FWD_UPD ? At(m, k) : At(k, m), id);
+            rd(Bt(k, bn), id);
+            wr(Bt(m, bn), id);
+            break;
+        default:
+            return CHAMELEON_ERR_ILLEGAL_VALUE;
+        }
+    }
+    *out = list_schedule(ct, workers, nbi);
+    *mode_out = mode;
+    if (!replay_ok(*out, mode, N, NB, NTB)) {
+        out->clear();
+        return CHAMELEON_ERR_NOT_SUPPORTED;
+    }
+    return 0;
+}
+
+int CHAM_B200_Dag_Schedule(CHAM_b200_dag_t dag, int N, int NB, int nrhs, int NBB, int workers, void *out, int cap) {
+    using namespace chb;
+    if (!dag || N <= 0 || NB <= 0 || nrhs < 0 || (nrhs > 0 && NBB <= 0) || workers <= 0)
+        return CHAMELEON_ERR_ILLEGAL_VALUE;
+    std::vector<Task> tl;
+    int mode = 0;
+    if (int rc = dag_to_tasks(*dag, N, NB, nrhs, NBB, workers, &tl, &mode)) return rc;
+    const int n = std::min<int>((int)tl.size(), cap);
+    if (out) memcpy(out, tl.data(), sizeof(Task) * (size_t)std::max(0, n));
+    return (int)tl.size();
+}
+
+int CHAM_B200_Dag_Run(CHAM_b200_dag_t dag, cham_uplo_t uplo, int N, int NB, double *A, const int64_t *a_off,
+                      const int *a_ld, int nrhs, int NBB, double *B, const int64_t *b_off, const int *b_ld,
+                      int *info) {
+    using namespace chb;
+    int rc = ensure_init();
+    if (rc) return rc;
+    if (!dag || !A || !a_off || !a_ld || N <= 0 || NB <= 0 || (uplo != ChamUpper && uplo != ChamLower) ||
+        (nrhs > 0 && (!B || !b_off || !b_ld || NBB <= 0)))
+        return CHAMELEON_ERR_ILLEGAL_VALUE;
+    if (info) *info = 0;
+    if (dag->rec.empty()) return 0;
+    Context &c = ctx();
+    const int NT = (N + NB - 1) / NB, NTB = nrhs > 0 ? (nrhs + NBB - 1) / NBB : 0;
+    auto sch = std::make_unique<Schedule>();
+    int mode = 0;
+    if ((rc = dag_to_tasks(*dag, N, NB, nrhs, NBB, c.num_sms, &sch->tasks, &mode))) return rc;
+    if ((rc = upload_schedule(sch.get()))) return rc;
+    CHAM_desc_t *dA = nullptr, *dB = nullptr;
+    rc = desc_create_from_tables(&dA, A, NB, N, N, a_off, a_ld);
+    if (!rc && NTB) rc = desc_create_from_tables(&dB, B, NB, N, nrhs, b_off, b_ld, NBB);
+    ExecResult res;
+    if (!rc) {
+        t_given = sch.get();
+        rc = run_cholesky_dag(mode, uplo, dA, dB, c.stream, &res, 0, nullptr, 0, 0, nullptr);
+        t_given = nullptr;
+    }
+    if (dA) CHAMELEON_Desc_Destroy(&dA);
+    if (dB) CHAMELEON_Desc_Destroy(&dB);
+    dev_free(sch->d_tasks);
+    if (rc) return rc;
+    if (res.error) return res.error;
+    if (info) *info = res.info;
+    (void)NT;
+    return 0;
+}
+
+}  // extern "C"

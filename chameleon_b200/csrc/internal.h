@@ -91,6 +91,10 @@ int desc_tile_cols(const CHAM_desc_t *d, int n);
 int64_t desc_tile_off(const CHAM_desc_t *d, int m, int n);
 int desc_tile_ld(const CHAM_desc_t *d, int m);
 int desc_upload(CHAM_desc_t *d);
+// Descriptor over tiles addressed by caller tables (host arrays): tile (m, n)
+// at base + off[m + mt n], leading dimension ld[m]; mb x nb tiles (nb <= 0: mb).
+int desc_create_from_tables(CHAM_desc_t **desc, double *base, int mb, int m, int n, const int64_t *off,
+                            const int *ld, int nb = 0);
 cudaStream_t meta_stream();   // private stream of descriptor metadata uploads
 // Workspace memory allocated / released in stream order on the meta stream
 // (no device-wide synchronization, no kernel); contents undefined.

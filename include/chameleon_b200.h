@@ -283,6 +283,53 @@ int CUDA_slag2d(int m, int n, const float *SA, int ldsa, double *A, int lda,
                 cublasHandle_t handle);
 
 /* ------------------------------------------------------------------------- */
+/* Recorded tile DAGs: the runtime-plugin boundary of the reference           */
+/* (include/chameleon/tasks_z.h:64-380 INSERT_TASK_*, include/chameleon/      */
+/* runtime.h:51-714 RUNTIME_*).  A Chameleon runtime plugin (runtime/b200,    */
+/* chameleon_b200/runtime/runtime_b200.c) appends one record per INSERT_TASK  */
+/* call of chameleon_pdpotrf / chameleon_pdtrsm (compute/pzpotrf.c:84-194,    */
+/* compute/pztrsm.c:58-200, unchanged) and runs the DAG at                    */
+/* RUNTIME_sequence_wait.  Records (kind, m, n, k, bn):                       */
+/*   POTRF (k, k, k, 0): factor diagonal tile k of A                          */
+/*   PANEL (m, k, k, 0): A(m,k) <- A(m,k) L(k,k)^-T                            */
+/*   UPDATE (m, n, k, 0): A(m,n) -= A(m,k) A(n,k)^T, m >= n > k (SYRK if m == n)*/
+/*   FWD_SOLVE (k, k, k, bn) / BWD_SOLVE: B(k,bn) <- L(k,k)^-1 / ^-T B(k,bn)    */
+/*   FWD_UPDATE (m, k, k, bn): B(m,bn) -= L(m,k) B(k,bn), m > k                 */
+/*   BWD_UPDATE (m, k, k, bn): B(m,bn) -= L(k,m)^T B(k,bn), m < k               */
+/* with tiles of the logical lower triangle (Upper storage: transposed views).*/
+/* ------------------------------------------------------------------------- */
+#define CHAM_B200_DAG_POTRF      1
+#define CHAM_B200_DAG_PANEL      2
+#define CHAM_B200_DAG_UPDATE     3
+#define CHAM_B200_DAG_FWD_SOLVE  4
+#define CHAM_B200_DAG_FWD_UPDATE 5
+#define CHAM_B200_DAG_BWD_SOLVE  6
+#define CHAM_B200_DAG_BWD_UPDATE 7
+typedef struct cham_b200_dag_s *CHAM_b200_dag_t;
+int CHAM_B200_Dag_Create(CHAM_b200_dag_t *dag);
+int CHAM_B200_Dag_Destroy(CHAM_b200_dag_t dag);
+int CHAM_B200_Dag_Clear(CHAM_b200_dag_t dag);
+int CHAM_B200_Dag_Record(CHAM_b200_dag_t dag, int kind, int m, int n, int k, int bn);
+int CHAM_B200_Dag_Size(CHAM_b200_dag_t dag);
+/* the records, 5 ints each, in submission order; returns the count written */
+int CHAM_B200_Dag_Get(CHAM_b200_dag_t dag, int *out, int cap);
+/* The executor's task list for the recorded DAG (16-byte tasks, as
+ * CHAM_B200_Schedule_Build); returns its length, or CHAMELEON_ERR_NOT_SUPPORTED
+ * when the executor cannot run the records in their submission order. */
+int CHAM_B200_Dag_Schedule(CHAM_b200_dag_t dag, int N, int NB, int nrhs, int NBB, int workers, void *out,
+                           int cap);
+/* Run the recorded DAG (FP64) on A (order N, NB x NB tiles at A + a_off[m +
+ * NT n], leading dimension a_ld[m]; device memory) and B (N x nrhs, NB x NBB
+ * tiles likewise; may be NULL with nrhs == 0).  Synchronous; *info receives
+ * LAPACK's info of the factorization. */
+int CHAM_B200_Dag_Run(CHAM_b200_dag_t dag, cham_uplo_t uplo, int N, int NB, double *A, const int64_t *a_off,
+                      const int *a_ld, int nrhs, int NBB, double *B, const int64_t *b_off, const int *b_ld,
+                      int *info);
+/* CHAMELEON_Init of this library under a name of its own (for runtime plugins
+ * linked into a Chameleon build, whose own CHAMELEON_Init is the reference's) */
+int CHAM_B200_Init(void);
+
+/* ------------------------------------------------------------------------- */
 /* Uneven batch (new; the reference batch API is uniform-size,                */
 /* compute/zpotrf_batch.c:66-118).  Matrix i is n[i] x n[i] column-major at   */
 /* A + a_off[i] (ld = n[i]); its right-hand sides are n[i] x nrhs[i] at        */

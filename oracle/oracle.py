@@ -51,6 +51,19 @@ def build_ref(force=False):
     return REF_SO
 
 
+def build_plugin(force=False):
+    """The reference's dposv drivers linked with the B200 runtime plugin
+    (oracle/build_plugin.sh; needs the reference sources and libchameleon_b200.so)."""
+    out = os.path.join(HERE, "_ref", "libchamb200rt.so")
+    src = [os.path.join(HERE, "plugin_harness.c"), os.path.join(HERE, "build_plugin.sh"),
+           os.path.join(os.path.dirname(HERE), "chameleon_b200", "runtime", "runtime_b200.c"),
+           os.path.join(os.path.dirname(HERE), "chameleon_b200", "libchameleon_b200.so")]
+    if not force and os.path.exists(out) and all(os.path.getmtime(out) >= os.path.getmtime(f) for f in src):
+        return out
+    subprocess.check_call(["bash", os.path.join(HERE, "build_plugin.sh")])
+    return out
+
+
 _port = None
 _ref = None
 
