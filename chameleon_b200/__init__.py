@@ -73,6 +73,15 @@ class CHAM_desc_t(ctypes.Structure):
     ]
 
 
+class CHAM_tile_t(ctypes.Structure):
+    """include/chameleon/struct.h:53-61 (without the trace name)."""
+    _fields_ = [("mat", ctypes.c_void_p), ("rank", ctypes.c_int), ("m", ctypes.c_int), ("n", ctypes.c_int),
+                ("ld", ctypes.c_int), ("format", ctypes.c_int8), ("flttype", ctypes.c_int)]
+
+
+CHAMELEON_TILE_FULLRANK, CHAMELEON_TILE_DESC, CHAMELEON_TILE_HMAT = 1, 2, 4
+
+
 class RefineInfo(ctypes.Structure):
     _fields_ = [("iterations", ctypes.c_int), ("fallback", ctypes.c_int), ("precision", ctypes.c_int),
                 ("backward_error", ctypes.c_double), ("seconds", ctypes.c_double)]
@@ -140,6 +149,24 @@ PROTOS = {
     "CHAMELEON_dpotrs_Tile_Async": (_i, [_i, _D, _D, _vp, _vp]),
     "CHAMELEON_dpotrf_batch_Tile": (_i, [_i, _D]),
     "CHAMELEON_dtrsm_batch_Tile": (_i, [_i, _i, _i, _i, ctypes.c_double, _D, _D]),
+    "CHAMELEON_dtrtri": (_i, [_i, _i, _i, _vp, _i]),
+    "CHAMELEON_dlauum": (_i, [_i, _i, _vp, _i]),
+    "CHAMELEON_dpotri": (_i, [_i, _i, _vp, _i]),
+    "CHAMELEON_dtrtri_Tile": (_i, [_i, _i, _D]),
+    "CHAMELEON_dlauum_Tile": (_i, [_i, _D]),
+    "CHAMELEON_dpotri_Tile": (_i, [_i, _D]),
+    "CHAMELEON_lapacke_dposv": (_i, [_i, ctypes.c_char, _i, _i, _vp, _i, _vp, _i]),
+    "CHAMELEON_lapacke_dpotrf": (_i, [_i, ctypes.c_char, _i, _vp, _i]),
+    "CHAMELEON_lapacke_dpotrs": (_i, [_i, ctypes.c_char, _i, _i, _vp, _i, _vp, _i]),
+    "CHAMELEON_lapacke_dpotri": (_i, [_i, ctypes.c_char, _i, _vp, _i]),
+    "CHAMELEON_lapacke_dlauum": (_i, [_i, ctypes.c_char, _i, _vp, _i]),
+    "CHAMELEON_lapacke_dtrtri": (_i, [_i, ctypes.c_char, ctypes.c_char, _i, _vp, _i]),
+    "chameleon_lapack_dposv_": (None, [_vp] * 8),
+    "chameleon_lapack_dpotrf_": (None, [_vp] * 5),
+    "chameleon_lapack_dpotrs_": (None, [_vp] * 8),
+    "chameleon_lapack_dpotri_": (None, [_vp] * 5),
+    "chameleon_lapack_dlauum_": (None, [_vp] * 5),
+    "chameleon_lapack_dtrtri_": (None, [_vp] * 6),
     "CHAMELEON_dplgsy": (_i, [ctypes.c_double, _i, _i, _vp, _i, _ull]),
     "CHAMELEON_dplgsy_Tile": (_i, [ctypes.c_double, _i, _D, _ull]),
     "CHAMELEON_dplrnt": (_i, [_i, _i, _vp, _i, _ull]),
@@ -156,6 +183,14 @@ PROTOS = {
     "CUDA_dtrsm": (_i, [_i, _i, _i, _i, _i, _i, _dp, _vp, _i, _vp, _i, _vp]),
     "CUDA_dpotrf": (_i, [_i, _i, _vp, _i, _vp, _i, _vp, _vp]),
     "CUDA_spotrf": (_i, [_i, _i, _vp, _i, _vp, _i, _vp, _vp]),
+    "TCUDA_dgemm": (_i, [_i, _i, _i, _i, _i, _dp, _vp, _vp, _dp, _vp, _vp]),
+    "TCUDA_dsyrk": (_i, [_i, _i, _i, _i, _dp, _vp, _dp, _vp, _vp]),
+    "TCUDA_dtrsm": (_i, [_i, _i, _i, _i, _i, _i, _dp, _vp, _vp, _vp]),
+    "TCUDA_dpotrf": (_i, [_i, _i, _vp, _vp, _i, _vp, _vp]),
+    "TCUDA_dplgsy": (_i, [_dp, _i, _i, _vp, _i, _i, _i, _ull, _vp]),
+    "TCUDA_dplrnt": (_i, [_i, _i, _vp, _i, _i, _i, _ull, _vp]),
+    "TCUDA_dlag2s": (_i, [_i, _i, _vp, _vp, _vp]),
+    "TCUDA_slag2d": (_i, [_i, _i, _vp, _vp, _vp]),
     "CUDA_dpotrf_noalloc": (_i, [_i, _i, _vp, _i, _vp, _vp]),
     "CUDA_dplgsy": (_i, [_dp, _i, _i, _vp, _i, _i, _i, _i, _ull, _vp]),
     "CUDA_dplrnt": (_i, [_i, _i, _vp, _i, _i, _i, _i, _ull, _vp]),
@@ -353,6 +388,39 @@ def dpotrf(uplo, N, A, LDA):
 def dpotrs(uplo, N, NRHS, A, LDA, B, LDB):
     init()
     return lib().CHAMELEON_dpotrs(uplo, N, NRHS, _addr(A), LDA, _addr(B), LDB)
+
+
+def dtrtri(uplo, diag, N, A, LDA):
+    """CHAMELEON_dtrtri (compute/ztrtri.c): the uplo triangle of A <- its inverse."""
+    init()
+    return lib().CHAMELEON_dtrtri(uplo, diag, N, _addr(A), LDA)
+
+
+def dlauum(uplo, N, A, LDA):
+    """CHAMELEON_dlauum (compute/zlauum.c): the uplo triangle of L^T L / U U^T."""
+    init()
+    return lib().CHAMELEON_dlauum(uplo, N, _addr(A), LDA)
+
+
+def dpotri(uplo, N, A, LDA):
+    """CHAMELEON_dpotri (compute/zpotri.c): A^-1 from the Cholesky factor in A."""
+    init()
+    return lib().CHAMELEON_dpotri(uplo, N, _addr(A), LDA)
+
+
+def dtrtri_Tile(uplo, diag, A):
+    init()
+    return lib().CHAMELEON_dtrtri_Tile(uplo, diag, A.ptr)
+
+
+def dlauum_Tile(uplo, A):
+    init()
+    return lib().CHAMELEON_dlauum_Tile(uplo, A.ptr)
+
+
+def dpotri_Tile(uplo, A):
+    init()
+    return lib().CHAMELEON_dpotri_Tile(uplo, A.ptr)
 
 
 def dplgsy(bump, uplo, N, A, LDA, seed):

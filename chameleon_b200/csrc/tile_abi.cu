@@ -372,4 +372,50 @@ int CUDA_slag2d(int m, int n, const float *SA, int ldsa, double *A, int lda, cub
     return cudaGetLastError() == cudaSuccess ? CHAMELEON_SUCCESS : CHAMELEON_ERR_UNEXPECTED;
 }
 
+
+// ---- tile forms (gpucublas_ztile.h): tile -> address + leading dimension ----
+static bool full_rank(const CHAM_tile_t *t) { return t && t->mat && (t->format & CHAMELEON_TILE_FULLRANK); }
+
+int TCUDA_dgemm(cham_trans_t transA, cham_trans_t transB, int m, int n, int k, const double *alpha,
+                const CHAM_tile_t *A, const CHAM_tile_t *B, const double *beta, CHAM_tile_t *C,
+                cublasHandle_t handle) {
+    if (!full_rank(A) || !full_rank(B) || !full_rank(C)) return CHAMELEON_ERR_NOT_SUPPORTED;
+    return CUDA_dgemm(transA, transB, m, n, k, alpha, (const double *)A->mat, A->ld, (const double *)B->mat, B->ld,
+                      beta, (double *)C->mat, C->ld, handle);
+}
+int TCUDA_dsyrk(cham_uplo_t uplo, cham_trans_t trans, int n, int k, const double *alpha, const CHAM_tile_t *A,
+                const double *beta, CHAM_tile_t *C, cublasHandle_t handle) {
+    if (!full_rank(A) || !full_rank(C)) return CHAMELEON_ERR_NOT_SUPPORTED;
+    return CUDA_dsyrk(uplo, trans, n, k, alpha, (const double *)A->mat, A->ld, beta, (double *)C->mat, C->ld, handle);
+}
+int TCUDA_dtrsm(cham_side_t side, cham_uplo_t uplo, cham_trans_t transA, cham_diag_t diag, int m, int n,
+                const double *alpha, const CHAM_tile_t *A, CHAM_tile_t *B, cublasHandle_t handle) {
+    if (!full_rank(A) || !full_rank(B)) return CHAMELEON_ERR_NOT_SUPPORTED;
+    return CUDA_dtrsm(side, uplo, transA, diag, m, n, alpha, (const double *)A->mat, A->ld, (double *)B->mat, B->ld,
+                      handle);
+}
+int TCUDA_dpotrf(cham_uplo_t uplo, int n, CHAM_tile_t *A, double *WORK, int lwork, int *d_info,
+                 cusolverDnHandle_t handle) {
+    if (!full_rank(A)) return CHAMELEON_ERR_NOT_SUPPORTED;
+    return CUDA_dpotrf(uplo, n, (double *)A->mat, A->ld, WORK, lwork, d_info, handle);
+}
+int TCUDA_dplgsy(const double *bump, int m, int n, CHAM_tile_t *A, int bigM, int m0, int n0,
+                 unsigned long long int seed, cublasHandle_t handle) {
+    if (!full_rank(A)) return CHAMELEON_ERR_NOT_SUPPORTED;
+    return CUDA_dplgsy(bump, m, n, (double *)A->mat, A->ld, bigM, m0, n0, seed, handle);
+}
+int TCUDA_dplrnt(int m, int n, CHAM_tile_t *A, int bigM, int m0, int n0, unsigned long long int seed,
+                 cublasHandle_t handle) {
+    if (!full_rank(A)) return CHAMELEON_ERR_NOT_SUPPORTED;
+    return CUDA_dplrnt(m, n, (double *)A->mat, A->ld, bigM, m0, n0, seed, handle);
+}
+int TCUDA_dlag2s(int m, int n, const CHAM_tile_t *A, CHAM_tile_t *B, cublasHandle_t handle) {
+    if (!full_rank(A) || !full_rank(B)) return CHAMELEON_ERR_NOT_SUPPORTED;
+    return CUDA_dlag2s(m, n, (const double *)A->mat, A->ld, (float *)B->mat, B->ld, handle);
+}
+int TCUDA_slag2d(int m, int n, const CHAM_tile_t *A, CHAM_tile_t *B, cublasHandle_t handle) {
+    if (!full_rank(A) || !full_rank(B)) return CHAMELEON_ERR_NOT_SUPPORTED;
+    return CUDA_slag2d(m, n, (const float *)A->mat, A->ld, (double *)B->mat, B->ld, handle);
+}
+
 }  // extern "C"

@@ -212,6 +212,41 @@ int CHAMELEON_dplrnt_Tile(CHAM_desc_t *A, unsigned long long int seed);
 double CHAMELEON_dlansy_Tile(cham_normtype_t norm, cham_uplo_t uplo, CHAM_desc_t *A);
 double CHAMELEON_dlange_Tile(cham_normtype_t norm, CHAM_desc_t *A);
 
+/* Inverses from the Cholesky factor (compute/ztrtri.c, zlauum.c, zpotri.c:
+ * zpotri = pztrtri then pzlauum).  LAPACK semantics: only the uplo triangle of
+ * A is read and written; dtrtri returns i > 0 when A(i,i) == 0 (A unchanged);
+ * dpotri takes the factor from dpotrf and returns the uplo triangle of A^-1. */
+int CHAMELEON_dtrtri(cham_uplo_t uplo, cham_diag_t diag, int N, double *A, int LDA);
+int CHAMELEON_dlauum(cham_uplo_t uplo, int N, double *A, int LDA);
+int CHAMELEON_dpotri(cham_uplo_t uplo, int N, double *A, int LDA);
+int CHAMELEON_dtrtri_Tile(cham_uplo_t uplo, cham_diag_t diag, CHAM_desc_t *A);
+int CHAMELEON_dlauum_Tile(cham_uplo_t uplo, CHAM_desc_t *A);
+int CHAMELEON_dpotri_Tile(cham_uplo_t uplo, CHAM_desc_t *A);
+
+/* LAPACKE interface (lapack_api/src/lapack_z{posv,potrf,potrs,potri,lauum,
+ * trtri}.c after z->d; include/chameleon/chameleon_zlapack.h:102-119):
+ * column-major only (matrix_layout CHAMELEON_LAPACK_COL_MAJOR = CblasColMajor),
+ * uplo / diag as LAPACK characters; -1 for another layout. */
+#define CHAMELEON_LAPACK_COL_MAJOR 102
+int CHAMELEON_lapacke_dposv(int matrix_layout, char uplo, int N, int NRHS, double *A, int lda, double *B, int ldb);
+int CHAMELEON_lapacke_dpotrf(int matrix_layout, char uplo, int N, double *A, int lda);
+int CHAMELEON_lapacke_dpotrs(int matrix_layout, char uplo, int N, int NRHS, const double *A, int lda, double *B,
+                             int ldb);
+int CHAMELEON_lapacke_dpotri(int matrix_layout, char uplo, int N, double *A, int lda);
+int CHAMELEON_lapacke_dlauum(int matrix_layout, char uplo, int N, double *A, int lda);
+int CHAMELEON_lapacke_dtrtri(int matrix_layout, char uplo, char diag, int N, double *A, int lda);
+/* Fortran LAPACK interface of the same (lapack_api/src/lapack_zposv.c:25-33
+ * and siblings; the reference names them through CMake's Fortran mangling,
+ * here the gfortran convention: lower case with a trailing underscore). */
+void chameleon_lapack_dposv_(const char *uplo, const int *n, const int *nrhs, double *a, const int *lda, double *b,
+                             const int *ldb, int *info);
+void chameleon_lapack_dpotrf_(const char *uplo, const int *n, double *a, const int *lda, int *info);
+void chameleon_lapack_dpotrs_(const char *uplo, const int *n, const int *nrhs, const double *a, const int *lda,
+                              double *b, const int *ldb, int *info);
+void chameleon_lapack_dpotri_(const char *uplo, const int *n, double *a, const int *lda, int *info);
+void chameleon_lapack_dlauum_(const char *uplo, const int *n, double *a, const int *lda, int *info);
+void chameleon_lapack_dtrtri_(const char *uplo, const char *diag, const int *n, double *a, const int *lda, int *info);
+
 /* ------------------------------------------------------------------------- */
 /* Mixed precision (new; in the spirit of the reference's commented-out      */
 /* zcposv, include/chameleon/chameleon_zc.h:33-42, and LAPACK dsposv)         */
@@ -281,6 +316,31 @@ int CUDA_dlag2s(int m, int n, const double *A, int lda, float *SA, int ldsa,
                 cublasHandle_t handle);
 int CUDA_slag2d(int m, int n, const float *SA, int ldsa, double *A, int lda,
                 cublasHandle_t handle);
+
+/* Tile forms of the kernels above (gpucublas/include/gpucublas/gpucublas_ztile.h
+ * :30,46-48,51,55 and gpucublas_zctile.h:22-23 after z->d / zc->ds
+ * generation): the operands are CHAM_tile_t (device address + leading
+ * dimension), as the runtimes' codelets pass them.  Full-rank tiles only
+ * (format CHAMELEON_TILE_FULLRANK); other formats return
+ * CHAMELEON_ERR_NOT_SUPPORTED.  Formats: include/chameleon/struct.h:37-39. */
+#define CHAMELEON_TILE_FULLRANK (1 << 0)
+#define CHAMELEON_TILE_DESC     (1 << 1)
+#define CHAMELEON_TILE_HMAT     (1 << 2)
+int TCUDA_dgemm(cham_trans_t transA, cham_trans_t transB, int m, int n, int k, const double *alpha,
+                const CHAM_tile_t *A, const CHAM_tile_t *B, const double *beta, CHAM_tile_t *C,
+                cublasHandle_t handle);
+int TCUDA_dsyrk(cham_uplo_t uplo, cham_trans_t trans, int n, int k, const double *alpha, const CHAM_tile_t *A,
+                const double *beta, CHAM_tile_t *C, cublasHandle_t handle);
+int TCUDA_dtrsm(cham_side_t side, cham_uplo_t uplo, cham_trans_t transA, cham_diag_t diag, int m, int n,
+                const double *alpha, const CHAM_tile_t *A, CHAM_tile_t *B, cublasHandle_t handle);
+int TCUDA_dpotrf(cham_uplo_t uplo, int n, CHAM_tile_t *A, double *WORK, int lwork, int *d_info,
+                 cusolverDnHandle_t handle);
+int TCUDA_dplgsy(const double *bump, int m, int n, CHAM_tile_t *A, int bigM, int m0, int n0,
+                 unsigned long long int seed, cublasHandle_t handle);
+int TCUDA_dplrnt(int m, int n, CHAM_tile_t *A, int bigM, int m0, int n0, unsigned long long int seed,
+                 cublasHandle_t handle);
+int TCUDA_dlag2s(int m, int n, const CHAM_tile_t *A, CHAM_tile_t *B, cublasHandle_t handle);
+int TCUDA_slag2d(int m, int n, const CHAM_tile_t *A, CHAM_tile_t *B, cublasHandle_t handle);
 
 /* ------------------------------------------------------------------------- */
 /* Recorded tile DAGs: the runtime-plugin boundary of the reference           */

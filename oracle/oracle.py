@@ -117,6 +117,8 @@ def reference(ncores=0):
                                           ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp, _dp]
         L.chamref_lapacke_dsposv.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp, ctypes.c_int, _dp,
                                              ctypes.c_int, _dp, ctypes.c_int, _ip, _dp]
+        L.chamref_dinverse.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp,
+                                       ctypes.c_int]
         L.chamref_init(ncores if ncores > 0 else (os.cpu_count() or 1))
     return _ref
 
@@ -188,3 +190,13 @@ def ref_dplrnt(M, N, seed, NB=384):
     A = np.zeros((M, N), order="F")
     L.chamref_dplrnt(M, N, _ptr(A), max(M, 1), NB, seed)
     return A
+
+
+def ref_dinverse(op, uplo, A, NB, diag=131):
+    """Reference CHAMELEON_dpotri / dtrtri / dlauum (op "potri" / "trtri" /
+    "lauum"; compute/zpotri.c, ztrtri.c, zlauum.c) on a copy; returns (A', info)."""
+    L = reference()
+    X = np.asfortranarray(A.copy())
+    N = X.shape[0]
+    info = L.chamref_dinverse({"potri": 0, "trtri": 1, "lauum": 2}[op], uplo, diag, N, NB, _ptr(X), max(N, 1))
+    return X, info

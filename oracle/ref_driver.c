@@ -104,6 +104,25 @@ int chamref_dpotrs(int uplo, int N, int nrhs, int nb, double *A, int lda,
     return rc;
 }
 
+/* CHAMELEON_dpotri / dtrtri / dlauum (compute/zpotri.c, ztrtri.c, zlauum.c)
+ * on caller arrays: op 0 = potri, 1 = trtri, 2 = lauum. */
+int chamref_dinverse(int op, int uplo, int diag, int N, int nb, double *A, int lda)
+{
+    int rc = 0;
+    CHAMELEON_Set(CHAMELEON_TILE_SIZE, nb);
+#pragma omp parallel
+#pragma omp master
+    {
+        if (op == 0)
+            rc = CHAMELEON_dpotri((cham_uplo_t)uplo, N, A, lda);
+        else if (op == 1)
+            rc = CHAMELEON_dtrtri((cham_uplo_t)uplo, (cham_diag_t)diag, N, A, lda);
+        else
+            rc = CHAMELEON_dlauum((cham_uplo_t)uplo, N, A, lda);
+    }
+    return rc;
+}
+
 /*
  * The testing driver's descriptor path (testing/testing_zposv.c:40-109):
  * tile-allocated descriptors, A from dplgsy(bump = N, uplo, seedA) (only the

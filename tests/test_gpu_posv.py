@@ -392,3 +392,53 @@ def test_default_stream_writes_are_ordered_before_the_call(cb, uplo):
         assert r < 60, r
         dA.destroy()
         dB.destroy()
+
+
+def test_tcuda_tile_forms_match_the_array_forms(cb, orc, handle):
+    """TCUDA_d* (gpucublas_ztile.h) take CHAM_tile_t operands, as the runtimes'
+    codelets pass them, and give the CUDA_d* results bit for bit; a tile that
+    is not full-rank is refused."""
+    import torch
+    L = cb.lib()
+    n, k = 96, 64
+
+    def tile(t, rows, cols, fmt=cb.CHAMELEON_TILE_FULLRANK):
+        return cb.CHAM_tile_t(t.data_ptr(), 0, rows, cols, rows, fmt, cb.ChamRealDouble)
+
+    rng = np.random.default_rng(5)
+    A = _dev(rng.standard_normal((n, k)))
+    B = _dev(rng.standard_normal((n, k)))
+    C1 = _dev(rng.standard_normal((n, n)))
+    C2 = C1.clone()
+    al, be = ctypes.c_double(-1.0), ctypes.c_double(1.0)
+    assert L.CUDA_dgemm(111, 112, n, n, k, ctypes.byref(al), ctypes.c_void_p(A.data_ptr()), n,
+                        ctypes.c_void_p(B.data_ptr()), n, ctypes.byref(be), ctypes.c_void_p(C1.data_ptr()), n,
+                        handle) == 0
+    tA, tB, tC = tile(A, n, k), tile(B, n, k), tile(C2, n, n)
+    assert L.TCUDA_dgemm(111, 112, n, n, k, ctypes.byref(al), ctypes.byref(tA), ctypes.byref(tB), ctypes.byref(be),
+                         ctypes.byref(tC), handle) == 0
+    torch.cuda.synchronize()
+    assert torch.equal(C1, C2)
+    S = orc.dplgsy(float(n), n, 7)
+    P1, P2 = _dev(S), _dev(S)
+    i1 = torch.zeros(1, dtype=torch.int32, device="cuda")
+    i2 = torch.zeros(1, dtype=torch.int32, device="cuda")
+    assert L.CUDA_dpotrf(122, n, ctypes.c_void_p(P1.data_ptr()), n, None, 0, ctypes.c_void_p(i1.data_ptr()),
+                         handle) == 0
+    tP = tile(P2, n, n)
+    assert L.TCUDA_dpotrf(122, n, ctypes.byref(tP), None, 0, ctypes.c_void_p(i2.data_ptr()), handle) == 0
+    torch.cuda.synchronize()
+    assert torch.equal(P1, P2) and int(i1.item()) == int(i2.item()) == 0
+    X1, X2 = _dev(rng.standard_normal((n, k))), None
+    X2 = X1.clone()
+    one = ctypes.c_double(1.0)
+    assert L.CUDA_dtrsm(141, 122, 111, 131, n, k, ctypes.byref(one), ctypes.c_void_p(P1.data_ptr()), n,
+                        ctypes.c_void_p(X1.data_ptr()), n, handle) == 0
+    tX = tile(X2, n, k)
+    assert L.TCUDA_dtrsm(141, 122, 111, 131, n, k, ctypes.byref(one), ctypes.byref(tP), ctypes.byref(tX),
+                         handle) == 0
+    torch.cuda.synchronize()
+    assert torch.equal(X1, X2)
+    bad = tile(C2, n, n, cb.CHAMELEON_TILE_DESC)
+    assert L.TCUDA_dsyrk(122, 111, n, k, ctypes.byref(al), ctypes.byref(tA), ctypes.byref(be), ctypes.byref(bad),
+                         handle) == -103

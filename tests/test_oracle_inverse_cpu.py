@@ -1,0 +1,34 @@
+"""The reference's CPU dpotri / dtrtri / dlauum (compute/zpotri.c, ztrtri.c,
+zlauum.c, built from its sources into the oracle) agree with numpy, so that
+the GPU parity tests may use them as the checker."""
+import numpy as np
+import pytest
+
+EPS = 1.1102230246251565e-16
+
+
+@pytest.fixture(scope="module")
+def ref(orc):
+    if not orc.reference_available():
+        pytest.skip("reference CPU build absent")
+    return orc
+
+
+@pytest.mark.parametrize("uplo", [121, 122])
+def test_reference_potri_trtri_lauum_vs_numpy(ref, uplo):
+    N = 300
+    tri = np.triu if uplo == 121 else np.tril
+    A = ref.dplgsy(float(N), N, 51)
+    L = np.linalg.cholesky(A)
+    F = L.T if uplo == 121 else L
+    Xr, info = ref.ref_dinverse("potri", uplo, F, 64)
+    assert info == 0
+    inv = np.linalg.inv(A)
+    assert np.abs(tri(Xr) - tri(inv)).max() <= 64 * N * EPS * np.abs(inv).max()
+    Tr, info = ref.ref_dinverse("trtri", uplo, F, 96)
+    assert info == 0
+    assert np.abs(tri(Tr) - np.linalg.inv(F)).max() <= 64 * N * EPS * np.abs(np.linalg.inv(F)).max() ** 2
+    Pr, info = ref.ref_dinverse("lauum", uplo, F, 80)
+    assert info == 0
+    P = F.T @ F if uplo == 122 else F @ F.T
+    assert np.abs(tri(Pr) - tri(P)).max() <= 4 * N * EPS * np.abs(P).max()
