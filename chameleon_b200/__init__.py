@@ -149,6 +149,9 @@ PROTOS = {
     "CHAMELEON_dpotrs_Tile_Async": (_i, [_i, _D, _D, _vp, _vp]),
     "CHAMELEON_dpotrf_batch_Tile": (_i, [_i, _D]),
     "CHAMELEON_dtrsm_batch_Tile": (_i, [_i, _i, _i, _i, ctypes.c_double, _D, _D]),
+    "CHAM_B200_Dispatch_Cost": (ctypes.c_double, [_i, _i]),
+    "CHAM_B200_Dispatch_Bytes": (ctypes.c_double, [_i, _i]),
+    "CHAM_B200_Dispatch_Plan": (_i, [_i, _vp, _vp, _vp, _i, _vp, _vp, _vp, _vp, _vp]),
     "CHAMELEON_dtrtri": (_i, [_i, _i, _i, _vp, _i]),
     "CHAMELEON_dlauum": (_i, [_i, _i, _vp, _i]),
     "CHAMELEON_dpotri": (_i, [_i, _i, _vp, _i]),

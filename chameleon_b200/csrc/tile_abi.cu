@@ -137,27 +137,65 @@ __global__ void plrnt_tile_kernel(double *A, int lda, int M, int N, int bigM, in
 }
 
 // dlag2s: FP64 -> FP32 with LAPACK's overflow rule (|a| > FLT_MAX sets the
-// flag); the reference's GPU kernel (gpucublas/compute/cuda_zlag2c.cu:38-106)
-// tests `ind > m` where `ind >= m` is meant and never reports its flag; here
-// rows are bounded by `m` and the flag is kept in the handle.
+// flag; NaN does not); the reference's GPU kernel (gpucublas/compute/
+// cuda_zlag2c.cu:38-106) tests `ind > m` where `ind >= m` is meant and never
+// reports its flag; here rows are bounded by `m` and the flag is kept in the
+// handle.  Both casts run column-blocked (blockIdx.y strides the columns, so
+// no division per element) with 4 rows per thread: two 16-byte FP64 accesses
+// and one 16-byte FP32 access where the column pointers allow it.
+constexpr double kFltMax = 3.4028234663852886e38;
+
+__device__ __forceinline__ bool aligned16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
+
 __global__ void dlag2s_kernel(const double *A, int lda, float *SA, int ldsa, int M, int N, int *flag) {
-    const int64_t total = (int64_t)M * N;
-    for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
-         idx += (int64_t)gridDim.x * blockDim.x) {
-        const int i = (int)(idx % M), j = (int)(idx / M);
-        const double a = A[i + (int64_t)j * lda];
-        if (fabs(a) > 3.4028234663852886e38) *flag = 1;
-        SA[i + (int64_t)j * ldsa] = __double2float_rn(a);
+    bool ovf = false;
+    for (int j = blockIdx.y; j < N; j += gridDim.y) {
+        const double *a = A + (int64_t)j * lda;
+        float *sa = SA + (int64_t)j * ldsa;
+        const bool vec = aligned16(a) && aligned16(sa);
+        for (int i0 = (blockIdx.x * blockDim.x + threadIdx.x) * 4; i0 < M; i0 += gridDim.x * blockDim.x * 4) {
+            if (vec && i0 + 3 < M) {
+                const double2 x = *reinterpret_cast<const double2 *>(a + i0);
+                const double2 y = *reinterpret_cast<const double2 *>(a + i0 + 2);
+                ovf |= fabs(x.x) > kFltMax || fabs(x.y) > kFltMax || fabs(y.x) > kFltMax || fabs(y.y) > kFltMax;
+                *reinterpret_cast<float4 *>(sa + i0) =
+                    make_float4(__double2float_rn(x.x), __double2float_rn(x.y), __double2float_rn(y.x),
+                                __double2float_rn(y.y));
+            } else {
+                for (int i = i0; i < min(i0 + 4, M); ++i) {
+                    const double v = a[i];
+                    ovf |= fabs(v) > kFltMax;
+                    sa[i] = __double2float_rn(v);
+                }
+            }
+        }
     }
+    if (ovf) *flag = 1;
 }
 
 __global__ void slag2d_kernel(const float *SA, int ldsa, double *A, int lda, int M, int N) {
-    const int64_t total = (int64_t)M * N;
-    for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
-         idx += (int64_t)gridDim.x * blockDim.x) {
-        const int i = (int)(idx % M), j = (int)(idx / M);
-        A[i + (int64_t)j * lda] = (double)SA[i + (int64_t)j * ldsa];
+    for (int j = blockIdx.y; j < N; j += gridDim.y) {
+        const float *sa = SA + (int64_t)j * ldsa;
+        double *a = A + (int64_t)j * lda;
+        const bool vec = aligned16(a) && aligned16(sa);
+        for (int i0 = (blockIdx.x * blockDim.x + threadIdx.x) * 4; i0 < M; i0 += gridDim.x * blockDim.x * 4) {
+            if (vec && i0 + 3 < M) {
+                const float4 x = *reinterpret_cast<const float4 *>(sa + i0);
+                *reinterpret_cast<double2 *>(a + i0) = make_double2(x.x, x.y);
+                *reinterpret_cast<double2 *>(a + i0 + 2) = make_double2(x.z, x.w);
+            } else {
+                for (int i = i0; i < min(i0 + 4, M); ++i) a[i] = (double)sa[i];
+            }
+        }
     }
+}
+
+// Column-blocked grid of the casts: x covers the rows (1024 per block), y the
+// columns, about 16 blocks of 256 threads per SM in all.
+static dim3 cast_grid(int m, int n) {
+    const int gx = std::max(1, std::min((m + 1023) / 1024, 148 * 16));
+    const int gy = std::max(1, std::min({n, 65535, std::max(1, 148 * 16 / gx)}));
+    return dim3(gx, gy);
 }
 
 static int ew_grid(int64_t total) {
@@ -355,7 +393,7 @@ int CUDA_dlag2s(int m, int n, const double *A, int lda, float *SA, int ldsa, cub
     if (lda < std::max(1, m)) return -4;
     if (ldsa < std::max(1, m)) return -6;
     if (m == 0 || n == 0) return 0;
-    dlag2s_kernel<<<ew_grid((int64_t)m * n), 256, 0, handle->stream>>>(A, lda, SA, ldsa, m, n, handle->flag);
+    dlag2s_kernel<<<cast_grid(m, n), 256, 0, handle->stream>>>(A, lda, SA, ldsa, m, n, handle->flag);
     CHB_LAUNCHED(1);
     return cudaGetLastError() == cudaSuccess ? CHAMELEON_SUCCESS : CHAMELEON_ERR_UNEXPECTED;
 }
@@ -367,7 +405,7 @@ int CUDA_slag2d(int m, int n, const float *SA, int ldsa, double *A, int lda, cub
     if (ldsa < std::max(1, m)) return -4;
     if (lda < std::max(1, m)) return -6;
     if (m == 0 || n == 0) return 0;
-    slag2d_kernel<<<ew_grid((int64_t)m * n), 256, 0, handle->stream>>>(SA, ldsa, A, lda, m, n);
+    slag2d_kernel<<<cast_grid(m, n), 256, 0, handle->stream>>>(SA, ldsa, A, lda, m, n);
     CHB_LAUNCHED(1);
     return cudaGetLastError() == cudaSuccess ? CHAMELEON_SUCCESS : CHAMELEON_ERR_UNEXPECTED;
 }

@@ -447,6 +447,26 @@ int    CHAM_B200_Serve_Stats(CHAM_b200_server_t server, CHAM_b200_serve_stats_t 
 int    CHAM_B200_Serve_Destroy(CHAM_b200_server_t server);     /* drains first          */
 double CHAM_B200_Serve_Now(void);
 
+/* ------------------------------------------------------------------------- */
+/* Multi-GPU dispatch of independent systems (new; host planning only, no    */
+/* device call).  Batches and serving requests shard over the GPUs of a node  */
+/* with no collective: the plan says which GPU solves which system.          */
+/* ------------------------------------------------------------------------- */
+/* Estimated device seconds / device bytes of one system of order n with nrhs
+ * right-hand sides inside a batch or serving wave. */
+double CHAM_B200_Dispatch_Cost(int n, int nrhs);
+double CHAM_B200_Dispatch_Bytes(int n, int nrhs);
+/* Longest-first list schedule of `count` systems over `nranks` GPUs: owner[i]
+ * = the GPU of system i (pin[i] >= 0 forces a live GPU; pin may be NULL),
+ * only GPUs with alive[r] != 0, each GPU's systems of one wave fitting in
+ * free_bytes[r]; load_s[r] (may be NULL) = seconds of work the GPU already
+ * has; wave[i] (may be NULL) = the wave of system i.  Returns the number of
+ * waves, CHAMELEON_ERR_OUT_OF_RESOURCES when a system fits on no live GPU,
+ * CHAMELEON_ERR_NOT_INITIALIZED when no GPU is alive. */
+int CHAM_B200_Dispatch_Plan(int count, const int *n, const int *nrhs, const int *pin, int nranks,
+                            const int *alive, const double *free_bytes, const double *load_s, int *owner,
+                            int *wave);
+
 #ifdef __cplusplus
 }
 #endif

@@ -322,9 +322,10 @@ def test_cuda_generators_match_oracle(cb, orc, handle):
         assert np.array_equal(_host(dA, (m, n)), full[mm0:mm0 + m, nn0:nn0 + n])
 
 
-def test_cuda_lag2(cb, handle):
+@pytest.mark.parametrize("m,n", [(70, 33), (4096, 64), (1027, 5), (1, 1), (3, 300)])
+def test_cuda_lag2(cb, handle, m, n):
+    """Aligned (vector) and unaligned (scalar) columns, ragged row ends."""
     import torch
-    m, n = 70, 33
     rng = np.random.default_rng(1)
     A = rng.standard_normal((m, n))
     dA = _dev(A)
@@ -339,6 +340,17 @@ def test_cuda_lag2(cb, handle):
                                 handle) == 0
     torch.cuda.synchronize()
     assert np.array_equal(_host(dB, (m, n)), A.astype(np.float32).astype(np.float64))
+    # LAPACK's overflow rule: |a| > FLT_MAX sets the flag, NaN does not
+    A[m // 2, n - 1] = np.nan
+    dN = _dev(A)
+    assert cb.lib().CUDA_dlag2s(m, n, ctypes.c_void_p(dN.data_ptr()), m, ctypes.c_void_p(dS.data_ptr()), m,
+                                handle) == 0
+    assert cb.lib().CHAM_B200_Handle_Overflow(handle) == 0
+    A[m - 1, n // 2] = -1e39
+    dO = _dev(A)
+    assert cb.lib().CUDA_dlag2s(m, n, ctypes.c_void_p(dO.data_ptr()), m, ctypes.c_void_p(dS.data_ptr()), m,
+                                handle) == 0
+    assert cb.lib().CHAM_B200_Handle_Overflow(handle) == 1
 
 
 @pytest.mark.parametrize("uplo", [121, 122])
