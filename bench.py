@@ -361,7 +361,29 @@ def batch_section(args, cb, world, rank):
             assert rc == 0, rc
         torch.cuda.synchronize()
         plain_ms = (time.perf_counter() - t0) * 1e3 * count / m
-    tune = (ctypes.c_double * 5)()
+    # second plain path: the tile ABI per matrix (CUDA_dpotrf + two CUDA_dtrsm,
+    # all on one stream, device arrays), every matrix of the batch
+    A.copy_(A0)
+    B.copy_(B0)
+    torch.cuda.synchronize()
+    hh = ctypes.c_void_p()
+    assert L.CHAM_B200_Handle_Create(ctypes.byref(hh), None) == 0
+    dinfo = torch.zeros(1, dtype=torch.int32, device="cuda")
+    one = ctypes.c_double(1.0)
+    L.CHAM_B200_Event_Record(6)
+    for i in range(count):
+        ni, ki = int(n[i]), int(k[i])
+        pa = ctypes.c_void_p(A.data_ptr() + 8 * int(a_off[i]))
+        pb = ctypes.c_void_p(B.data_ptr() + 8 * int(b_off[i]))
+        assert L.CUDA_dpotrf(cb.ChamLower, ni, pa, ni, None, 0, ptr(dinfo), hh) == 0
+        assert L.CUDA_dtrsm(cb.ChamLeft, cb.ChamLower, cb.ChamNoTrans, cb.ChamNonUnit, ni, ki, ctypes.byref(one),
+                            pa, ni, pb, ni, hh) == 0
+        assert L.CUDA_dtrsm(cb.ChamLeft, cb.ChamLower, cb.ChamTrans, cb.ChamNonUnit, ni, ki, ctypes.byref(one),
+                            pa, ni, pb, ni, hh) == 0
+    L.CHAM_B200_Event_Record(7)
+    tile_abi_ms = L.CHAM_B200_Event_Elapsed(6, 7)
+    L.CHAM_B200_Handle_Destroy(hh)
+    tune = (ctypes.c_double * 28)()
     L.CHAM_B200_Batch_Tuning(cb.ChamRealDouble, tune)
     # FP32 systems: the same batch cast to FP32 through CHAM_B200_sposv_batch
     A32, B32 = A0.float(), B0.float()
@@ -391,13 +413,18 @@ def batch_section(args, cb, world, rank):
                               "sampled_matrices": min(count, args.batch_plain),
                               "api": "CHAMELEON_dposv per matrix (device arrays)"} if plain_ms else None),
         "speedup_vs_plain": (plain_ms / ms_max) if plain_ms else None,
+        "plain_tile_abi": {"solves_per_s": count / (tile_abi_ms * 1e-3), "ms": tile_abi_ms,
+                           "api": "CUDA_dpotrf + 2 x CUDA_dtrsm per matrix on one stream (device arrays)"},
+        "speedup_vs_tile_abi": tile_abi_ms / ms_max,
         "fp32": {"solves_per_s": count * world / (ms32 * 1e-3), "ms_per_step": ms32,
                  "api": "CHAM_B200_sposv_batch (FP32 systems)"},
-        "size_bins": {"small_n_max": 64, "small_bin_mode": int(tune[0]),
-                      "small_bin_modes_ms": {"generic": tune[1], "small_x1": tune[2], "small_x2": tune[3],
-                                             "small_x3": tune[4]},
-                      "note": "autotuner: the small bin runs on the generic kernel or the small-system kernel at "
-                              "1..3 CTAs per SM, whichever was fastest on 4096 synthetic systems"},
+        "size_bins": {"ranges": ["n<=64", "65..128", "129..256", "257+"],
+                      "shape_per_range": [int(tune[r]) for r in range(4)],
+                      "shape_ms_per_range": [[round(tune[4 + 6 * r + j], 4) for j in range(6)] for r in range(4)],
+                      "shapes": ["generic x1", "small x1", "small x2", "small x3", "lean x2", "lean x3"],
+                      "note": "autotuner: each size range runs the shape (kernel and CTAs per SM) that was "
+                              "fastest on a synthetic batch of that range (-1: not admissible); adjacent "
+                              "ranges with the same shape run as one launch"},
         "roofline": {"bound": "fp64", "achieved": flops / (ms_max * 1e-3) / 1e12, "peak": 40.0,
                      "unit": "TFLOP/s", "frac": flops / (ms_max * 1e-3) / 1e12 / 40.0,
                      "peak_source": "FP64 spec 40 TFLOP/s (fallback: no FP64 entry in the measured peaks)"},

@@ -233,6 +233,7 @@ EXTRAS = {
     "CHAM_B200_Test_TC05": (_i, [_vp, _vp, _i, _vp]),
     "CHAM_B200_Mixed_Factor_Only": (_i, [_i, _i, _D, _D, ctypes.POINTER(ctypes.c_float)]),
     "CHAM_B200_Batch_Tuning": (_i, [_i, _dp]),
+    "CHAM_B200_Batch_SetShape": (_i, [_i, _i, _i]),
 }
 
 _lib = None

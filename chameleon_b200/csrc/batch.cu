@@ -3,24 +3,29 @@
 // Reference: CHAMELEON_dpotrf_batch_Tile / CHAMELEON_dtrsm_batch_Tile
 // (compute/zpotrf_batch.c:28-118, compute/ztrsm_batch.c:37-213) map one CPU task
 // per tile through chameleon_pmap (compute/pmap.c:25-93); potrf has no GPU
-// path there (`.cudafunc = NULL`, zpotrf_batch.c:58-64).  Here a batch is split
-// into two size bins, each ONE persistent launch where a CTA takes the next
-// system from an atomic cursor (largest first, so the long tail starts early):
+// path there (`.cudafunc = NULL`, zpotrf_batch.c:58-64).  Here a batch is
+// sorted largest first and split into size ranges (n <= 64, 65..128,
+// 129..256, 257+); each range runs as ONE persistent launch in which a CTA
+// takes the next system from an atomic cursor, in one of these shapes:
 //
-//   * n > 64: the tile routines (64-wide leaf Cholesky, panel GEMMs on the
+//   * generic: the tile routines (64-wide leaf Cholesky, panel GEMMs on the
 //     tensor cores, inverted diagonal blocks in a per-CTA scratch slot), one
-//     256-thread CTA per SM;
-//   * n <= 64: the whole system in shared memory -- leaf Cholesky + inverse,
-//     then X = L^-T L^-1 B by two small products -- with a footprint that lets
-//     several CTAs share an SM.  How the small bin runs (the generic kernel, or
-//     the small kernel at 1..3 CTAs per SM) is chosen once per device and
-//     element type by timing each option on synthetic systems (autotune_small).
+//     177 KB CTA per SM;
+//   * lean generic: the same routines with 64-row panels and the leaf blocks
+//     aliased onto the GEMM staging area (74 KB for FP64), 2 or 3 CTAs per SM,
+//     so that the latency-bound leaf of one system overlaps the work of the
+//     systems beside it;
+//   * small (n <= 64): the whole system in shared memory -- leaf Cholesky +
+//     inverse, then X = L^-T L^-1 B by two small products over the live
+//     right-hand-side columns -- at 1..3 CTAs per SM.
 //
-// The small bin runs on a side stream, so its CTAs fill SMs as the large bin's
-// tail drains.  CHAM_B200_dposv_batch / sposv_batch (uneven sizes, no
-// reference equivalent: the reference batch API is uniform-size) capture the
-// whole sequence in a CUDA graph per batch signature and replay it when the
-// same batch comes again.
+// The shape of each range is picked once per device and element type by
+// timing the admissible shapes on synthetic systems of that range; adjacent
+// ranges with the same shape merge into one launch.  A small-kernel range
+// runs on a side stream, so its CTAs fill SMs as the larger ranges drain.
+// CHAM_B200_dposv_batch / sposv_batch (uneven sizes, no reference equivalent:
+// the reference batch API is uniform-size) capture the whole sequence in a
+// CUDA graph per batch signature and replay it when the same batch comes again.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -35,10 +40,13 @@
 namespace chb {
 
 // Generic bin: factor (+ forward and backward solve) of one system per task.
-template <class T>
-__global__ void __launch_bounds__(NT_CTA, 1) posv_batch_kernel(const BatchItem *items, int count, T *A, T *B,
-                                                               int upper, int *info, int *cursor, T *scratch,
-                                                               int nib) {
+// LEAN: 64-row panels and the leaf blocks aliased onto the GEMM staging area
+// (rec::lean_smem_elems), MINB CTAs per SM, so that the latency-bound leaf of
+// one system overlaps the GEMMs and leaves of the systems beside it.
+template <class T, bool LEAN = false, int MINB = 1>
+__global__ void __launch_bounds__(NT_CTA, MINB) posv_batch_kernel(const BatchItem *items, int count, T *A, T *B,
+                                                                  int upper, int *info, int *cursor, T *scratch,
+                                                                  int nib) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     T *smem = reinterpret_cast<T *>(smem_raw);
     __shared__ int s_i;
@@ -51,7 +59,8 @@ __global__ void __launch_bounds__(NT_CTA, 1) posv_batch_kernel(const BatchItem *
         if (i >= count) break;
         const BatchItem it = items[i];
         const ViewT<T> Lv = upper ? ViewT<T>{A + it.a_off, it.lda, 1} : ViewT<T>{A + it.a_off, 1, it.lda};
-        const int r = rec::tile_potrf_blk<T, SPLIT_BF16X3>(Lv, it.n, invd, smem);
+        const int r = LEAN ? rec::tile_potrf_blk<T, SPLIT_BF16X3, 64, true>(Lv, it.n, invd, smem)
+                           : rec::tile_potrf_blk<T, SPLIT_BF16X3>(Lv, it.n, invd, smem);
         if (threadIdx.x == 0 && info) info[it.info_idx] = r;
         if (r == 0 && it.nrhs > 0) {
             const ViewT<T> X{B + it.b_off, 1, it.ldb};
@@ -65,18 +74,19 @@ __global__ void __launch_bounds__(NT_CTA, 1) posv_batch_kernel(const BatchItem *
     }
 }
 
+template <class T>
+constexpr size_t lean_smem_bytes() {
+    return sizeof(T) * rec::lean_smem_elems<T, SPLIT_BF16X3>() + 64;
+}
+
 // Small bin (n <= 64): system in shared memory.  sD holds the identity-padded
 // block, then L, then the right-hand sides being solved; sX the inverse.
 template <class T>
 constexpr size_t small_smem_bytes() {
     return 2 * 64 * rec::LDS * sizeof(T);
 }
-template <class T>
-constexpr int small_min_blocks() {
-    return sizeof(T) == 8 ? 2 : 3;
-}
-template <class T>
-__global__ void __launch_bounds__(NT_CTA, small_min_blocks<T>())
+template <class T, int MINB>
+__global__ void __launch_bounds__(NT_CTA, MINB)
     posv_small_kernel(const BatchItem *items, int count, T *A, T *B, int upper, int *info, int *cursor) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     T *sD = reinterpret_cast<T *>(smem_raw);
@@ -110,31 +120,37 @@ __global__ void __launch_bounds__(NT_CTA, small_min_blocks<T>())
                 sD[rr + cc * LDS] = (rr < n && cc < w) ? Bc[rr + (int64_t)cc * it.ldb] : T(0);
             }
             __syncthreads();
+            // thread (rr = tid & 63, cc = tid / 64 + 4 q) owns output (rr, cc);
+            // only the w live columns are computed (cc is uniform per warp)
             T y[16];
             // Y = X B (X lower, zero above the diagonal, identity beyond n)
 #pragma unroll
             for (int q = 0; q < 16; ++q) {
                 const int idx = tid + NT_CTA * q, rr = idx & 63, cc = idx >> 6;
                 T acc = T(0);
+                if (cc < w) {
 #pragma unroll 8
-                for (int k = 0; k < 64; ++k) acc += sX[rr + k * LDS] * sD[k + cc * LDS];
+                    for (int k = 0; k < 64; ++k) acc += sX[rr + k * LDS] * sD[k + cc * LDS];
+                }
                 y[q] = acc;
             }
             __syncthreads();
 #pragma unroll
             for (int q = 0; q < 16; ++q) {
                 const int idx = tid + NT_CTA * q;
-                sD[(idx & 63) + (idx >> 6) * LDS] = y[q];
+                if ((idx >> 6) < w) sD[(idx & 63) + (idx >> 6) * LDS] = y[q];
             }
             __syncthreads();
             // X_out = X^T Y
 #pragma unroll
             for (int q = 0; q < 16; ++q) {
                 const int idx = tid + NT_CTA * q, rr = idx & 63, cc = idx >> 6;
-                T acc = T(0);
+                if (cc < w) {
+                    T acc = T(0);
 #pragma unroll 8
-                for (int k = 0; k < 64; ++k) acc += sX[k + rr * LDS] * sD[k + cc * LDS];
-                if (rr < n && cc < w) Bc[rr + (int64_t)cc * it.ldb] = acc;
+                    for (int k = 0; k < 64; ++k) acc += sX[k + rr * LDS] * sD[k + cc * LDS];
+                    if (rr < n) Bc[rr + (int64_t)cc * it.ldb] = acc;
+                }
             }
         }
         __syncthreads();
@@ -195,7 +211,7 @@ BatchWs g_bws;
 
 // Grow-only, stream-ordered (no device-wide synchronization when growing).
 int bws_reserve(BatchWs &ws, size_t item_bytes, size_t scratch_bytes, size_t ninfo) {
-    if (!ws.cursor && !(ws.cursor = (int *)dev_alloc(2 * sizeof(int)))) return CHAMELEON_ERR_OUT_OF_RESOURCES;
+    if (!ws.cursor && !(ws.cursor = (int *)dev_alloc(8 * sizeof(int)))) return CHAMELEON_ERR_OUT_OF_RESOURCES;
     if (item_bytes > ws.items_bytes) {
         dev_free(ws.items);
         ws.items_bytes = 0;
@@ -225,28 +241,116 @@ int set_attrs() {
                                   (int)tile_smem_bytes<double>()));
     CHB_CUDA(cudaFuncSetAttribute(posv_batch_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)tile_smem_bytes<float>()));
-    CHB_CUDA(cudaFuncSetAttribute(posv_small_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)small_smem_bytes<double>()));
-    CHB_CUDA(cudaFuncSetAttribute(posv_small_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)small_smem_bytes<float>()));
+    CHB_CUDA(cudaFuncSetAttribute(posv_batch_kernel<double, true, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)lean_smem_bytes<double>()));
+    CHB_CUDA(cudaFuncSetAttribute(posv_batch_kernel<double, true, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)lean_smem_bytes<double>()));
+    CHB_CUDA(cudaFuncSetAttribute(posv_batch_kernel<float, true, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)lean_smem_bytes<float>()));
+    CHB_CUDA(cudaFuncSetAttribute(posv_batch_kernel<float, true, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)lean_smem_bytes<float>()));
+#define CHB_SMALL_ATTR(T, K)                                                                          \
+    CHB_CUDA(cudaFuncSetAttribute(posv_small_kernel<T, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                  (int)small_smem_bytes<T>()))
+    CHB_SMALL_ATTR(double, 1);
+    CHB_SMALL_ATTR(double, 2);
+    CHB_SMALL_ATTR(double, 3);
+    CHB_SMALL_ATTR(float, 1);
+    CHB_SMALL_ATTR(float, 2);
+    CHB_SMALL_ATTR(float, 3);
+#undef CHB_SMALL_ATTR
     CHB_CUDA(cudaFuncSetAttribute(trsm_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)TILE_KERNEL_SMEM_BYTES));
     g_attr = true;
     return 0;
 }
 
-// How the small bin runs: 0 = generic kernel, k >= 1 = small kernel with k CTAs
-// per SM.  Chosen by autotune_small (per element type), times kept for reporting.
-struct SmallTune {
-    int mode = -1;
-    float ms[4] = {-1.f, -1.f, -1.f, -1.f};
+// Size ranges of a batch and the kernel shapes that can run them.  Range 0 is
+// n <= 64 (whole system in shared memory possible), ranges 1..3 are 65..128,
+// 129..256 and 257+.  Shapes: 0 = generic kernel, one 177 KB CTA per SM;
+// 1..3 = small-system kernel at 1..3 CTAs per SM (range 0 only); 4 / 5 = lean
+// generic kernel at 2 / 3 CTAs per SM.  The shape of each range is chosen once
+// per device and element type, the first time a batch has systems in that
+// range, by timing every admissible shape on synthetic systems of the range
+// (autotune_range); adjacent ranges that pick the same shape run as one bin
+// (one persistent launch), so the bin boundaries follow from the tuning.
+constexpr int NRANGE = 4;
+constexpr int NSHAPE = 6;
+constexpr int RANGE_LO[NRANGE] = {1, 65, 129, 257};
+constexpr int RANGE_HI[NRANGE] = {64, 128, 256, 1 << 30};
+constexpr int TUNE_HI[NRANGE] = {64, 128, 256, 512};   // synthetic sizes of the top range
+
+int range_of(int n) {
+    int r = 0;
+    while (r < NRANGE - 1 && n > RANGE_HI[r]) ++r;
+    return r;
+}
+
+struct BinTune {
+    int mode[NRANGE] = {-1, -1, -1, -1};
+    float ms[NRANGE][NSHAPE];
+    BinTune() {
+        for (auto &r : ms)
+            for (float &v : r) v = -1.f;
+    }
 };
-SmallTune g_tune[2];   // [0] double, [1] float
+BinTune g_tune[2];   // [0] double, [1] float
 std::mutex g_tune_mu;
 
 template <class T>
 constexpr int tidx() {
     return sizeof(T) == 8 ? 0 : 1;
+}
+
+// CTAs per SM of a shape, and whether the device runs it at that occupancy.
+int shape_ctas(int shape) { return shape == 0 ? 1 : shape <= 3 ? shape : shape - 2; }
+
+template <class T>
+bool shape_fits(int shape) {
+    int occ = 0;
+    switch (shape) {
+    case 0: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, posv_batch_kernel<T, false, 1>, NT_CTA, tile_smem_bytes<T>()); break;
+    case 1: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, posv_small_kernel<T, 1>, NT_CTA, small_smem_bytes<T>()); break;
+    case 2: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, posv_small_kernel<T, 2>, NT_CTA, small_smem_bytes<T>()); break;
+    case 3: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, posv_small_kernel<T, 3>, NT_CTA, small_smem_bytes<T>()); break;
+    case 4: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, posv_batch_kernel<T, true, 2>, NT_CTA, lean_smem_bytes<T>()); break;
+    case 5: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, posv_batch_kernel<T, true, 3>, NT_CTA, lean_smem_bytes<T>()); break;
+    default: return false;
+    }
+    cudaGetLastError();
+    return occ >= shape_ctas(shape);
+}
+
+// One persistent launch of `shape` over items [0, cnt) of d_items (largest
+// first); nmax = the largest order among them.  Stream operations only.
+template <class T>
+int launch_shape(int shape, const BatchItem *d_items, int cnt, int nmax, T *A, T *B, int upper, int *info,
+                 int *cursor, cudaStream_t st, BatchWs &ws) {
+    if (cnt <= 0) return 0;
+    const int sms = ctx().num_sms;
+    const int grid = std::min(sms * shape_ctas(shape), cnt);
+    const int nib = std::max(1, (std::max(nmax, 64) + IB - 1) / IB);
+    T *scr = (T *)ws.scratch;
+    switch (shape) {
+    case 0: posv_batch_kernel<T, false, 1><<<grid, NT_CTA, tile_smem_bytes<T>(), st>>>(d_items, cnt, A, B, upper, info, cursor, scr, nib); break;
+    case 1: posv_small_kernel<T, 1><<<grid, NT_CTA, small_smem_bytes<T>(), st>>>(d_items, cnt, A, B, upper, info, cursor); break;
+    case 2: posv_small_kernel<T, 2><<<grid, NT_CTA, small_smem_bytes<T>(), st>>>(d_items, cnt, A, B, upper, info, cursor); break;
+    case 3: posv_small_kernel<T, 3><<<grid, NT_CTA, small_smem_bytes<T>(), st>>>(d_items, cnt, A, B, upper, info, cursor); break;
+    case 4: posv_batch_kernel<T, true, 2><<<grid, NT_CTA, lean_smem_bytes<T>(), st>>>(d_items, cnt, A, B, upper, info, cursor, scr, nib); break;
+    case 5: posv_batch_kernel<T, true, 3><<<grid, NT_CTA, lean_smem_bytes<T>(), st>>>(d_items, cnt, A, B, upper, info, cursor, scr, nib); break;
+    default: return CHAMELEON_ERR_ILLEGAL_VALUE;
+    }
+    CHB_LAUNCHED(1);
+    CHB_CUDA(cudaGetLastError());
+    return 0;
+}
+
+// Scratch the generic shapes need: one slot of inverted diagonal blocks per
+// CTA, for up to 3 CTAs per SM.
+template <class T>
+size_t scratch_bytes(int nmax) {
+    const int nib = std::max(1, (std::max(nmax, 64) + IB - 1) / IB);
+    return (size_t)3 * ctx().num_sms * nib * IB * IB * sizeof(T);
 }
 
 // Synthetic symmetric diagonally dominant systems for the autotuner.
@@ -264,55 +368,53 @@ __global__ void tune_fill_kernel(const BatchItem *items, int count, T *A, T *B) 
     for (int idx = threadIdx.x; idx < it.n * it.nrhs; idx += blockDim.x) B[it.b_off + idx] = T(1);
 }
 
+// Time every admissible shape of range r on 6 systems per SM with orders
+// uniform over the range (4 right-hand sides) and keep the fastest.
 template <class T>
-int launch_bins(const BatchItem *d_items, int nlarge, int nsmall, int nmax_large, T *A, T *B, int upper, int *info,
-                cudaStream_t s, BatchWs &ws, int mode);
-
-// Time each way of running a small bin on 4096 synthetic systems (n ~ U{16..64},
-// 4 right-hand sides) and keep the fastest.  Once per device and element type.
-template <class T>
-int autotune_small(cudaStream_t s, BatchWs &ws) {
+int autotune_range(int r, cudaStream_t s, BatchWs &ws) {
     std::lock_guard<std::mutex> lk(g_tune_mu);
-    SmallTune &tu = g_tune[tidx<T>()];
-    if (tu.mode >= 0) return 0;
-    const int cnt = 4096, k = 4;
+    BinTune &tu = g_tune[tidx<T>()];
+    if (tu.mode[r] >= 0) return 0;
+    const int cnt = 6 * ctx().num_sms, k = 4;
+    const int lo = RANGE_LO[r] < 16 ? 16 : RANGE_LO[r], hi = TUNE_HI[r];
     std::vector<BatchItem> items(cnt);
     int64_t oa = 0, ob = 0;
-    uint32_t st = 12345u;
+    uint32_t st = 12345u + 977u * r;
     for (int i = 0; i < cnt; ++i) {
         st = st * 1664525u + 1013904223u;
-        const int n = 16 + (int)((st >> 8) % 49);
+        const int n = lo + (int)((st >> 8) % (uint32_t)(hi - lo + 1));
         items[i] = BatchItem{oa, ob, n, k, n, n, i, 0};
         oa += (int64_t)n * n;
         ob += (int64_t)n * k;
     }
     std::sort(items.begin(), items.end(), [](const BatchItem &a, const BatchItem &b) { return a.n > b.n; });
+    if (int rc = bws_reserve(ws, 0, scratch_bytes<T>(hi), 0)) return rc;
     T *A = (T *)dev_alloc(oa * sizeof(T)), *B = (T *)dev_alloc(ob * sizeof(T));
     BatchItem *d_items = (BatchItem *)dev_alloc(cnt * sizeof(BatchItem));
     int *d_info = (int *)dev_alloc(cnt * sizeof(int));
-    cudaEvent_t e0, e1;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
     int rc = (A && B && d_items && d_info) ? 0 : CHAMELEON_ERR_OUT_OF_RESOURCES;
     if (!rc) rc = (cudaEventCreate(&e0) == cudaSuccess && cudaEventCreate(&e1) == cudaSuccess) ? 0 : CHAMELEON_ERR_UNEXPECTED;
     if (!rc && cudaMemcpyAsync(d_items, items.data(), cnt * sizeof(BatchItem), cudaMemcpyHostToDevice, s) != cudaSuccess)
         rc = CHAMELEON_ERR_UNEXPECTED;
-    int occ = 1;
-    if (!rc) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, posv_small_kernel<T>, NT_CTA, small_smem_bytes<T>());
     int best = 0;
     float best_ms = 1e30f;
-    for (int mode = 0; mode <= std::min(3, occ) && !rc; ++mode) {
+    for (int shape = 0; shape < NSHAPE && !rc; ++shape) {
+        if ((r > 0 && shape >= 1 && shape <= 3) || !shape_fits<T>(shape)) continue;
         float t = 0.f;
         for (int rep = 0; rep < 2 && !rc; ++rep) {   // rep 0 warms the kernel up
             tune_fill_kernel<T><<<cnt, 128, 0, s>>>(d_items, cnt, A, B);
+            if (cudaMemsetAsync(ws.cursor + 7, 0, sizeof(int), s) != cudaSuccess) rc = CHAMELEON_ERR_UNEXPECTED;
             cudaEventRecord(e0, s);
-            rc = launch_bins<T>(d_items, 0, cnt, 0, A, B, 0, d_info, s, ws, mode);
+            if (!rc) rc = launch_shape<T>(shape, d_items, cnt, items[0].n, A, B, 0, d_info, ws.cursor + 7, s, ws);
             cudaEventRecord(e1, s);
             if (!rc && cudaEventSynchronize(e1) != cudaSuccess) rc = CHAMELEON_ERR_UNEXPECTED;
             if (!rc) cudaEventElapsedTime(&t, e0, e1);
         }
-        tu.ms[mode] = t;
+        tu.ms[r][shape] = t;
         if (!rc && t < best_ms) {
             best_ms = t;
-            best = mode;
+            best = shape;
         }
     }
     cudaStreamSynchronize(s);
@@ -320,68 +422,90 @@ int autotune_small(cudaStream_t s, BatchWs &ws) {
     dev_free(B);
     dev_free(d_items);
     dev_free(d_info);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
     if (rc) return rc;
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    tu.mode = best;
+    tu.mode[r] = best;
     return 0;
 }
 
-// Launch the two bins: items [0, nlarge) (n > 64, largest first) on the generic
-// kernel on `s`, items [nlarge, nlarge + nsmall) on the side stream per `mode`;
-// `s` waits for both.  Only stream operations (capturable).
+// Items sorted largest first, split into the size ranges: range r is
+// [beg[r], beg[r] + cnt[r]), nmax[r] its largest order.
+struct Bins {
+    int beg[NRANGE] = {0, 0, 0, 0}, cnt[NRANGE] = {0, 0, 0, 0}, nmax[NRANGE] = {0, 0, 0, 0};
+    int nmax_all = 0;
+};
+Bins make_bins(std::vector<BatchItem> &items) {
+    std::stable_sort(items.begin(), items.end(), [](const BatchItem &a, const BatchItem &b) { return a.n > b.n; });
+    Bins b;
+    b.nmax_all = items.empty() ? 0 : items[0].n;
+    for (int i = 0; i < (int)items.size(); ++i) {
+        const int r = range_of(items[i].n);
+        if (b.cnt[r]++ == 0) {
+            b.beg[r] = i;
+            b.nmax[r] = items[i].n;
+        }
+    }
+    return b;
+}
+
+// Launch the bins: the generic-kernel ranges on `s` one after another (from
+// the largest orders down; adjacent ranges with the same shape merge into one
+// launch), a small-kernel range 0 concurrently on the side stream; `s` waits
+// for both.  Stream operations only (capturable).  *nlaunch = kernels launched.
 template <class T>
-int launch_bins(const BatchItem *d_items, int nlarge, int nsmall, int nmax_large, T *A, T *B, int upper, int *info,
-                cudaStream_t s, BatchWs &ws, int mode) {
-    const int sms = ctx().num_sms;
-    const int nib = std::max(1, (std::max(nmax_large, 64) + IB - 1) / IB);
-    CHB_CUDA(cudaMemsetAsync(ws.cursor, 0, 2 * sizeof(int), s));
-    if (nsmall > 0 && mode >= 1) {
+int launch_bins(const BatchItem *d_items, const Bins &b, const int *mode, T *A, T *B, int upper, int *info,
+                cudaStream_t s, BatchWs &ws, int *nlaunch) {
+    *nlaunch = 0;
+    CHB_CUDA(cudaMemsetAsync(ws.cursor, 0, 8 * sizeof(int), s));
+    const bool side = b.cnt[0] > 0 && mode[0] >= 1 && mode[0] <= 3;
+    if (side) {
         CHB_CUDA(cudaEventRecord(ws.fork, s));
         CHB_CUDA(cudaStreamWaitEvent(ws.side, ws.fork, 0));
-        const int grid = std::min(sms * mode, nsmall);
-        posv_small_kernel<T><<<grid, NT_CTA, small_smem_bytes<T>(), ws.side>>>(d_items + nlarge, nsmall, A, B,
-                                                                                 upper, info, ws.cursor + 1);
-        CHB_LAUNCHED(1);
-        CHB_CUDA(cudaGetLastError());
+        if (int rc = launch_shape<T>(mode[0], d_items + b.beg[0], b.cnt[0], b.nmax[0], A, B, upper, info, ws.cursor + 6,
+                                     ws.side, ws))
+            return rc;
+        ++*nlaunch;
         CHB_CUDA(cudaEventRecord(ws.join, ws.side));
     }
-    // the generic kernel runs the large bin, and the small bin too when mode == 0
-    const int ngen = nlarge + ((mode == 0) ? nsmall : 0);
-    if (ngen > 0) {
-        const int grid = std::min(sms, ngen);
-        posv_batch_kernel<T><<<grid, NT_CTA, tile_smem_bytes<T>(), s>>>(d_items, ngen, A, B, upper, info, ws.cursor,
-                                                                      (T *)ws.scratch, nib);
-        CHB_LAUNCHED(1);
-        CHB_CUDA(cudaGetLastError());
+    int seg_shape = -1, seg_beg = 0, seg_cnt = 0, seg_nmax = 0, slot = 0;
+    auto flush = [&]() -> int {
+        if (seg_cnt == 0) return 0;
+        const int rc = launch_shape<T>(seg_shape, d_items + seg_beg, seg_cnt, seg_nmax, A, B, upper, info,
+                                       ws.cursor + slot++, s, ws);
+        ++*nlaunch;
+        seg_cnt = 0;
+        return rc;
+    };
+    for (int r = NRANGE - 1; r >= 0; --r) {
+        if (b.cnt[r] == 0 || (r == 0 && side)) continue;
+        if (seg_cnt > 0 && mode[r] == seg_shape) {
+            seg_cnt += b.cnt[r];
+            continue;
+        }
+        if (int rc = flush()) return rc;
+        seg_shape = mode[r];
+        seg_beg = b.beg[r];
+        seg_cnt = b.cnt[r];
+        seg_nmax = b.nmax[r];
     }
-    if (nsmall > 0 && mode >= 1) CHB_CUDA(cudaStreamWaitEvent(s, ws.join, 0));
+    if (int rc = flush()) return rc;
+    if (side) CHB_CUDA(cudaStreamWaitEvent(s, ws.join, 0));
     return 0;
 }
 
-// Host items -> bins (sorted largest first within each bin), device upload of
-// the item list to `d_items` (capacity checked by the caller).
-void make_bins(std::vector<BatchItem> &items, int *nlarge, int *nsmall, int *nmax_large) {
-    std::stable_sort(items.begin(), items.end(), [](const BatchItem &a, const BatchItem &b) { return a.n > b.n; });
-    int nl = 0;
-    while (nl < (int)items.size() && items[nl].n > 64) ++nl;
-    *nlarge = nl;
-    *nsmall = (int)items.size() - nl;
-    *nmax_large = nl ? items[0].n : 0;
-}
-
 template <class T>
-int prepare(BatchWs &ws, cudaStream_t s, size_t nitems, int nmax) {
+int prepare(BatchWs &ws, cudaStream_t s, size_t nitems, const Bins &b) {
     if (int rc = set_attrs()) return rc;
     if (!ws.side) {
         CHB_CUDA(cudaStreamCreateWithFlags(&ws.side, cudaStreamNonBlocking));
         CHB_CUDA(cudaEventCreateWithFlags(&ws.fork, cudaEventDisableTiming));
         CHB_CUDA(cudaEventCreateWithFlags(&ws.join, cudaEventDisableTiming));
     }
-    const int nib = std::max(1, (std::max(nmax, 64) + IB - 1) / IB);
-    if (int rc = bws_reserve(ws, nitems * sizeof(BatchItem), (size_t)ctx().num_sms * nib * IB * IB * sizeof(T), 1))
-        return rc;
-    return autotune_small<T>(s, ws);
+    for (int r = 0; r < NRANGE; ++r)
+        if (b.cnt[r] > 0)
+            if (int rc = autotune_range<T>(r, s, ws)) return rc;
+    return bws_reserve(ws, nitems * sizeof(BatchItem), scratch_bytes<T>(b.nmax_all), 1);
 }
 }  // namespace
 
@@ -391,12 +515,11 @@ template <class T>
 int launch_posv_batch_t(std::vector<BatchItem> &items, T *A, T *B, int upper, int *info, cudaStream_t s,
                         BatchWs &ws) {
     if (items.empty()) return 0;
-    int nl, ns, nmax;
-    make_bins(items, &nl, &ns, &nmax);
-    if (int rc = prepare<T>(ws, s, items.size(), nmax)) return rc;
+    const Bins b = make_bins(items);
+    if (int rc = prepare<T>(ws, s, items.size(), b)) return rc;
     CHB_CUDA(cudaMemcpyAsync(ws.items, items.data(), items.size() * sizeof(BatchItem), cudaMemcpyHostToDevice, s));
-    return launch_bins<T>((const BatchItem *)ws.items, nl, ns, nmax, A, B, upper, info, s, ws,
-                          g_tune[tidx<T>()].mode);
+    int nl = 0;
+    return launch_bins<T>((const BatchItem *)ws.items, b, g_tune[tidx<T>()].mode, A, B, upper, info, s, ws, &nl);
 }
 
 int launch_posv_batch(std::vector<BatchItem> &items, double *A, double *B, int upper, int *info, cudaStream_t s,
@@ -411,6 +534,7 @@ struct BatchGraph {
     uint64_t key = 0;
     cudaGraphExec_t exec = nullptr;
     BatchItem *d_items = nullptr;
+    int nlaunch = 0;   // kernels in the graph
 };
 std::list<BatchGraph> g_graphs;   // most recent first
 std::mutex g_graph_mu;
@@ -425,21 +549,21 @@ uint64_t fnv(uint64_t h, const void *p, size_t n) {
 template <class T>
 int posv_batch_graph(std::vector<BatchItem> &items, T *A, T *B, int upper, int *info, int count, cudaStream_t s) {
     BatchWs &ws = g_bws;
-    int nl, ns, nmax;
-    make_bins(items, &nl, &ns, &nmax);
-    if (int rc = prepare<T>(ws, s, items.size(), nmax)) return rc;
-    const int mode = g_tune[tidx<T>()].mode;
+    const Bins b = make_bins(items);
+    if (int rc = prepare<T>(ws, s, items.size(), b)) return rc;
+    const int *mode = g_tune[tidx<T>()].mode;
     uint64_t key = 1469598103934665603ull;
     key = fnv(key, items.data(), items.size() * sizeof(BatchItem));
     const void *ptrs[4] = {A, B, info, ws.scratch};
-    const int ints[5] = {upper, count, mode, (int)sizeof(T), (int)items.size()};
+    const int ints[4] = {upper, count, (int)sizeof(T), (int)items.size()};
     key = fnv(key, ptrs, sizeof ptrs);
     key = fnv(key, ints, sizeof ints);
+    key = fnv(key, mode, NRANGE * sizeof(int));
     std::lock_guard<std::mutex> lk(g_graph_mu);
     for (auto it = g_graphs.begin(); it != g_graphs.end(); ++it) {
         if (it->key != key) continue;
         g_graphs.splice(g_graphs.begin(), g_graphs, it);
-        CHB_LAUNCHED(ns > 0 && mode >= 1 ? 2 : 1);
+        CHB_LAUNCHED(g_graphs.front().nlaunch);
         CHB_CUDA(cudaGraphLaunch(g_graphs.front().exec, s));
         return 0;
     }
@@ -450,7 +574,7 @@ int posv_batch_graph(std::vector<BatchItem> &items, T *A, T *B, int upper, int *
     cudaGraph_t graph = nullptr;
     CHB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     if (info) cudaMemsetAsync(info, 0, count * sizeof(int), s);
-    const int rcl = launch_bins<T>(g.d_items, nl, ns, nmax, A, B, upper, info, s, ws, mode);
+    const int rcl = launch_bins<T>(g.d_items, b, mode, A, B, upper, info, s, ws, &g.nlaunch);
     const cudaError_t ec = cudaStreamEndCapture(s, &graph);
     if (rcl || ec != cudaSuccess) {
         if (graph) cudaGraphDestroy(graph);
@@ -609,11 +733,34 @@ int CHAM_B200_sposv_batch(cham_uplo_t uplo, int count, const int *n, const int *
 // Autotuner choice for the small bin (n <= 64) of element type `dtype`
 // (ChamRealDouble / ChamRealFloat): out[0] = mode (0: generic kernel, k: small
 // kernel at k CTAs per SM), out[1..4] = the timed ms of modes 0..3 (-1: not run).
+// Forces the shape of size range r for an element type (shape -1: tune again
+// at the next batch).  For tests and experiments; CHAMELEON_ERR_NOT_SUPPORTED
+// when the device cannot run the shape, or it does not apply to the range.
+int CHAM_B200_Batch_SetShape(int dtype, int range, int shape) {
+    if (range < 0 || range >= NRANGE || shape < -1 || shape >= NSHAPE) return CHAMELEON_ERR_ILLEGAL_VALUE;
+    if (int rc = ensure_init()) return rc;
+    if (int rc = set_attrs()) return rc;
+    const bool dbl = dtype != ChamRealFloat;
+    if (shape >= 0) {
+        if (range > 0 && shape >= 1 && shape <= 3) return CHAMELEON_ERR_NOT_SUPPORTED;
+        if (!(dbl ? shape_fits<double>(shape) : shape_fits<float>(shape))) return CHAMELEON_ERR_NOT_SUPPORTED;
+    }
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune[dbl ? 0 : 1].mode[range] = shape;
+    return 0;
+}
+
+// The batch autotuner's choices for an element type: out[r] = the shape of
+// size range r (4 ranges: n <= 64, 65..128, 129..256, 257+; -1 = not tuned
+// yet), out[4 + 6 r + k] = the milliseconds shape k took on range r's
+// synthetic batch (-1: not admissible).  28 doubles.
 int CHAM_B200_Batch_Tuning(int dtype, double *out) {
     if (!out) return CHAMELEON_ERR_ILLEGAL_VALUE;
-    const SmallTune &tu = g_tune[dtype == ChamRealFloat ? 1 : 0];
-    out[0] = tu.mode;
-    for (int m = 0; m < 4; ++m) out[1 + m] = tu.ms[m];
+    const BinTune &tu = g_tune[dtype == ChamRealFloat ? 1 : 0];
+    for (int r = 0; r < NRANGE; ++r) {
+        out[r] = tu.mode[r];
+        for (int k = 0; k < NSHAPE; ++k) out[NRANGE + NSHAPE * r + k] = tu.ms[r][k];
+    }
     return 0;
 }
 

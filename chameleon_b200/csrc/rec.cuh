@@ -125,8 +125,14 @@ __device__ __noinline__ int warp_chol32r(T *S) {
         const T r = rsqrt_wp(d);
         const T l = (lane == j) ? d * r : a[0] * r;
         if (lane >= j) S[lane + j * LDS] = l;
+        __syncwarp();
+        // column j of L, read back as broadcasts (one shared load per entry
+        // instead of two 32-bit shuffles for an FP64 value); the wrapped
+        // slots read stale entries above the diagonal, as the shuffles read
+        // the unused lanes, and are never read back
+        const T *col = S + j * LDS;
 #pragma unroll
-        for (int k = 1; k < 32; ++k) a[k - 1] = a[k] - l * __shfl_sync(FULL, l, (j + k) & 31);
+        for (int k = 1; k < 32; ++k) a[k - 1] = a[k] - l * col[(j + k) & 31];
         a[31] = T(0);
     }
     __syncwarp();
@@ -141,9 +147,11 @@ __device__ __noinline__ void warp_trinv32r(const T *S, T *Xs) {
     T x[32];
 #pragma unroll
     for (int k = 0; k < 32; ++k) x[k] = (k == lane) ? T(1) : T(0);
+    // the 32 diagonal reciprocals at once, off the step chain (lane i: 1 / L(i, i))
+    const T rdl = T(1) / S[lane + lane * LDS];
 #pragma unroll 1
     for (int i = 0; i < 32; ++i) {
-        const T xi = x[0] * (T(1) / S[i + i * LDS]);   // X(i, lane), final (zero above the diagonal)
+        const T xi = x[0] * __shfl_sync(FULL, rdl, i);   // X(i, lane), final (zero above the diagonal)
         Xs[i + lane * LDS] = xi;
 #pragma unroll
         for (int k = 1; k < 32; ++k) x[k - 1] = x[k] - S[((i + k) & 31) + i * LDS] * xi;
@@ -280,11 +288,20 @@ __device__ __noinline__ int leaf64(const ViewT<T> &A, const ViewT<T> &X, int n, 
 // contract as CORE_dpotrf (coreblas/compute/core_zpotrf.c:75-81).
 // ph (optional, tracing): thread 0 adds the clock cycles spent in the block-
 // column updates, the leaves and the panels to ph[0..2].
+// PR: rows of one panel step (128 or 64).  LEAN: the leaf's two 64 x 64
+// blocks share the GEMM staging area instead of following it (the leaf runs
+// between GEMMs), so that smem needs only lean_smem_elems() -- the footprint
+// that lets several CTAs share an SM.
 template <class T, int SP>
+constexpr size_t lean_smem_elems() {
+    return Cfg64<T, SP>::SMEM_ELEMS > 2 * IB * LDS ? Cfg64<T, SP>::SMEM_ELEMS : 2 * IB * LDS;
+}
+template <class T, int SP, int PR = 128, bool LEAN = false>
 __device__ int tile_potrf_blk(const ViewT<T> &Tv, int n, T *invd, T *smem, unsigned *ph = nullptr) {
-    using CP = Cfg12864<T, SP>;
+    static_assert(PR == 128 || PR == 64, "panel rows");
+    using CP = typename std::conditional<PR == 128, Cfg12864<T, SP>, Cfg64<T, SP>>::type;
     using CD = Cfg64<T, SP>;
-    T *sD = smem + CP::SMEM_ELEMS;
+    T *sD = LEAN ? smem : smem + CP::SMEM_ELEMS;   // cta_gemm ends with a barrier
     T *sX = sD + IB * LDS;
     long long c0 = (ph && threadIdx.x == 0) ? clock64() : 0;
     auto lap = [&](int i) {
@@ -315,8 +332,8 @@ __device__ int tile_potrf_blk(const ViewT<T> &Tv, int n, T *invd, T *smem, unsig
         }
         cta_sync();
         // panel below the inner diagonal block
-        for (int r0 = jb + nbk; r0 < n; r0 += 128) {
-            const int mr = min(128, n - r0);
+        for (int r0 = jb + nbk; r0 < n; r0 += PR) {
+            const int mr = min(PR, n - r0);
             Acc<CP> pa;
             if (jb > 0) {
                 pa.zero();

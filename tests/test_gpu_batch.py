@@ -170,10 +170,41 @@ def test_sposv_batch_fp32(cb, orc, uplo):
 
 
 def test_batch_autotuner_picked_the_fastest(cb, orc):
-    ns, rs, As, Bs = _uneven_batch(orc, 20, 16, 64, 2, 99)
-    _run_batch(cb, "CHAM_B200_dposv_batch", 122, ns, rs, As, Bs, np.float64)   # tunes on first use
-    out = (ctypes.c_double * 5)()
+    ns, rs, As, Bs = _uneven_batch(orc, 40, 16, 300, 2, 99)
+    _run_batch(cb, "CHAM_B200_dposv_batch", 122, ns, rs, As, Bs, np.float64)   # tunes the ranges on first use
+    out = (ctypes.c_double * 28)()
     assert cb.lib().CHAM_B200_Batch_Tuning(cb.ChamRealDouble, out) == 0
-    mode, times = int(out[0]), [t for t in out[1:] if t >= 0]
-    assert 0 <= mode <= 3 and len(times) >= 2
-    assert out[1 + mode] == min(times)
+    tuned = 0
+    for r in range(4):
+        mode = int(out[r])
+        times = [out[4 + 6 * r + k] for k in range(6)]
+        if mode < 0:
+            continue
+        tuned += 1
+        admissible = [t for t in times if t >= 0]
+        assert len(admissible) >= 2
+        assert times[mode] == min(admissible)
+        if r > 0:
+            assert mode in (0, 4, 5)
+    assert tuned >= 3                       # ranges 0..2 at least (n in 16..300)
+
+
+@pytest.mark.parametrize("r,lo,hi", [(0, 8, 64), (1, 65, 128), (2, 129, 256), (3, 257, 400)])
+def test_every_batch_shape_is_correct(cb, orc, r, lo, hi):
+    """Each kernel shape the tuner may pick for a size range, forced in turn."""
+    ns, rs, As, Bs = _uneven_batch(orc, 50, lo, hi, 9, 500 + r)
+    L = cb.lib()
+    try:
+        ran = 0
+        for shape in range(6):
+            if L.CHAM_B200_Batch_SetShape(cb.ChamRealDouble, r, shape) != 0:
+                continue
+            ran += 1
+            for uplo in (121, 122):
+                Xs, inf = _run_batch(cb, "CHAM_B200_dposv_batch", uplo, ns, rs, As, Bs, np.float64)
+                assert (inf == 0).all(), (shape, uplo)
+                for A, X, B in zip(As, Xs, Bs):
+                    assert _residual(A, X, B, 1.1102230246251565e-16) < 60, (shape, uplo)
+        assert ran >= 2
+    finally:
+        L.CHAM_B200_Batch_SetShape(cb.ChamRealDouble, r, -1)
