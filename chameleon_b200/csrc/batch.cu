@@ -104,7 +104,7 @@ __global__ void __launch_bounds__(NT_CTA, MINB)
         const int n = it.n;
         const ViewT<T> Lv = upper ? ViewT<T>{A + it.a_off, it.lda, 1} : ViewT<T>{A + it.a_off, 1, it.lda};
         rec::leaf64_load(Lv, n, sD);
-        const int r = rec::leaf64_core<T, true>(sD, sX);
+        const int r = rec::leaf64_core<T, true>(sD);
         if (tid == 0 && info) info[it.info_idx] = r;
         if (r != 0) continue;   // uniform across the CTA
         for (int idx = tid; idx < n * n; idx += NT_CTA) {

@@ -116,14 +116,17 @@ std::vector<Task> build_order(const Shape &s) {
     const double nb = s.NB;
     const Calib &cal = kCalib[(s.prof >= 0 && s.prof < 3) ? s.prof : 0];
     // tcgen05 path: task durations in microseconds from per-task device traces
-    // at NB = 256 and 512 (N = 32768).  The diagonal and panel tasks there are
+    // at NB = 256 and 512 (N = 32768; the diagonal factorization measured
+    // alone, 1.05 t: under the full load it runs ~20% longer, but the lower
+    // figure ordered the list best -- 1.25 t and 0.8 t both lengthened the
+    // launch by 5-8%).  The diagonal and panel tasks there are
     // latency-bound and grow linearly with the tile order, not with its flops,
     // so a flop model misorders the list (tasks whose inputs are not ready are
     // claimed first and their CTAs wait).
     const bool lat = (s.prof == PROF_F32_TC05);
-    auto c_potrf = [&](double t) { return lat ? 1.6 * t : cal.potrf * 6.0 * t * t * t / 3.0; };
+    auto c_potrf = [&](double t) { return lat ? 1.05 * t : cal.potrf * 6.0 * t * t * t / 3.0; };
     auto c_xinv = [&](double t) { return lat ? 1.5 * t : cal.potrf * 6.0 * t * t * t / 3.0; };
-    auto c_trsm = [&]() { return lat ? 0.34 * nb : cal.trsm * 2.0 * SUBB * nb * nb; };
+    auto c_trsm = [&]() { return lat ? 0.27 * nb : cal.trsm * 2.0 * SUBB * nb * nb; };
     auto c_upd = [&](int cnt) {
         return lat ? 5.0 + 0.011 * nb * cnt
                    : cal.upd * SUBB * SUBB * nb * 2.0 * (cnt + cal.upd_fix) / (1.0 + cal.upd_fix);

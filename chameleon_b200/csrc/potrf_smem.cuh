@@ -50,7 +50,8 @@ constexpr size_t SMEM_BYTES = (size_t)SMEM_FLOATS * sizeof(float);
 // into sD (64 x LDI) for the warp-level 64 x 64 leaf of rec.cuh (32 x 32
 // Cholesky and inverse kernels in rolled form).  Returns LAPACK info.  All 256
 // threads; ends with a barrier.
-static __device__ __noinline__ int leaf(float *D, int ldd, int nbk, float *sD, float *Xs) {
+static __device__ __noinline__ int leaf(float *D, int ldd, int nbk, float *sD) {
+    float *Xs = sD + BW * LDI;   // the leaf's inverse follows the staged block
     for (int idx = threadIdx.x; idx < 64 * 64; idx += NT_CTA) {
         const int r = idx & 63, c = idx >> 6;
         float v = (r == c) ? 1.f : 0.f;
@@ -58,7 +59,7 @@ static __device__ __noinline__ int leaf(float *D, int ldd, int nbk, float *sD, f
         sD[c * LDI + r] = v;
     }
     __syncthreads();
-    const int info = rec::leaf64_core<float, true>(sD, Xs);
+    const int info = rec::leaf64_core<float, true>(sD);
     if (info) return info;
     for (int idx = threadIdx.x; idx < 64 * 64; idx += NT_CTA) {
         const int r = idx & 63, c = idx >> 6;
@@ -113,7 +114,8 @@ static __device__ __forceinline__ void gemm64(Frag &acc, const float *Xm, int ld
 static __device__ int potrf(const ViewF &T, int n, float *invd, float *sm, unsigned *ph = nullptr) {
     const int tid = threadIdx.x;
     const int nb = (n + BW - 1) / BW;
-    float *Xs = sm + blk_off(n, nb);
+    float *sDl = sm + blk_off(n, nb);   // staged leaf block, then its inverse
+    float *Xs = sDl + BW * LDI;
     // tracing (ph != null): thread 0 adds the clock cycles of the leaves, the
     // panel products and the trailing updates (with the load and the
     // write-back) to ph[0..2]
@@ -171,7 +173,7 @@ static __device__ int potrf(const ViewF &T, int n, float *invd, float *sm, unsig
     for (int b = 0; b < nb; ++b) {
         float *Sb = sm + blk_off(n, b);
         const int ldb = blk_ld(n, b), nbk = min(BW, n - BW * b);
-        const int linfo = leaf(Sb, ldb, nbk, Xs + BW * LDI, Xs);
+        const int linfo = leaf(Sb, ldb, nbk, sDl);
         lap(0);
         if (linfo) {
             info = BW * b + linfo;

@@ -109,38 +109,56 @@ __device__ __noinline__ void warp_trinv32(const T *S, T *Xs) {
 // slot k writes slot k - 1, so slot 0 is always the current column (row) and
 // the shift costs no moves.
 template <class T>
-__device__ __noinline__ int warp_chol32r(T *S) {
+__device__ __noinline__ int warp_chol32r(T *S, T *bc) {
     const int lane = threadIdx.x & 31;
     T a[32];   // a[k]: entry (lane, j + k)
 #pragma unroll
     for (int c = 0; c < 32; ++c) a[c] = (c <= lane) ? S[lane + c * LDS] : T(0);
     int info = 0;
+    // pivot and reciprocal square root of step 0; every step computes those of
+    // the next one right after the entry that holds it, so that the shuffle
+    // and the square root overlap the rest of the update
+    T d = __shfl_sync(FULL, a[0], 0);
+    if (!(d > T(0))) {   // also catches NaN
+        info = 1;
+        d = T(1);
+    }
+    T r = rsqrt_wp(d);
 #pragma unroll 1
     for (int j = 0; j < 32; ++j) {
-        T d = __shfl_sync(FULL, a[0], j);
-        if (!(d > T(0))) {   // also catches NaN
-            if (info == 0) info = j + 1;
-            d = T(1);
-        }
-        const T r = rsqrt_wp(d);
         const T l = (lane == j) ? d * r : a[0] * r;
         if (lane >= j) S[lane + j * LDS] = l;
+        // column j broadcast through bc (two buffers of 64 entries, by step
+        // parity): buf[m] = l of lane m & 31, so that slot k reads buf[j + k]
+        // at a fixed offset (one shared load per entry, no lane arithmetic);
+        // the wrapped slots read the unused lanes' values, as shuffles would,
+        // and are never read back
+        T *buf = bc + ((j & 1) << 6);
+        buf[lane] = l;
+        buf[lane + 32] = l;
         __syncwarp();
-        // column j of L, read back as broadcasts (one shared load per entry
-        // instead of two 32-bit shuffles for an FP64 value); the wrapped
-        // slots read stale entries above the diagonal, as the shuffles read
-        // the unused lanes, and are never read back
-        const T *col = S + j * LDS;
+        const T *col = buf + j;
+        a[0] = a[1] - l * col[1];
+        T dn = __shfl_sync(FULL, a[0], (j + 1) & 31);
 #pragma unroll
-        for (int k = 1; k < 32; ++k) a[k - 1] = a[k] - l * col[(j + k) & 31];
+        for (int k = 2; k < 32; ++k) a[k - 1] = a[k] - l * col[k];
         a[31] = T(0);
+        if (!(dn > T(0))) {
+            if (info == 0 && j + 1 < 32) info = j + 2;
+            dn = T(1);
+        }
+        d = dn;
+        r = rsqrt_wp(dn);
     }
     __syncwarp();
     return info;
 }
 
 // X = L^-1 for the 32 x 32 lower block at S, lane c = column c of X, slot k =
-// row i + k at step i (the entries of columns of L are broadcast loads).
+// row i + k at step i (the entries of columns of L are broadcast loads at
+// fixed offsets from S(i, i): rows i + 1 .. i + 31, so up to 31 entries past
+// row 31 of column i -- the wrapped slots, never read back; the caller keeps
+// that range inside its shared memory: leaf64_core's sX follows sD).
 template <class T>
 __device__ __noinline__ void warp_trinv32r(const T *S, T *Xs) {
     const int lane = threadIdx.x & 31;
@@ -153,8 +171,9 @@ __device__ __noinline__ void warp_trinv32r(const T *S, T *Xs) {
     for (int i = 0; i < 32; ++i) {
         const T xi = x[0] * __shfl_sync(FULL, rdl, i);   // X(i, lane), final (zero above the diagonal)
         Xs[i + lane * LDS] = xi;
+        const T *col = S + i * (LDS + 1);                 // S(i, i)
 #pragma unroll
-        for (int k = 1; k < 32; ++k) x[k - 1] = x[k] - S[((i + k) & 31) + i * LDS] * xi;
+        for (int k = 1; k < 32; ++k) x[k - 1] = x[k] - col[k] * xi;
         x[31] = T(0);
     }
     __syncwarp();
@@ -181,18 +200,20 @@ __device__ __forceinline__ void small_mm32(const T *P, const T *Q, T (&o)[4]) {
 
 // 64 x 64 leaf on shared memory.  sD (ld LDS) holds the block, lower
 // triangle, identity-padded beyond the matrix and zero above the diagonal.
-// FACT: sD is factored in place (L), else it already holds L.  sX (ld LDS)
-// receives the full inverse (zeros above the diagonal).  Returns LAPACK info.
-// Called by all threads; ends with a barrier.
+// FACT: sD is factored in place (L), else it already holds L.  sX = sD + 64
+// LDS (ld LDS) receives the full inverse (zeros above the diagonal); the
+// inverse kernel's column reads run up to 29 entries past the end of sD, into
+// sX.  Returns LAPACK info.  Called by all threads; ends with a barrier.
 template <class T, bool FACT>
-__device__ __noinline__ int leaf64_core(T *sD, T *sX) {
+__device__ __noinline__ int leaf64_core(T *sD) {
+    T *sX = sD + 64 * LDS;
     __shared__ int s_info;
     const int tid = threadIdx.x, warp = tid >> 5;
     if (tid == 0) s_info = 0;
     __syncthreads();
     if (FACT) {
         if (warp == 0) {
-            const int info = warp_chol32r(sD);
+            const int info = warp_chol32r(sD, sX);   // sX (2 columns) is free until the inverse
             if (tid == 0) s_info = info;
         }
         __syncthreads();
@@ -218,7 +239,8 @@ __device__ __noinline__ int leaf64_core(T *sD, T *sX) {
         }
         __syncthreads();
         if (warp == 0) {
-            const int info = warp_chol32r(sD + 32 + 32 * LDS);
+            // the columns 32, 33 of sX are free until X22 and W are written
+            const int info = warp_chol32r(sD + 32 + 32 * LDS, sX + 32 * LDS);
             if (tid == 0) s_info = info ? 32 + info : 0;
         }
         __syncthreads();
@@ -268,7 +290,7 @@ __device__ __noinline__ int leaf64(const ViewT<T> &A, const ViewT<T> &X, int n, 
     T *sD = smem;              // 64 x LDS
     T *sX = smem + 64 * LDS;   // 64 x LDS
     leaf64_load(A, n, sD);
-    const int info = leaf64_core<T, FACT>(sD, sX);
+    const int info = leaf64_core<T, FACT>(sD);
     if (info) return info;
     for (int idx = threadIdx.x; idx < n * n; idx += NT_CTA) {
         const int r = idx % n, c = idx / n;
@@ -321,7 +343,7 @@ __device__ int tile_potrf_blk(const ViewT<T> &Tv, int n, T *invd, T *smem, unsig
             if (r < nbk && c < nbk && r >= c) sD[r + c * LDS] -= v;
         });
         lap(0);
-        const int info = leaf64_core<T, true>(sD, sX);
+        const int info = leaf64_core<T, true>(sD);
         lap(1);
         if (info) return jb + info;
         T *inv = invd + (int64_t)(jb / IB) * IB * IB;
@@ -361,7 +383,7 @@ __device__ void tile_inv_blk(const ViewT<T> &Tv, int n, T *invd, T *smem) {
     for (int jb = 0; jb < n; jb += IB) {
         const int nbk = min(IB, n - jb);
         leaf64_load(Tv.sub(jb, jb), nbk, sD);
-        leaf64_core<T, false>(sD, sX);
+        leaf64_core<T, false>(sD);
         T *inv = invd + (int64_t)(jb / IB) * IB * IB;
         for (int idx = threadIdx.x; idx < IB * IB; idx += NT_CTA) {
             const int r = idx % IB, c = idx / IB;
