@@ -152,6 +152,8 @@ PROTOS = {
     "CHAM_B200_Dispatch_Cost": (ctypes.c_double, [_i, _i]),
     "CHAM_B200_Dispatch_Bytes": (ctypes.c_double, [_i, _i]),
     "CHAM_B200_Dispatch_Plan": (_i, [_i, _vp, _vp, _vp, _i, _vp, _vp, _vp, _vp, _vp]),
+    "CHAMELEON_dgemm_batch_Tile": (_i, [_i, _i, ctypes.c_double, _D, _D, ctypes.c_double, _D]),
+    "CHAMELEON_dsyrk_batch_Tile": (_i, [_i, _i, ctypes.c_double, _D, ctypes.c_double, _D]),
     "CHAMELEON_dtrtri": (_i, [_i, _i, _i, _vp, _i]),
     "CHAMELEON_dlauum": (_i, [_i, _i, _vp, _i]),
     "CHAMELEON_dpotri": (_i, [_i, _i, _vp, _i]),

@@ -201,6 +201,14 @@ int CHAMELEON_dpotrf_batch_Tile(cham_uplo_t uplo, CHAM_desc_t *A);
 /* compute/ztrsm_batch.c:180 -- tile (m,n) of B solved with tile (m,n) of A */
 int CHAMELEON_dtrsm_batch_Tile(cham_side_t side, cham_uplo_t uplo, cham_trans_t trans,
                                cham_diag_t diag, double alpha, CHAM_desc_t *A, CHAM_desc_t *B);
+/* compute/zgemm_batch.c:193 / zherk_batch.c:176 (zherk -> dsyrk): one
+ * independent product per tile (m, n) of C: gemm C(m,n) <- alpha op(A(m,n))
+ * op(B(m,n)) + beta C(m,n); syrk C(m,n) <- alpha op(A(m,n)) op(A(m,n))^T +
+ * beta C(m,n) on the uplo triangle of the tile.  C is not read when beta == 0. */
+int CHAMELEON_dgemm_batch_Tile(cham_trans_t transA, cham_trans_t transB, double alpha, CHAM_desc_t *A,
+                               CHAM_desc_t *B, double beta, CHAM_desc_t *C);
+int CHAMELEON_dsyrk_batch_Tile(cham_uplo_t uplo, cham_trans_t trans, double alpha, CHAM_desc_t *A, double beta,
+                               CHAM_desc_t *C);
 /* Generators: compute/zplgsy.c:276 (pzplgsy.c:29-80), compute/zplrnt.c (pzplrnt.c) */
 int CHAMELEON_dplgsy(double bump, cham_uplo_t uplo, int N, double *A, int LDA,
                      unsigned long long int seed);

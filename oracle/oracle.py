@@ -117,6 +117,10 @@ def reference(ncores=0):
                                           ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp, _dp]
         L.chamref_lapacke_dsposv.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp, ctypes.c_int, _dp,
                                              ctypes.c_int, _dp, ctypes.c_int, _ip, _dp]
+        L.chamref_dgemm_batch.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double] + \
+            [ctypes.c_int] * 7 + [_dp, _dp, _dp]
+        L.chamref_dsyrk_batch.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double] + \
+            [ctypes.c_int] * 4 + [_dp, _dp]
         L.chamref_dinverse.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp,
                                        ctypes.c_int]
         L.chamref_init(ncores if ncores > 0 else (os.cpu_count() or 1))
@@ -200,3 +204,38 @@ def ref_dinverse(op, uplo, A, NB, diag=131):
     N = X.shape[0]
     info = L.chamref_dinverse({"potri": 0, "trtri": 1, "lauum": 2}[op], uplo, diag, N, NB, _ptr(X), max(N, 1))
     return X, info
+
+
+def _stack(X):
+    """count x r x c per-tile matrices -> the column-major (count r) x c matrix
+    whose tile row i is X[i] (the stacked descriptor the harness builds)."""
+    return np.asfortranarray(np.concatenate(list(X), axis=0))
+
+
+def _unstack(M, cnt):
+    r = M.shape[0] // cnt
+    return np.stack([M[i * r:(i + 1) * r] for i in range(cnt)])
+
+
+def ref_dgemm_batch(transA, transB, alpha, A, B, beta, C):
+    """Reference CHAMELEON_dgemm_batch_Tile on stacked tiles: A (count, am, an),
+    B (count, bm, bn), C (count, m, n) arrays of per-tile matrices; returns C'."""
+    L = reference()
+    cnt, am, an = A.shape
+    _, bm, bn = B.shape
+    _, m, n = C.shape
+    a, b, c = _stack(A), _stack(B), _stack(C)
+    rc = L.chamref_dgemm_batch(transA, transB, alpha, beta, am, an, bm, bn, m, n, cnt, _ptr(a), _ptr(b), _ptr(c))
+    assert rc == 0, rc
+    return _unstack(c, cnt)
+
+
+def ref_dsyrk_batch(uplo, trans, alpha, A, beta, C):
+    """Reference CHAMELEON_dsyrk_batch_Tile (zherk_batch.c after z->d) on stacked tiles."""
+    L = reference()
+    cnt, am, an = A.shape
+    n = C.shape[1]
+    a, c = _stack(A), _stack(C)
+    rc = L.chamref_dsyrk_batch(uplo, trans, alpha, beta, am, an, n, cnt, _ptr(a), _ptr(c))
+    assert rc == 0, rc
+    return _unstack(c, cnt)

@@ -211,6 +211,43 @@ int chamref_dtrsm_batch(int side, int uplo, int trans, int diag, double alpha,
     return rc;
 }
 
+/* CHAMELEON_dgemm_batch_Tile / dsyrk_batch_Tile (compute/zgemm_batch.c:193,
+ * zherk_batch.c:176): `count` tiles stacked in one tile column of a
+ * column-major (count am) x an array (likewise B: bm x bn, C: m x n tiles). */
+int chamref_dgemm_batch(int transA, int transB, double alpha, double beta, int am, int an, int bm, int bn,
+                        int m, int n, int count, double *A, double *B, double *C)
+{
+    CHAM_desc_t *dA = NULL, *dB = NULL, *dC = NULL;
+    int rc = CHAMELEON_Desc_Create(&dA, A, ChamRealDouble, am, an, am * an, count * am, an, 0, 0, count * am, an, 1, 1);
+    if (!rc) rc = CHAMELEON_Desc_Create(&dB, B, ChamRealDouble, bm, bn, bm * bn, count * bm, bn, 0, 0, count * bm, bn, 1, 1);
+    if (!rc) rc = CHAMELEON_Desc_Create(&dC, C, ChamRealDouble, m, n, m * n, count * m, n, 0, 0, count * m, n, 1, 1);
+    if (!rc) {
+#pragma omp parallel
+#pragma omp master
+        rc = CHAMELEON_dgemm_batch_Tile((cham_trans_t)transA, (cham_trans_t)transB, alpha, dA, dB, beta, dC);
+    }
+    if (dA) CHAMELEON_Desc_Destroy(&dA);
+    if (dB) CHAMELEON_Desc_Destroy(&dB);
+    if (dC) CHAMELEON_Desc_Destroy(&dC);
+    return rc;
+}
+
+int chamref_dsyrk_batch(int uplo, int trans, double alpha, double beta, int am, int an, int n, int count,
+                        double *A, double *C)
+{
+    CHAM_desc_t *dA = NULL, *dC = NULL;
+    int rc = CHAMELEON_Desc_Create(&dA, A, ChamRealDouble, am, an, am * an, count * am, an, 0, 0, count * am, an, 1, 1);
+    if (!rc) rc = CHAMELEON_Desc_Create(&dC, C, ChamRealDouble, n, n, n * n, count * n, n, 0, 0, count * n, n, 1, 1);
+    if (!rc) {
+#pragma omp parallel
+#pragma omp master
+        rc = CHAMELEON_dsyrk_batch_Tile((cham_uplo_t)uplo, (cham_trans_t)trans, alpha, dA, beta, dC);
+    }
+    if (dA) CHAMELEON_Desc_Destroy(&dA);
+    if (dC) CHAMELEON_Desc_Destroy(&dC);
+    return rc;
+}
+
 /* LAPACKE_dsposv from the same OpenBLAS: the CPU mixed-precision comparator. */
 extern int scipy_LAPACKE_dsposv(int layout, char uplo, int n, int nrhs, double *a, int lda,
                                 double *b, int ldb, double *x, int ldx, int *iter);

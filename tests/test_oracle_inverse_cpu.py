@@ -32,3 +32,16 @@ def test_reference_potri_trtri_lauum_vs_numpy(ref, uplo):
     assert info == 0
     P = F.T @ F if uplo == 122 else F @ F.T
     assert np.abs(tri(Pr) - tri(P)).max() <= 4 * N * EPS * np.abs(P).max()
+
+
+def test_reference_gemm_syrk_batch_vs_numpy(ref):
+    rng = np.random.default_rng(1)
+    A, B, C = rng.standard_normal((3, 20, 30)), rng.standard_normal((3, 30, 25)), rng.standard_normal((3, 20, 25))
+    out = ref.ref_dgemm_batch(111, 111, 1.5, A, B, -0.5, C)
+    assert np.abs(out - (1.5 * A @ B - 0.5 * C)).max() < 1e-12
+    S = rng.standard_normal((3, 20, 20))
+    out = ref.ref_dsyrk_batch(122, 111, 2.0, A, 1.0, S)
+    exp = 2.0 * A @ np.swapaxes(A, 1, 2) + S
+    for i in range(3):
+        assert np.abs(np.tril(out[i]) - np.tril(exp[i])).max() < 1e-12
+        assert np.array_equal(np.triu(out[i], 1), np.triu(S[i], 1))
