@@ -154,6 +154,9 @@ PROTOS = {
     "CHAM_B200_Dispatch_Plan": (_i, [_i, _vp, _vp, _vp, _i, _vp, _vp, _vp, _vp, _vp]),
     "CHAMELEON_dgemm_batch_Tile": (_i, [_i, _i, ctypes.c_double, _D, _D, ctypes.c_double, _D]),
     "CHAMELEON_dsyrk_batch_Tile": (_i, [_i, _i, ctypes.c_double, _D, ctypes.c_double, _D]),
+    "CHAMELEON_dgered_Tile": (_i, [_i, ctypes.c_double, _D]),
+    "CHAMELEON_dgerst_Tile": (_i, [_i, _D]),
+    "CHAM_B200_Tile_Precision": (_i, [_D, _i, _i]),
     "CHAMELEON_dtrtri": (_i, [_i, _i, _i, _vp, _i]),
     "CHAMELEON_dlauum": (_i, [_i, _i, _vp, _i]),
     "CHAMELEON_dpotri": (_i, [_i, _i, _vp, _i]),

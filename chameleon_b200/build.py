@@ -15,7 +15,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libchameleon_b200.so")
 
-SOURCES = ["control.cu", "executor.cu", "exec_f64.cu", "exec_f32.cu", "exec_f32tc.cu", "exec_tf32.cu", "tile_abi.cu", "mixed.cu", "batch.cu", "tc05.cu", "noalloc.cu", "serve.cu", "inverse.cu", "dispatch.cu", "batch_blas.cu"]
+SOURCES = ["control.cu", "executor.cu", "exec_f64.cu", "exec_f32.cu", "exec_f32tc.cu", "exec_tf32.cu", "tile_abi.cu", "mixed.cu", "batch.cu", "tc05.cu", "noalloc.cu", "serve.cu", "inverse.cu", "dispatch.cu", "batch_blas.cu", "gered.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

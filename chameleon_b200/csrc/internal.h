@@ -84,6 +84,7 @@ struct DescDev {
 struct DescPriv {
     DescDev dev;
     int cm_view = 0;          // 1: column-major user array view (LAPACK-layout entry points)
+    std::vector<signed char> prec;   // per tile (m + mt n): 0 FP64, 1 FP32, 2 FP16 values (gered.cu)
 };
 DescPriv *priv(const CHAM_desc_t *d);
 int desc_tile_rows(const CHAM_desc_t *d, int m);

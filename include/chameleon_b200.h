@@ -209,6 +209,16 @@ int CHAMELEON_dgemm_batch_Tile(cham_trans_t transA, cham_trans_t transB, double 
                                CHAM_desc_t *B, double beta, CHAM_desc_t *C);
 int CHAMELEON_dsyrk_batch_Tile(cham_uplo_t uplo, cham_trans_t trans, double alpha, CHAM_desc_t *A, double beta,
                                CHAM_desc_t *C);
+/* compute/zgered.c / pzgered.c:160-260 and pzgerst.c (z -> d): adaptive per-
+ * tile precision.  gered rounds each tile of the uplo triangle whose
+ * Frobenius norm is small against the matrix's (threshold eps ||A||_F /
+ * min(MT, NT), eps = prec or the FP64 unit roundoff when prec < 0) to FP16 or
+ * FP32 values and tags it; gerst resets the tags to FP64.  The descriptor
+ * keeps its FP64 storage (the reference changes the tile's storage type). */
+int CHAMELEON_dgered_Tile(cham_uplo_t uplo, double prec, CHAM_desc_t *A);
+int CHAMELEON_dgerst_Tile(cham_uplo_t uplo, CHAM_desc_t *A);
+/* The precision tag of tile (m, n): ChamRealDouble, ChamRealFloat or ChamRealHalf. */
+int CHAM_B200_Tile_Precision(const CHAM_desc_t *A, int m, int n);
 /* Generators: compute/zplgsy.c:276 (pzplgsy.c:29-80), compute/zplrnt.c (pzplrnt.c) */
 int CHAMELEON_dplgsy(double bump, cham_uplo_t uplo, int N, double *A, int LDA,
                      unsigned long long int seed);

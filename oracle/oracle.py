@@ -239,3 +239,40 @@ def ref_dsyrk_batch(uplo, trans, alpha, A, beta, C):
     rc = L.chamref_dsyrk_batch(uplo, trans, alpha, beta, am, an, n, cnt, _ptr(a), _ptr(c))
     assert rc == 0, rc
     return _unstack(c, cnt)
+
+
+def gered(uplo, prec, A, mb):
+    """Restatement of chameleon_pzgered (compute/pzgered.c:160-260) with the
+    conversion rule of INSERT_TASK_zgered in a CUDA double-precision build
+    (runtime/starpu/codelets/codelet_zgered.c): returns (A with the reduced
+    tiles rounded, tags[mt, nt] with 0 FP64 / 1 FP32 / 2 FP16)."""
+    A = np.array(A, dtype=np.float64, order="F")
+    N = A.shape[0]
+    mt = (N + mb - 1) // mb
+    lower, upper = uplo == 122, uplo == 121
+    tiles = []
+    for m in range(mt):
+        nmin = m if upper else 0
+        nmax = min(m + 1, mt) if lower else mt
+        for n in range(nmin, nmax):
+            sl = np.s_[m * mb:min(N, (m + 1) * mb), n * mb:min(N, (n + 1) * mb)]
+            T = A[sl]
+            if m == n and (lower or upper):
+                T = np.tril(T) if lower else np.triu(T)
+            tiles.append((m, n, sl, float(np.sqrt((T * T).sum()))))
+    gnorm = float(np.sqrt(sum(t[3] ** 2 for t in tiles)))
+    eps = 2.0 ** -53 if prec < 0 else prec
+    eps_diag = 2.0 ** -24
+    thr = eps * gnorm / mt
+    thr_diag = thr if eps < eps_diag else eps_diag * gnorm / mt
+    tags = np.zeros((mt, mt), dtype=np.int8)
+    for m, n, sl, ln in tiles:
+        th = thr_diag if m == n else thr
+        if ln < th / 1e-4:
+            tags[m, n] = 2
+            with np.errstate(over="ignore"):
+                A[sl] = A[sl].astype(np.float16).astype(np.float64)
+        elif ln < th / eps_diag:
+            tags[m, n] = 1
+            A[sl] = A[sl].astype(np.float32).astype(np.float64)
+    return A, tags

@@ -83,3 +83,27 @@ def test_live_reference_agrees_when_built(orc):
         assert orc.check_solve(A, X, B) < 60.0
         Xp = orc.dpotrs_tiled(uplo, orc.dpotrf_tiled(uplo, A, NB)[0], B, NB)
         assert np.abs(Xp - X).max() < 1e-13
+
+
+def test_gered_restatement_rule():
+    """The oracle's gered (compute/pzgered.c:160-260 with the CUDA rule of
+    codelet_zgered.c): a hand-checked 2 x 2 tile case."""
+    from oracle import oracle as o
+    mb = 4
+    A = np.zeros((8, 8))
+    A[:4, :4] = 10 * np.eye(4)            # diagonal tiles: ||.||_F = 20 each
+    A[4:, 4:] = 10 * np.eye(4)
+    A[4:, :4] = 1e-3                      # off-diagonal tile: ||.||_F = 4e-3
+    A[:4, 4:] = 1e-3
+    # lower: gnorm = sqrt(20^2 + 20^2 + 4e-3^2) ~ 28.28; prec 1e-6 -> threshold
+    # 1e-6 * 28.28 / 2 = 1.41e-5: 4e-3 < 1.41e-5 / 1e-4 = 0.141 -> FP16
+    R, tags = o.gered(122, 1e-6, A, mb)
+    assert tags.tolist() == [[0, 0], [2, 0]]
+    assert np.array_equal(R[4:, :4], np.float64(np.float16(1e-3)) * np.ones((4, 4)))
+    assert np.array_equal(R[:4, 4:], A[:4, 4:])            # outside the triangle: untouched
+    # prec 1e-9: threshold 1.41e-8; FP16 needs < 1.41e-4, FP32 < 1.41e-8 / 2^-24 = 0.237 -> FP32
+    R, tags = o.gered(122, 1e-9, A, mb)
+    assert tags.tolist() == [[0, 0], [1, 0]]
+    # the diagonal tiles use the FP32 unit roundoff once prec exceeds it
+    R, tags = o.gered(122, 1e-2, A, mb)
+    assert tags[0, 0] == 0 and tags[1, 1] == 0
