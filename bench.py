@@ -616,6 +616,24 @@ def serve_section(args, cb, rank):
 # ---------------------------------------------------------------------------
 # B200 arm
 # ---------------------------------------------------------------------------
+TRAFFIC_PROFILE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "profiles",
+                               "cholesky_dag_f32_bf16x3_tcgen05_launch_traffic.md")
+
+
+def traffic_capture():
+    """(n0, bytes per launch, file) from the profile summary's key lines
+    `order: <n0>` and `dram_bytes_per_launch: <bytes>`, or None."""
+    try:
+        kv = {}
+        for line in open(TRAFFIC_PROFILE):
+            if ":" in line and line.split(":", 1)[0].strip() in ("order", "dram_bytes_per_launch"):
+                k, v = line.split(":", 1)
+                kv[k.strip()] = float(v.split()[0])
+        return int(kv["order"]), kv["dram_bytes_per_launch"], os.path.basename(TRAFFIC_PROFILE)
+    except (OSError, KeyError, ValueError, IndexError):
+        return None
+
+
 def b200_arm(args, world, rank, local):
     import torch
     import chameleon_b200 as cb
@@ -675,17 +693,18 @@ def b200_arm(args, world, rank, local):
     else:
         peak, peak_src = pk.get("fp64_tflops"), "fp64"
     achieved = mult * fact_flops / (fact_ms * 1e-3) / 1e12 if fact_ms > 0 else None
-    # DRAM bytes of the factor+solve launch from 1-pass ncu captures of the whole
-    # launch (dram__bytes_read.sum + dram__bytes_write.sum: 89.95 GB + 26.10 GB
-    # at N = 32768, 1.52 GB at N = 8192); other sizes scale the nearer capture
-    # by the update work (N/N0)^3, the traffic being dominated by the trailing
-    # updates
+    # DRAM bytes of the factor+solve launch: read from the committed summary of
+    # a one-kernel ncu capture (dram__bytes_read.sum + dram__bytes_write.sum of
+    # the launch at a smaller order n0), scaled to N by (N/n0)^3 -- the traffic
+    # is dominated by the trailing updates' operand and C traffic
     traffic, traffic_src = None, None
     if args.precision == "bf16x3":
-        n0, b0 = (32768, 1.1605e11) if N >= 16384 else (8192, 1.5234e9)
-        traffic = b0 * (N / float(n0)) ** 3
-        traffic_src = "ncu dram__bytes_read.sum + dram__bytes_write.sum of the launch at N=%d%s" % (
-            n0, "" if N == n0 else " scaled by (N/%d)^3" % n0)
+        cap = traffic_capture()
+        if cap:
+            n0, b0, fname = cap
+            traffic = b0 * (N / float(n0)) ** 3
+            traffic_src = "ncu dram__bytes_read.sum + dram__bytes_write.sum of the launch at N=%d (%s)%s" % (
+                n0, fname, "" if N == n0 else ", scaled by (N/%d)^3" % n0)
     roofline = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                 "frac": (achieved / peak) if (achieved and peak) else None, "traffic": traffic,
                 "traffic_source": traffic_src,

@@ -161,6 +161,8 @@ PROTOS = {
     "CHAMELEON_dlauum": (_i, [_i, _i, _vp, _i]),
     "CHAMELEON_dpotri": (_i, [_i, _i, _vp, _i]),
     "CHAMELEON_dtrtri_Tile": (_i, [_i, _i, _D]),
+    "CHAMELEON_dpotrimm": (_i, [_i, _i, _vp, _i, _vp, _i, _vp, _i]),
+    "CHAMELEON_dpotrimm_Tile": (_i, [_i, _D, _D, _D]),
     "CHAMELEON_dlauum_Tile": (_i, [_i, _D]),
     "CHAMELEON_dpotri_Tile": (_i, [_i, _D]),
     "CHAMELEON_lapacke_dposv": (_i, [_i, ctypes.c_char, _i, _i, _vp, _i, _vp, _i]),

@@ -67,8 +67,8 @@ cublasHandle_t lib_handle() {
     return h;
 }
 
-double *g_w1 = nullptr, *g_w2 = nullptr;
-size_t g_w1_bytes = 0, g_w2_bytes = 0;
+double *g_w1 = nullptr, *g_w2 = nullptr, *g_w3 = nullptr, *g_w4 = nullptr;
+size_t g_w1_bytes = 0, g_w2_bytes = 0, g_w3_bytes = 0, g_w4_bytes = 0;
 int *g_flag = nullptr;
 
 double *work(double **buf, size_t *cap, size_t bytes) {
@@ -138,6 +138,38 @@ int lauum_dev(cham_uplo_t uplo, int N, double *A, int lda) {
 int potri_dev(cham_uplo_t uplo, int N, double *A, int lda) {
     if (int rc = trtri_dev(uplo, ChamNonUnit, N, A, lda)) return rc;
     return lauum_dev(uplo, N, A, lda);
+}
+
+// S (N x N, ld N) <- the symmetric matrix whose uplo triangle is in A.
+__global__ void sym_full_kernel(const double *A, int64_t lda, double *S, int N, int upper) {
+    const int64_t total = (int64_t)N * N;
+    for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
+         idx += (int64_t)gridDim.x * blockDim.x) {
+        const int i = (int)(idx % N), j = (int)(idx / N);
+        const bool in = upper ? i <= j : i >= j;
+        S[i + (int64_t)j * N] = in ? A[i + (int64_t)j * lda] : A[j + (int64_t)i * lda];
+    }
+}
+
+// compute/pzpotrimm.c: A <- A^-1 (uplo triangle; A is the SPD matrix on
+// entry: potrf, trtri, lauum), then C = B A^-1 (the symm of its last loop
+// nest, alpha = 1, beta = 0).  Device arrays.
+int potrimm_dev(cham_uplo_t uplo, int N, double *A, int lda, const double *B, int ldb, double *C, int ldc) {
+    int rc = CHAMELEON_dpotrf(uplo, N, A, lda);
+    if (rc) return rc;
+    if ((rc = potri_dev(uplo, N, A, lda))) return rc;
+    cudaStream_t s = ctx().stream;
+    cublasHandle_t h = lib_handle();
+    if (!h) return CHAMELEON_ERR_UNEXPECTED;
+    double *S = work(&g_w1, &g_w1_bytes, (size_t)N * N * sizeof(double));
+    if (!S) return CHAMELEON_ERR_OUT_OF_RESOURCES;
+    sym_full_kernel<<<grid_for((int64_t)N * N), 256, 0, s>>>(A, lda, S, N, uplo == ChamUpper);
+    CHB_LAUNCHED(1);
+    const double one = 1.0, zero = 0.0;
+    if ((rc = CUDA_dgemm(ChamNoTrans, ChamNoTrans, N, N, N, &one, B, ldb, S, N, &zero, C, ldc, h))) return rc;
+    CHB_CUDA(cudaGetLastError());
+    CHB_CUDA(cudaStreamSynchronize(s));
+    return 0;
 }
 
 // LAPACK layout: A on the host or the device.
@@ -238,6 +270,90 @@ int CHAMELEON_dpotri(cham_uplo_t uplo, int N, double *A, int LDA) {
     if (N == 0) return 0;
     return inverse_lapack(OP_POTRI, uplo, ChamNonUnit, N, A, LDA);
 }
+// compute/zpotrimm.c:72 (LAPACK layout): A, B, C host or device arrays.
+int CHAMELEON_dpotrimm(cham_uplo_t uplo, int N, double *A, int LDA, double *B, int LDB, double *C, int LDC) {
+    int rc = ensure_init();
+    if (rc) return rc;
+    if (uplo != ChamUpper && uplo != ChamLower) return -1;
+    if (N < 0) return -2;
+    if (LDA < std::max(1, N)) return -4;
+    if (LDB < std::max(1, N)) return -6;
+    if (LDC < std::max(1, N)) return -8;
+    if (N == 0) return 0;
+    cudaStream_t s = ctx().stream;
+    auto on_dev = [](const void *p) {
+        cudaPointerAttributes at;
+        if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
+    };
+    const bool da = on_dev(A), db = on_dev(B), dc = on_dev(C);
+    double *dA = A, *dB = B, *dC = C;
+    int lda = LDA, ldb = LDB, ldc = LDC;
+    if (!da) {
+        if (!(dA = stage_in(0, A, LDA, N, N, s))) return CHAMELEON_ERR_OUT_OF_RESOURCES;
+        lda = N;
+    }
+    if (!db) {
+        if (!(dB = work(&g_w3, &g_w3_bytes, (size_t)N * N * sizeof(double)))) return CHAMELEON_ERR_OUT_OF_RESOURCES;
+        CHB_CUDA(cudaMemcpy2DAsync(dB, (size_t)N * sizeof(double), B, (size_t)LDB * sizeof(double),
+                                   (size_t)N * sizeof(double), N, cudaMemcpyHostToDevice, s));
+        ldb = N;
+    }
+    if (!dc) {
+        if (!(dC = work(&g_w4, &g_w4_bytes, (size_t)N * N * sizeof(double)))) return CHAMELEON_ERR_OUT_OF_RESOURCES;
+        ldc = N;
+    }
+    rc = potrimm_dev(uplo, N, dA, lda, dB, ldb, dC, ldc);
+    if (rc >= 0) {
+        if (!da)
+            if (int r2 = stage_out(A, LDA, dA, N, N, s)) return r2;
+        if (!dc && rc == 0)
+            CHB_CUDA(cudaMemcpy2DAsync(C, (size_t)LDC * sizeof(double), dC, (size_t)N * sizeof(double),
+                                       (size_t)N * sizeof(double), N, cudaMemcpyDeviceToHost, s));
+        CHB_CUDA(cudaStreamSynchronize(s));
+    }
+    return rc;
+}
+
+// compute/zpotrimm.c:202 (tile layout): square descriptors of one order.
+int CHAMELEON_dpotrimm_Tile(cham_uplo_t uplo, CHAM_desc_t *A, CHAM_desc_t *B, CHAM_desc_t *C) {
+    int rc = ensure_init();
+    if (rc) return rc;
+    if (uplo != ChamUpper && uplo != ChamLower) return CHAMELEON_ERR_ILLEGAL_VALUE;
+    for (CHAM_desc_t *d : {A, B, C})
+        if (!d || d->dtyp != ChamRealDouble || d->m != d->n || d->mb != d->nb) return CHAMELEON_ERR_ILLEGAL_VALUE;
+    if (B->n != A->n || C->n != A->n) return CHAMELEON_ERR_ILLEGAL_VALUE;
+    const int N = A->n;
+    if (N == 0) return 0;
+    cudaStream_t s = ctx().stream;
+    double *DA = staging(1, (size_t)N * N * sizeof(double));
+    double *DB = work(&g_w3, &g_w3_bytes, (size_t)N * N * sizeof(double));
+    double *DC = work(&g_w4, &g_w4_bytes, (size_t)N * N * sizeof(double));
+    if (!DA || !DB || !DC) return CHAMELEON_ERR_OUT_OF_RESOURCES;
+    for (CHAM_desc_t *d : {A, B, C})
+        if ((rc = desc_upload(d))) return rc;
+    auto conv = [&](CHAM_desc_t *d, double *D, int to_dense) {
+        const DescDev &dv = priv(d)->dev;
+        tiles_dense_kernel<<<grid_for((int64_t)N * N), 256, 0, s>>>((double *)d->mat, dv.off, dv.ld, d->mt, d->mb,
+                                                                    d->nb, N, D, to_dense);
+        CHB_LAUNCHED(1);
+    };
+    conv(A, DA, 1);
+    conv(B, DB, 1);
+    rc = potrimm_dev(uplo, N, DA, N, DB, N, DC, N);
+    if (rc == 0) {
+        conv(A, DA, 0);
+        conv(C, DC, 0);
+        CHB_CUDA(cudaStreamSynchronize(s));
+        if (int r2 = desc_sync_to_host(A)) return r2;
+        if (int r2 = desc_sync_to_host(C)) return r2;
+    }
+    return rc;
+}
+
 int CHAMELEON_dtrtri_Tile(cham_uplo_t uplo, cham_diag_t diag, CHAM_desc_t *A) {
     int rc = ensure_init();
     if (rc) return rc;

@@ -238,6 +238,10 @@ int CHAMELEON_dtrtri(cham_uplo_t uplo, cham_diag_t diag, int N, double *A, int L
 int CHAMELEON_dlauum(cham_uplo_t uplo, int N, double *A, int LDA);
 int CHAMELEON_dpotri(cham_uplo_t uplo, int N, double *A, int LDA);
 int CHAMELEON_dtrtri_Tile(cham_uplo_t uplo, cham_diag_t diag, CHAM_desc_t *A);
+/* compute/zpotrimm.c:72,202 (pzpotrimm.c): A (SPD on entry) <- the uplo
+ * triangle of A^-1 (potrf, trtri, lauum), then C <- B A^-1; N x N each. */
+int CHAMELEON_dpotrimm(cham_uplo_t uplo, int N, double *A, int LDA, double *B, int LDB, double *C, int LDC);
+int CHAMELEON_dpotrimm_Tile(cham_uplo_t uplo, CHAM_desc_t *A, CHAM_desc_t *B, CHAM_desc_t *C);
 int CHAMELEON_dlauum_Tile(cham_uplo_t uplo, CHAM_desc_t *A);
 int CHAMELEON_dpotri_Tile(cham_uplo_t uplo, CHAM_desc_t *A);
 

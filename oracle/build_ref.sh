@@ -101,7 +101,8 @@ CORE_Z="core_zgemm core_zsyrk core_ztrsm core_zpotrf core_zplgsy core_zplrnt
         core_zlauum core_ztrtri"
 COMPUTE_Z="zposv zpotrf zpotrs pzpotrf pztrsm zplgsy pzplgsy zplrnt pzplrnt pzlacpy zlacpy
            zlansy pzlansy zlange pzlange zlaset pzlaset zpotrf_batch ztrsm_batch ztile
-           zpotri ztrtri zlauum pztrtri pzlauum zgemm_batch zherk_batch"
+           zpotri ztrtri zlauum pztrtri pzlauum zgemm_batch zherk_batch
+           zpotrimm pzpotrimm"
 CODELET_Z="codelet_zgemm codelet_zsyrk codelet_ztrsm codelet_zpotrf codelet_zplgsy
            codelet_zplrnt codelet_zlacpy codelet_zlaset codelet_zlansy codelet_zlange
            codelet_zgessq codelet_zsyssq codelet_zplssq codelet_zlascal codelet_zgeadd

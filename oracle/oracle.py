@@ -121,6 +121,8 @@ def reference(ncores=0):
             [ctypes.c_int] * 7 + [_dp, _dp, _dp]
         L.chamref_dsyrk_batch.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double] + \
             [ctypes.c_int] * 4 + [_dp, _dp]
+        L.chamref_dpotrimm.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp, ctypes.c_int, _dp,
+                                       ctypes.c_int, _dp, ctypes.c_int]
         L.chamref_dinverse.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp,
                                        ctypes.c_int]
         L.chamref_init(ncores if ncores > 0 else (os.cpu_count() or 1))
@@ -276,3 +278,15 @@ def gered(uplo, prec, A, mb):
             tags[m, n] = 1
             A[sl] = A[sl].astype(np.float32).astype(np.float64)
     return A, tags
+
+
+def ref_dpotrimm(uplo, A, B, NB):
+    """Reference CHAMELEON_dpotrimm (compute/zpotrimm.c, pzpotrimm.c) on copies:
+    returns (A' = uplo triangle of A^-1, C = B A^-1, info)."""
+    L = reference()
+    Aw = np.asfortranarray(A.copy())
+    Bw = np.asfortranarray(B.copy())
+    N = Aw.shape[0]
+    C = np.zeros((N, N), order="F")
+    info = L.chamref_dpotrimm(uplo, N, NB, _ptr(Aw), max(N, 1), _ptr(Bw), max(N, 1), _ptr(C), max(N, 1))
+    return Aw, C, info

@@ -211,6 +211,17 @@ int chamref_dtrsm_batch(int side, int uplo, int trans, int diag, double alpha,
     return rc;
 }
 
+/* CHAMELEON_dpotrimm (compute/zpotrimm.c:72) on caller arrays. */
+int chamref_dpotrimm(int uplo, int N, int nb, double *A, int lda, double *B, int ldb, double *C, int ldc)
+{
+    int rc = 0;
+    CHAMELEON_Set(CHAMELEON_TILE_SIZE, nb);
+#pragma omp parallel
+#pragma omp master
+    rc = CHAMELEON_dpotrimm((cham_uplo_t)uplo, N, A, lda, B, ldb, C, ldc);
+    return rc;
+}
+
 /* CHAMELEON_dgemm_batch_Tile / dsyrk_batch_Tile (compute/zgemm_batch.c:193,
  * zherk_batch.c:176): `count` tiles stacked in one tile column of a
  * column-major (count am) x an array (likewise B: bm x bn, C: m x n tiles). */

@@ -215,3 +215,41 @@ def test_lapacke_and_fortran_entry_points(cb, orc):
                               cb._addr(Ab), ctypes.byref(c_int(N)), cb._addr(Bw), ctypes.byref(c_int(N)),
                               ctypes.byref(info))
     assert info.value == 301
+
+
+@pytest.mark.parametrize("uplo", [UPPER, LOWER])
+@pytest.mark.parametrize("N", [1, 130, 1000])
+def test_dpotrimm_lapack_and_tile(cb, orc, uplo, N):
+    """compute/zpotrimm.c: A (SPD) <- uplo triangle of A^-1, C <- B A^-1."""
+    A = spd(orc, N, seed=23)
+    B = orc.dplrnt(N, N, 77)
+    inv = np.linalg.inv(A)
+    sentinel = np.full((N, N), 5.5)
+    Aw = np.asfortranarray(tri(uplo)(A) + other(uplo, sentinel))
+    Bw = np.asfortranarray(B.copy())
+    C = np.zeros((N, N), order="F")
+    L = cb.lib()
+    assert L.CHAMELEON_dpotrimm(uplo, N, cb._addr(Aw), N, cb._addr(Bw), N, cb._addr(C), N) == 0
+    assert np.array_equal(other(uplo, Aw), other(uplo, sentinel))
+    scale = np.abs(inv).max()
+    assert np.abs(tri(uplo)(Aw) - tri(uplo)(inv)).max() <= 64 * N * EPS * scale
+    tolc = 64 * N * EPS * scale * np.abs(B).max() * max(1, N) ** 0.5
+    assert np.abs(C - B @ inv).max() <= tolc
+    assert np.array_equal(Bw, B)
+    if orc.reference_available() and N > 1:
+        Ar, Cr, info = orc.ref_dpotrimm(uplo, A, B, 320)
+        assert info == 0
+        assert np.abs(tri(uplo)(Aw) - tri(uplo)(Ar)).max() <= 64 * N * EPS * scale
+        assert np.abs(C - Cr).max() <= tolc
+    if N >= 130:
+        dA, dB, dC = (cb.Desc.create(N, N, 96) for _ in range(3))
+        dA.from_numpy(A)
+        dB.from_numpy(B)
+        assert L.CHAMELEON_dpotrimm_Tile(uplo, dA.ptr, dB.ptr, dC.ptr) == 0
+        assert np.abs(tri(uplo)(dA.to_numpy()) - tri(uplo)(Aw)).max() <= 16 * N * EPS * scale
+        assert np.abs(dC.to_numpy() - C).max() <= tolc
+    if N > 1:
+        # not positive definite: info from the factorization
+        Ab = np.asfortranarray(A.copy())
+        Ab[N // 2, N // 2] = -1.0
+        assert L.CHAMELEON_dpotrimm(uplo, N, cb._addr(Ab), N, cb._addr(Bw), N, cb._addr(C), N) == N // 2 + 1

@@ -45,3 +45,18 @@ def test_reference_gemm_syrk_batch_vs_numpy(ref):
     for i in range(3):
         assert np.abs(np.tril(out[i]) - np.tril(exp[i])).max() < 1e-12
         assert np.array_equal(np.triu(out[i], 1), np.triu(S[i], 1))
+
+
+@pytest.mark.parametrize("uplo", [121, 122])
+def test_reference_potrimm_vs_numpy(ref, uplo):
+    rng = np.random.default_rng(uplo)
+    N = 150
+    M = rng.standard_normal((N, N))
+    A = M @ M.T / N + np.eye(N)
+    B = rng.standard_normal((N, N))
+    Aw, C, info = ref.ref_dpotrimm(uplo, A, B, 48)
+    assert info == 0
+    inv = np.linalg.inv(A)
+    tri = np.triu if uplo == 121 else np.tril
+    assert np.abs(tri(Aw) - tri(inv)).max() < 1e-12
+    assert np.abs(C - B @ inv).max() < 1e-12
