@@ -11,12 +11,12 @@
 // threads with small loops, and written back once.
 //
 // Layout: the lower triangle by 64-wide block columns; block column b holds
-// rows 64 b .. n-1, column-major with a leading dimension rounded up to a
-// multiple of 4 (float4 row loads).  Right-looking over block columns:
+// rows 64 b .. n-1, column-major with a padded leading dimension (blk_ld).  Right-looking over block columns:
 //   leaf:     D_bb = L_bb L_bb^T and X_b = L_bb^-1 (the warp-level 64 x 64
 //             leaf of rec.cuh on a staged copy of the block)
 //   panel:    L_ib = A_ib X_b^T                      (i > b)
 //   trailing: A_ij -= L_ib L_jb^T                    (i >= j > b)
+// (the panel and trailing products on the tensor cores as 3xTF32)
 // Same contract as CORE_spotrf on a lower view (coreblas/compute/core_zpotrf.c
 // :75-81): lower triangle overwritten by L, upper untouched, LAPACK info; the
 // inverted blocks go to invd (IB x IB, ld IB, zero outside the block), as the
@@ -33,7 +33,11 @@ constexpr int BW = 64;      // block-column width (= IB)
 constexpr int LDI = 65;     // leading dimension of the staged block and its inverse
 static_assert(LDI == rec::LDS, "the staged leaf uses the leading dimension of rec.cuh");
 
-__host__ __device__ constexpr int blk_ld(int n, int b) { return ((n - BW * b) + 3) & ~3; }
+// Leading dimension of block column b: its rows rounded up to 32, plus 8
+// (8 mod 32: the tensor-core fragment loads -- 8 consecutive rows at 4
+// columns -- then hit 32 distinct banks; a multiple of 4 keeps the columns
+// 16-byte aligned for the vectorized load and write-back).
+__host__ __device__ constexpr int blk_ld(int n, int b) { return (((n - BW * b) + 31) & ~31) + 8; }
 __host__ __device__ constexpr int blk_off(int n, int b) {
     int o = 0;
     for (int i = 0; i < b; ++i) o += BW * blk_ld(n, i);
@@ -74,44 +78,84 @@ static __device__ __noinline__ int leaf(float *D, int ldd, int nbk, float *sD) {
 }
 
 // acc(i, c) = sum_{k < K} Xm(i, k) Ym(c, k) for rows i < M (M <= 192) and
-// columns c < 64.  Xm: column-major (ld ldx, multiple of 4; 16-byte aligned
-// base), Ym(c, k) at Ym[k * ldy + c].  Thread mapping: columns tj + 16 q,
-// rows 4 ti + e + 64 g (float4 loads of four rows).
+// columns c < 64 on the tensor cores: mma.sync m16n8k8 TF32 with each operand
+// split in two TF32 parts and three products (hi*hi + hi*lo + lo*hi, close to
+// FP32 accuracy).  Xm: column-major (ld ldx), Ym(c, k) at Ym[k * ldy + c].
+// Warp w owns rows 48 (w & 3) .. +47 (three 16-row tiles) and columns
+// 32 (w >> 2) .. +31 (four 8-column tiles); rows >= M and k >= K read as
+// zero, so no operand entry outside them is read.
 struct Frag {
-    float v[3][4][4];   // [row group g][row e][column q]
+    float v[3][4][4];   // [row tile][column tile][mma accumulator]
 };
-static __device__ __forceinline__ void gemm64(Frag &acc, const float *Xm, int ldx, int M, const float *Ym, int ldy, int K) {
-    const int tj = threadIdx.x & 15, ti = threadIdx.x >> 4;
+static __device__ __forceinline__ void gemm64(Frag &acc, const float *Xm, int ldx, int M, const float *Ym, int ldy,
+                                              int K) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int g = lane >> 2, t = lane & 3;
+    const int r0 = 48 * (w & 3), c0 = 32 * (w >> 2);
 #pragma unroll
-    for (int g = 0; g < 3; ++g)
+    for (int i = 0; i < 3; ++i)
 #pragma unroll
-        for (int e = 0; e < 4; ++e)
+        for (int j = 0; j < 4; ++j)
 #pragma unroll
-            for (int q = 0; q < 4; ++q) acc.v[g][e][q] = 0.f;
-    const int ng = (M + 63) / 64;
-#pragma unroll 2
-    for (int k = 0; k < K; ++k) {
-        float y[4];
+            for (int e = 0; e < 4; ++e) acc.v[i][j][e] = 0.f;
+    const int nm = M > r0 ? min(3, (M - r0 + 15) / 16) : 0;   // row tiles with rows < M (warp-uniform)
+    if (nm == 0) return;
+#pragma unroll 1
+    for (int k8 = 0; k8 < K; k8 += 8) {
+        const int ka = k8 + t, kb = k8 + t + 4;
+        const bool va = ka < K, vb = kb < K;
+        // the four column tiles' fragments stay live; each row tile's are
+        // loaded just before its products (fewer live registers)
+        uint32_t bh[4][2], bl[4][2];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) y[q] = Ym[k * ldy + tj + 16 * q];
+        for (int j = 0; j < 4; ++j) {
+            const int c = c0 + 8 * j + g;
+            split_tf32(va ? Ym[ka * ldy + c] : 0.f, bh[j][0], bl[j][0]);
+            split_tf32(vb ? Ym[kb * ldy + c] : 0.f, bh[j][1], bl[j][1]);
+        }
 #pragma unroll
-        for (int g = 0; g < 3; ++g) {
-            if (g < ng) {
-                const float4 xv = *reinterpret_cast<const float4 *>(Xm + k * ldx + 4 * ti + 64 * g);
-                const float xs[4] = {xv.x, xv.y, xv.z, xv.w};
+        for (int i = 0; i < 3; ++i) {
+            if (i < nm) {
+                const int ra = r0 + 16 * i + g, rb = ra + 8;
+                uint32_t ah[4], al[4];
+                split_tf32((va && ra < M) ? Xm[ka * ldx + ra] : 0.f, ah[0], al[0]);
+                split_tf32((va && rb < M) ? Xm[ka * ldx + rb] : 0.f, ah[1], al[1]);
+                split_tf32((vb && ra < M) ? Xm[kb * ldx + ra] : 0.f, ah[2], al[2]);
+                split_tf32((vb && rb < M) ? Xm[kb * ldx + rb] : 0.f, ah[3], al[3]);
 #pragma unroll
-                for (int e = 0; e < 4; ++e)
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) acc.v[g][e][q] = fmaf(xs[e], y[q], acc.v[g][e][q]);
+                for (int j = 0; j < 4; ++j) {
+                    mma_tf32_1688(acc.v[i][j], al, bh[j]);
+                    mma_tf32_1688(acc.v[i][j], ah, bl[j]);
+                    mma_tf32_1688(acc.v[i][j], ah, bh[j]);
+                }
             }
         }
     }
 }
 
+// f(row, column, value) over this thread's accumulators (rows may be >= M:
+// their values are zero and the caller's row guard skips them).
+template <class F>
+static __device__ __forceinline__ void frag_each(const Frag &acc, F &&f) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int g = lane >> 2, t = lane & 3;
+    const int r0 = 48 * (w & 3), c0 = 32 * (w >> 2);
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int r = r0 + 16 * i + g, c = c0 + 8 * j + 2 * t;
+            f(r, c, acc.v[i][j][0]);
+            f(r, c + 1, acc.v[i][j][1]);
+            f(r + 8, c, acc.v[i][j][2]);
+            f(r + 8, c + 1, acc.v[i][j][3]);
+        }
+}
+
 // Factor the n x n lower view T (n <= MAXN) through shared memory `sm`
 // (SMEM_BYTES, 16-byte aligned); inverted blocks to invd.  Returns info.
 // All 256 threads.
-static __device__ int potrf(const ViewF &T, int n, float *invd, float *sm, unsigned *ph = nullptr) {
+static __device__ __noinline__ int potrf(const ViewF &T, int n, float *invd, float *sm, unsigned *ph = nullptr) {
     const int tid = threadIdx.x;
     const int nb = (n + BW - 1) / BW;
     float *sDl = sm + blk_off(n, nb);   // staged leaf block, then its inverse
@@ -188,16 +232,9 @@ static __device__ int potrf(const ViewF &T, int n, float *invd, float *sm, unsig
             Frag acc;
             gemm64(acc, Sb + BW, ldb, M, Xs, LDI, nbk);   // X_b(c, k) at Xs[k * LDI + c]
             __syncthreads();
-            const int tj = tid & 15, ti = tid >> 4;
-#pragma unroll
-            for (int g = 0; g < 3; ++g)
-#pragma unroll
-                for (int e = 0; e < 4; ++e)
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        const int r = 4 * ti + e + 64 * g, c = tj + 16 * q;
-                        if (r < M && c < nbk) Sb[c * ldb + BW + r] = acc.v[g][e][q];
-                    }
+            frag_each(acc, [&](int r, int c, float v) {
+                if (r < M && c < nbk) Sb[c * ldb + BW + r] = v;
+            });
             __syncthreads();
         }
         lap(1);
@@ -208,16 +245,9 @@ static __device__ int potrf(const ViewF &T, int n, float *invd, float *sm, unsig
             Frag acc;
             // rows i >= 64 cb of panel b, against its rows 64 cb .. 64 cb + 63
             gemm64(acc, Sb + BW * (cb - b), ldb, Mc, Sb + BW * (cb - b), ldb, nbk);
-            const int tj = tid & 15, ti = tid >> 4;
-#pragma unroll
-            for (int g = 0; g < 3; ++g)
-#pragma unroll
-                for (int e = 0; e < 4; ++e)
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        const int r = 4 * ti + e + 64 * g, c = tj + 16 * q;
-                        if (r < Mc && c < wc && r >= c) Sc[c * ldc + r] -= acc.v[g][e][q];
-                    }
+            frag_each(acc, [&](int r, int c, float v) {
+                if (r < Mc && c < wc && r >= c) Sc[c * ldc + r] -= v;
+            });
         }
         __syncthreads();
         lap(2);
