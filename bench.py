@@ -828,7 +828,7 @@ def main():
     ap.add_argument("--batch-plain", type=int, default=BATCH_COUNT,
                     help="matrices timed through the plain per-matrix path (0: skip)")
     ap.add_argument("--no-serve", dest="serve", action="store_false")
-    ap.add_argument("--serve-slots", type=int, default=2)
+    ap.add_argument("--serve-slots", type=int, default=4)
     ap.add_argument("--serve-window", type=float, default=10.0, help="seconds of arrivals per load level")
     ap.add_argument("--serve-loads", type=float, nargs="+", default=[0.5, 0.8, 0.95])
     ap.add_argument("--serve-cap-requests", type=int, default=300)

@@ -491,7 +491,7 @@ class Server:
     caller keeps them alive until the request completes (`drain()`).
     """
 
-    def __init__(self, slots=2, hbm_budget_bytes=0.0, small_n=512):
+    def __init__(self, slots=4, hbm_budget_bytes=0.0, small_n=512):
         init()
         h = ctypes.c_void_p()
         check(lib().CHAM_B200_Serve_Create(ctypes.byref(h), slots, float(hbm_budget_bytes), small_n),

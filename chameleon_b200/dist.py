@@ -113,7 +113,7 @@ class _ServerSolver:
     """A rank's solver on its own GPU: the library's serving loop (batched FP64
     for n <= small_n, the mixed solver on `slots` streams above)."""
 
-    def __init__(self, uplo=ChamLower, slots=2):
+    def __init__(self, uplo=ChamLower, slots=4):
         from . import Server
         self.uplo = uplo
         self.server = Server(slots=slots)
