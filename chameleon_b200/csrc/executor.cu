@@ -134,7 +134,9 @@ std::vector<Task> build_order(const Shape &s) {
     auto c_strsm = [&](double t, double w, int parts) {
         return lat ? 13.0 + 0.01 * t : cal.strsm * 3.0 * t * t * w / parts;
     };
-    auto c_supd = [&](double t, double w) { return lat ? 8.0 + 0.04 * t : cal.supd * 2.0 * SUBB * t * w; };
+    auto c_supd = [&](double t, double w) {
+        return lat ? 8.0 + 0.04 * t : cal.supd * 2.0 * solve_rows(s.mode) * t * w;
+    };
     if (cast) {
         // the copy engine delivers the stored triangle one tile column after
         // the other (model-only tasks, in order); each tile's cast waits for
@@ -199,19 +201,22 @@ std::vector<Task> build_order(const Shape &s) {
         }
     }
     if (solve) {
+        // substitution row blocks (SOLB rows with full tile inverses)
+        const int srb = solve_rows(s.mode);
+        auto nsb = [&](int m) { return (tm(m) + srb - 1) / srb; };
         std::vector<int> F((size_t)NT * NTB, -1), lastFU((size_t)NT * NTB, -1);
         std::vector<int> Bk((size_t)NT * NTB, -1), lastBU((size_t)NT * NTB, -1);
         for (int bn = 0; bn < NTB; ++bn) {
             const double w = wB(bn);
             for (int k = 0; k < NT; ++k) {
                 // MODE_XINV: one sub-task per row block (each applies its rows of the inverse)
-                const int f = add(TK_FWD_TRSM, k, k, k, bn, xinv ? nbi(k) : 1,
-                                  c_strsm(tm(k), w, xinv ? nbi(k) : 1));
+                const int f = add(TK_FWD_TRSM, k, k, k, bn, xinv ? nsb(k) : 1,
+                                  c_strsm(tm(k), w, xinv ? nsb(k) : 1));
                 edge(xinv ? XI[k] : P[k], f);
                 edge(lastFU[k + (size_t)NT * bn], f);
                 F[k + (size_t)NT * bn] = f;
                 for (int m = k + 1; m < NT; ++m) {
-                    const int u = add(TK_FWD_UPD, m, k, k, bn, nbi(m), c_supd(tm(k), w));
+                    const int u = add(TK_FWD_UPD, m, k, k, bn, nsb(m), c_supd(tm(k), w));
                     edge(f, u);
                     if (fact) edge(Tr[m + (size_t)NT * k], u);
                     edge(lastFU[m + (size_t)NT * bn], u);
@@ -219,13 +224,13 @@ std::vector<Task> build_order(const Shape &s) {
                 }
             }
             for (int k = NT - 1; k >= 0; --k) {
-                const int b = add(TK_BWD_TRSM, k, k, k, bn, xinv ? nbi(k) : 1,
-                                  c_strsm(tm(k), w, xinv ? nbi(k) : 1));
+                const int b = add(TK_BWD_TRSM, k, k, k, bn, xinv ? nsb(k) : 1,
+                                  c_strsm(tm(k), w, xinv ? nsb(k) : 1));
                 edge(F[k + (size_t)NT * bn], b);
                 edge(lastBU[k + (size_t)NT * bn], b);
                 Bk[k + (size_t)NT * bn] = b;
                 for (int m = k - 1; m >= 0; --m) {
-                    const int u = add(TK_BWD_UPD, m, k, k, bn, nbi(m), c_supd(tm(k), w));
+                    const int u = add(TK_BWD_UPD, m, k, k, bn, nsb(m), c_supd(tm(k), w));
                     edge(b, u);
                     edge(lastBU[m + (size_t)NT * bn], u);
                     lastBU[m + (size_t)NT * bn] = u;
@@ -446,8 +451,10 @@ int run_cholesky_dag(int mode, cham_uplo_t uplo, CHAM_desc_t *A, CHAM_desc_t *B,
     // blocks of the last tile row, and on nrhs only through NTB (the kernel
     // takes the exact sizes from the parameters): key the cache on that
     // canonical shape so that callers with many distinct N share schedules.
-    const int last_sub = ((N - (NT - 1) * NB) + SUBB - 1) / SUBB;
-    const int canonN = (NT - 1) * NB + std::min(NB, last_sub * SUBB);
+    // (the finer of the update and substitution row blocks decides)
+    const int gran = std::min(SUBB, solve_rows(mode));
+    const int last_sub = ((N - (NT - 1) * NB) + gran - 1) / gran;
+    const int canonN = (NT - 1) * NB + std::min(NB, last_sub * gran);
     // nrhs enters the cost model (not the task list): keep it, with the last
     // block's width rounded up to 16, so that the costs stay close and the
     // number of distinct schedules stays small

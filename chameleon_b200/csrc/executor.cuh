@@ -81,6 +81,12 @@ static_assert(sizeof(Task) == 16, "Task is 16 bytes");
 enum ExecMode : int { MODE_FACT = 1, MODE_SOLVE = 2, MODE_XINV = 4, MODE_NOINV = 8, MODE_CAST = 16 };
 
 constexpr int SUBB = 128;      // sub-block edge of trailing updates / row blocks
+// Row block of the substitution tasks (FWD/BWD TRSM and UPD) with full
+// diagonal-tile inverses (MODE_XINV): the forward and backward solves are a
+// chain of 2 NT dependent steps, and 64-row tasks halve each step's latency.
+constexpr int SOLB = 64;
+// Row block of the substitution tasks of a launch mode.
+__host__ __device__ constexpr int solve_rows(int mode) { return (mode & 4 /*MODE_XINV*/) ? SOLB : SUBB; }
 
 struct ExecState {
     int next;          // dispatch cursor (alone in its 128-byte line: the contended atomic)

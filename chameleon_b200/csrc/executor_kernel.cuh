@@ -43,8 +43,13 @@ struct Dims {
     __device__ ViewT<T> Yt(int m, int bn) const {
         return ViewT<T>{static_cast<T *>(p.Y) + p.b_off[m + p.NT * bn], 1, p.b_ld[m]};
     }
+    // Row blocks of tile m in the substitution updates (SOLB rows with MODE_XINV).
+    __device__ int nsb(int m) const {
+        const int r = solve_rows(p.mode);
+        return (tm(m) + r - 1) / r;
+    }
     // Sub-tasks a substitution of tile k is split into (its row blocks, MODE_XINV).
-    __device__ int nsolve(int k) const { return (p.mode & MODE_XINV) ? nbi(k) : 1; }
+    __device__ int nsolve(int k) const { return (p.mode & MODE_XINV) ? nsb(k) : 1; }
     __device__ T *inv(int k) const {
         return static_cast<T *>(p.invd) + (p.full_inv ? (int64_t)k * p.NB * p.NB : (int64_t)k * p.NIB * IB * IB);
     }
@@ -107,20 +112,20 @@ __device__ Deps task_deps(const Task &t, const ExecParams &p, const Dims<T> &d) 
     case TK_FWD_TRSM:
         if (!(p.mode & MODE_XINV)) need(0, &p.panA[t.k + p.NT * t.k], 1);
         else if (!(p.mode & MODE_NOINV)) need(0, &p.xinvDone[t.k], 1);
-        need(1, &p.fwdB[t.k + p.NT * t.bn], t.k * d.nbi(t.k));
+        need(1, &p.fwdB[t.k + p.NT * t.bn], t.k * d.nsb(t.k));
         break;
     case TK_FWD_UPD:
         need(0, &p.fwdDone[t.k + p.NT * t.bn], d.nsolve(t.k));
         if (fact) need(1, &p.panA[t.m + p.NT * t.k], d.nbi(t.m));
-        need(2, &p.fwdB[t.m + p.NT * t.bn], t.k * d.nbi(t.m));
+        need(2, &p.fwdB[t.m + p.NT * t.bn], t.k * d.nsb(t.m));
         break;
     case TK_BWD_TRSM:
         need(0, &p.fwdDone[t.k + p.NT * t.bn], d.nsolve(t.k));
-        need(1, &p.bwdB[t.k + p.NT * t.bn], (p.NT - 1 - t.k) * d.nbi(t.k));
+        need(1, &p.bwdB[t.k + p.NT * t.bn], (p.NT - 1 - t.k) * d.nsb(t.k));
         break;
     case TK_BWD_UPD:
         need(0, &p.bwdDone[t.k + p.NT * t.bn], d.nsolve(t.k));
-        need(1, &p.bwdB[t.m + p.NT * t.bn], (p.NT - 1 - t.k) * d.nbi(t.m));
+        need(1, &p.bwdB[t.m + p.NT * t.bn], (p.NT - 1 - t.k) * d.nsb(t.m));
         break;
     default:
         r.bad = true;
@@ -360,14 +365,15 @@ __device__ void run_task(const Task &t, const ExecParams &p, const Dims<T> &d, T
         const int w = d.wB(t.bn);
         if constexpr (std::is_same<T, float>::value) {
             if (p.mode & MODE_XINV) {
-                // row block t.sub of the tile: forward Y_k = X_k B_k, backward B_k = X_k^T Y_k
-                const int r0 = t.sub * SUBB, n = d.tm(t.k);
-                const int mr = min(SUBB, n - r0);
+                // row block t.sub (SOLB rows) of the tile: forward Y_k = X_k B_k,
+                // backward B_k = X_k^T Y_k
+                const int r0 = t.sub * SOLB, n = d.tm(t.k);
+                const int mr = min(SOLB, n - r0);
                 const VT Xk = d.XI(t.k);
                 const VT Yk = d.Yt(t.k, t.bn);
                 for (int c0 = 0; c0 < w; c0 += 64) {
                     const int wc = min(64, w - c0);
-                    Acc<Cfg12864<T, SP>> acc;
+                    Acc<Cfg64<T, SP>> acc;
                     acc.zero();
                     if (t.kind == TK_FWD_TRSM) {
                         cta_gemm(acc, Xk.sub(r0, 0), X.sub(0, c0).t(), mr, wc, r0 + mr, smem);
@@ -393,20 +399,29 @@ __device__ void run_task(const Task &t, const ExecParams &p, const Dims<T> &d, T
     }
     case TK_FWD_UPD:
     case TK_BWD_UPD: {
-        const int r0 = t.sub * SUBB;
-        const int rows = min(SUBB, d.tm(t.m) - r0);
-        const int w = d.wB(t.bn);
-        // MODE_XINV: forward updates read Y_k into B_m, backward ones read B_k into Y_m
+        // MODE_XINV: forward updates read Y_k into B_m, backward ones read B_k
+        // into Y_m, in SOLB-row blocks
         const bool y = p.mode & MODE_XINV;
+        const int rb = y ? SOLB : SUBB;
+        const int r0 = t.sub * rb;
+        const int rows = min(rb, d.tm(t.m) - r0);
+        const int w = d.wB(t.bn);
         const VT Bm = ((y && t.kind == TK_BWD_UPD) ? d.Yt(t.m, t.bn) : d.Bt(t.m, t.bn)).sub(r0, 0);
         const VT Bk = (y && t.kind == TK_FWD_UPD) ? d.Yt(t.k, t.bn) : d.Bt(t.k, t.bn);
         const VT L = (t.kind == TK_FWD_UPD) ? d.A(t.m, t.k).sub(r0, 0) : d.A(t.k, t.m).t().sub(r0, 0);
         for (int c0 = 0; c0 < w; c0 += 64) {
             const int wc = min(64, w - c0);
-            Acc<Cfg12864<T, SP>> acc;
-            acc.zero();
-            cta_gemm(acc, L, Bk.sub(0, c0).t(), rows, wc, d.tm(t.k), smem);
-            acc.sub_from(Bm.sub(0, c0), rows, wc, false);
+            if (y) {
+                Acc<Cfg64<T, SP>> acc;
+                acc.zero();
+                cta_gemm(acc, L, Bk.sub(0, c0).t(), rows, wc, d.tm(t.k), smem);
+                acc.sub_from(Bm.sub(0, c0), rows, wc, false);
+            } else {
+                Acc<Cfg12864<T, SP>> acc;
+                acc.zero();
+                cta_gemm(acc, L, Bk.sub(0, c0).t(), rows, wc, d.tm(t.k), smem);
+                acc.sub_from(Bm.sub(0, c0), rows, wc, false);
+            }
         }
         break;
     }

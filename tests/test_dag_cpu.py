@@ -14,6 +14,7 @@ import scipy.linalg as sla
 
 TK_POTRF, TK_TRSM, TK_UPD, TK_FWD_TRSM, TK_FWD_UPD, TK_BWD_TRSM, TK_BWD_UPD, TK_INV, TK_XINV, TK_CAST = range(1, 11)
 SUBB = 128
+SOLB = 64     # row block of the substitutions with full tile inverses (MODE_XINV)
 FACT, SOLVE, XINV, NOINV, CAST = 1, 2, 4, 8, 16
 
 
@@ -43,7 +44,9 @@ def check_waits(tasks, mode, N, NB, nrhs, NBB, G=1):
     xinv = np.zeros(NT, int)
     fact = bool(mode & FACT)
     # with full tile inverses (XINV) each substitution is split into row blocks
-    ns = (lambda k: nbi(k)) if mode & XINV else (lambda k: 1)
+    srb = SOLB if mode & XINV else SUBB
+    nsb = lambda m: -(-tm(m) // srb)
+    ns = (lambda k: nsb(k)) if mode & XINV else (lambda k: 1)
     applied = {}   # (m, n, bi, bj) -> panels applied so far, in order
     cast = np.zeros((NT, NT), int)
     ccast = bool(mode & CAST)   # the host's arrival flags are external: assumed set
@@ -73,14 +76,14 @@ def check_waits(tasks, mode, N, NB, nrhs, NBB, G=1):
                 inv_ok = bool(mode & NOINV) or xinv[k] >= 1
             else:
                 inv_ok = pan[k, k] >= 1
-            ok = inv_ok and fwdB[k, bn] >= k * nbi(k); fwdD[k, bn] += 1
+            ok = inv_ok and fwdB[k, bn] >= k * nsb(k); fwdD[k, bn] += 1
         elif kind == TK_FWD_UPD:
-            ok = fwdD[k, bn] >= ns(k) and (not fact or pan[m, k] >= nbi(m)) and fwdB[m, bn] >= k * nbi(m)
+            ok = fwdD[k, bn] >= ns(k) and (not fact or pan[m, k] >= nbi(m)) and fwdB[m, bn] >= k * nsb(m)
             fwdB[m, bn] += 1
         elif kind == TK_BWD_TRSM:
-            ok = fwdD[k, bn] >= ns(k) and bwdB[k, bn] >= (NT - 1 - k) * nbi(k); bwdD[k, bn] += 1
+            ok = fwdD[k, bn] >= ns(k) and bwdB[k, bn] >= (NT - 1 - k) * nsb(k); bwdD[k, bn] += 1
         elif kind == TK_BWD_UPD:
-            ok = bwdD[k, bn] >= ns(k) and bwdB[m, bn] >= (NT - 1 - k) * nbi(m); bwdB[m, bn] += 1
+            ok = bwdD[k, bn] >= ns(k) and bwdB[m, bn] >= (NT - 1 - k) * nsb(m); bwdB[m, bn] += 1
         else:
             raise AssertionError(kind)
         assert ok, (kind, sub, m, n, k, bn)
@@ -132,10 +135,10 @@ def emulate(tasks, A, B, uplo, N, NB, NBB, xinv=False):
         elif kind in (TK_INV, TK_XINV):
             pass   # inverses of diagonal tiles: the emulation solves triangular systems directly
         elif kind == TK_FWD_TRSM and xinv:
-            r = slice(sub * SUBB, (sub + 1) * SUBB)
+            r = slice(sub * SOLB, (sub + 1) * SOLB)
             Yt(k, bn)[r] = np.linalg.inv(np.tril(L(k, k)))[r] @ Bt(k, bn)
         elif kind == TK_BWD_TRSM and xinv:
-            r = slice(sub * SUBB, (sub + 1) * SUBB)
+            r = slice(sub * SOLB, (sub + 1) * SOLB)
             Bt(k, bn)[r] = np.linalg.inv(np.tril(L(k, k))).T[r] @ Yt(k, bn)
         elif kind == TK_FWD_TRSM:
             X = Bt(k, bn); X[:] = sla.solve_triangular(np.tril(L(k, k)), X, lower=True)
@@ -143,10 +146,12 @@ def emulate(tasks, A, B, uplo, N, NB, NBB, xinv=False):
             X = Bt(k, bn); X[:] = sla.solve_triangular(np.tril(L(k, k)), X, lower=True, trans=1)
         elif kind == TK_FWD_UPD:
             src = Yt(k, bn) if xinv else Bt(k, bn)
-            Bt(m, bn)[sub * SUBB:(sub + 1) * SUBB] -= L(m, k)[sub * SUBB:(sub + 1) * SUBB] @ src
+            rb = SOLB if xinv else SUBB
+            Bt(m, bn)[sub * rb:(sub + 1) * rb] -= L(m, k)[sub * rb:(sub + 1) * rb] @ src
         elif kind == TK_BWD_UPD:
             dst = Yt(m, bn) if xinv else Bt(m, bn)
-            dst[sub * SUBB:(sub + 1) * SUBB] -= L(k, m)[:, sub * SUBB:(sub + 1) * SUBB].T @ Bt(k, bn)
+            rb = SOLB if xinv else SUBB
+            dst[sub * rb:(sub + 1) * rb] -= L(k, m)[:, sub * rb:(sub + 1) * rb].T @ Bt(k, bn)
 
 
 SHAPES = [(15, 16, 1, 16), (37, 17, 22, 17), (300, 128, 5, 128), (700, 256, 70, 64), (1000, 384, 3, 384),
@@ -262,7 +267,9 @@ def check_waits_prefix(prefix, mode, N, NB, nrhs, NBB, G=1):
     bwdB = np.zeros_like(fwdB); bwdD = np.zeros_like(fwdB)
     xinv = np.zeros(NT, int)
     fact = bool(mode & FACT)
-    ns = (lambda k: nbi(k)) if mode & XINV else (lambda k: 1)
+    srb = SOLB if mode & XINV else SUBB
+    nsb = lambda m: -(-tm(m) // srb)
+    ns = (lambda k: nsb(k)) if mode & XINV else (lambda k: 1)
     for kind, sub, m, n, k, bn, grp in prefix:
         if kind == TK_CAST:
             continue
@@ -279,14 +286,14 @@ def check_waits_prefix(prefix, mode, N, NB, nrhs, NBB, G=1):
             ok = pan[m, kl] >= nbi(m) and pan[n, kl] >= nbi(n) and upd[m, n] >= grp * S(m, n); upd[m, n] += 1
         elif kind == TK_FWD_TRSM:
             inv_ok = (bool(mode & NOINV) or xinv[k] >= 1) if mode & XINV else pan[k, k] >= 1
-            ok = inv_ok and fwdB[k, bn] >= k * nbi(k); fwdD[k, bn] += 1
+            ok = inv_ok and fwdB[k, bn] >= k * nsb(k); fwdD[k, bn] += 1
         elif kind == TK_FWD_UPD:
-            ok = fwdD[k, bn] >= ns(k) and (not fact or pan[m, k] >= nbi(m)) and fwdB[m, bn] >= k * nbi(m)
+            ok = fwdD[k, bn] >= ns(k) and (not fact or pan[m, k] >= nbi(m)) and fwdB[m, bn] >= k * nsb(m)
             fwdB[m, bn] += 1
         elif kind == TK_BWD_TRSM:
-            ok = fwdD[k, bn] >= ns(k) and bwdB[k, bn] >= (NT - 1 - k) * nbi(k); bwdD[k, bn] += 1
+            ok = fwdD[k, bn] >= ns(k) and bwdB[k, bn] >= (NT - 1 - k) * nsb(k); bwdD[k, bn] += 1
         else:
-            ok = bwdD[k, bn] >= ns(k) and bwdB[m, bn] >= (NT - 1 - k) * nbi(m); bwdB[m, bn] += 1
+            ok = bwdD[k, bn] >= ns(k) and bwdB[m, bn] >= (NT - 1 - k) * nsb(m); bwdB[m, bn] += 1
         assert ok
 
 
