@@ -9,7 +9,7 @@ reference's own code with names substituted; they are compiled by
 ``oracle/build_ref.sh`` into the reference CPU library that the parity tests and
 the CPU baseline use.  Nothing in the product links them.
 
-Rules written for this build (the reference's own rule tables live in
+Rules written for this oracle (the reference's own rule tables live in
 ``cmake_modules/local_subs.py`` and the absent precision generator):
 
 * types:   CHAMELEON_Complex64_t -> double, CHAMELEON_Complex32_t -> float,
