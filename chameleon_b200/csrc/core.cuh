@@ -12,8 +12,8 @@
 //                   float : split products on mma.sync with FP32 accumulation,
 //                           BF16x3 (x = hi + lo in bf16, hi*hi + hi*lo + lo*hi,
 //                           m16n8k16) or TF32x3 (same split in tf32, m16n8k8);
-//   blk_chol / blk_inv   Cholesky of a <= 64 x 64 block in shared memory and
-//                 the explicit inverse of its triangular factor;
+//   blk_inv       the explicit inverse of a <= 64 x 64 triangular block in
+//                 shared memory;
 //   trsm_rows / trsm_left   blocked triangular solves that apply the inverted
 //                 64 x 64 diagonal blocks, so that all bulk work is GEMM-shaped.
 //
@@ -466,36 +466,9 @@ __device__ void cta_gemm(Acc<C> &acc, const ViewT<typename C::T> &A, const ViewT
 }
 
 // ---------------------------------------------------------------------------
-// Inner-block Cholesky + triangular inverse in shared memory.
-// sD: n x n (n <= IB) column-major with leading dimension LDD, lower triangle
-// valid.  blk_chol leaves L in sD and returns 0, or the 1-based column of the
-// first non-positive pivot (LAPACK dpotrf info convention).
+// Inner-block triangular inverse in shared memory.  sD: n x n (n <= IB)
+// column-major with leading dimension LDD, lower triangle valid.
 // ---------------------------------------------------------------------------
-template <class T>
-__device__ inline int blk_chol(T *sD, int n) {
-    const int tid = threadIdx.x;
-    const int ri = tid & 63, cg = tid >> 6;   // 64 rows x 4 column classes
-    for (int j = 0; j < n; ++j) {
-        const T d = sD[j + j * LDD];
-        if (!(d > T(0))) {      // also catches NaN; uniform across the CTA
-            __syncthreads();
-            return j + 1;
-        }
-        const T ljj = sqrt(d);
-        const T inv = T(1) / ljj;
-        if (tid > j && tid < n) sD[tid + j * LDD] *= inv;
-        __syncthreads();
-        if (tid == 0) sD[j + j * LDD] = ljj;
-        // trailing update: row i = ri, columns c = j+1+cg, +4, ..., c <= i
-        if (ri > j && ri < n) {
-            const T lij = sD[ri + j * LDD];
-            for (int c = j + 1 + cg; c <= ri; c += 4) sD[ri + c * LDD] -= lij * sD[c + j * LDD];
-        }
-        __syncthreads();
-    }
-    return 0;
-}
-
 // sInv = L^{-1} for L = lower triangle of sD (n x n): row sweep, row i from
 // rows < i; 4 threads per column split the dot product (shuffle combine).
 template <class T>
@@ -600,79 +573,6 @@ __device__ inline void trsm_left(const ViewT<T> &X, int w, const ViewT<T> &L, in
         cta_gemm(acc, Inv, Xj.t(), nbk, w, nbk, smem);
         acc.store_to(Xj, nbk, w);
         cta_sync();
-    }
-}
-
-// ---------------------------------------------------------------------------
-// Diagonal-tile Cholesky (lower, on view Tv, n x n): left-looking over inner
-// blocks of IB; writes L into the lower triangle (upper untouched, as LAPACK
-// dpotrf), the inverted diagonal blocks into invd.  Returns LAPACK info.
-// Follows the semantics of CORE_dpotrf (coreblas/compute/core_zpotrf.c:75-81).
-// ---------------------------------------------------------------------------
-template <class T, int SP>
-__device__ inline int tile_potrf(const ViewT<T> &Tv, int n, T *invd, T *smem) {
-    using CP = Cfg12864<T, SP>;
-    using CD = Cfg64<T, SP>;
-    T *sD = smem + CP::SMEM_ELEMS;
-    T *sInv = sD + IB * LDD;
-    for (int jb = 0; jb < n; jb += IB) {
-        const int nbk = min(IB, n - jb);
-        Acc<CD> acc;
-        acc.zero();
-        if (jb > 0) cta_gemm(acc, Tv.sub(jb, 0), Tv.sub(jb, 0), nbk, nbk, jb, smem);
-        for (int idx = threadIdx.x; idx < nbk * nbk; idx += NT_CTA) {
-            const int r = idx % nbk, c = idx / nbk;
-            if (r >= c) sD[r + c * LDD] = *Tv.at(jb + r, jb + c);
-        }
-        __syncthreads();
-        acc.for_each([&](int r, int c, T v) {
-            if (r < nbk && c < nbk && r >= c) sD[r + c * LDD] -= v;
-        });
-        __syncthreads();
-        const int info = blk_chol(sD, nbk);
-        if (info) return jb + info;
-        blk_inv(sD, sInv, nbk);
-        for (int idx = threadIdx.x; idx < nbk * nbk; idx += NT_CTA) {
-            const int r = idx % nbk, c = idx / nbk;
-            if (r >= c) *Tv.at(jb + r, jb + c) = sD[r + c * LDD];
-        }
-        store_inv(invd + (int64_t)(jb / IB) * IB * IB, sInv);
-        cta_sync_global();
-        // panel below the inner diagonal block
-        for (int r0 = jb + nbk; r0 < n; r0 += 128) {
-            const int mr = min(128, n - r0);
-            Acc<CP> pa;
-            if (jb > 0) {
-                pa.zero();
-                cta_gemm(pa, Tv.sub(r0, 0), Tv.sub(jb, 0), mr, nbk, jb, smem);
-                pa.sub_from(Tv.sub(r0, jb), mr, nbk, false);
-                cta_sync_global();
-            }
-            pa.zero();
-            const ViewT<T> Inv{invd + (int64_t)(jb / IB) * IB * IB, 1, IB};
-            cta_gemm(pa, Tv.sub(r0, jb), Inv, mr, nbk, nbk, smem);
-            pa.store_to(Tv.sub(r0, jb), mr, nbk);
-            cta_sync_global();
-        }
-    }
-    return 0;
-}
-
-// Invert the inner diagonal blocks of an existing lower factor (n x n).
-template <class T>
-__device__ inline void tile_inv(const ViewT<T> &Tv, int n, T *invd, T *smem, bool unit = false) {
-    T *sD = smem;
-    T *sInv = sD + IB * LDD;
-    for (int jb = 0; jb < n; jb += IB) {
-        const int nbk = min(IB, n - jb);
-        for (int idx = threadIdx.x; idx < nbk * nbk; idx += NT_CTA) {
-            const int r = idx % nbk, c = idx / nbk;
-            sD[r + c * LDD] = (r >= c) ? *Tv.at(jb + r, jb + c) : T(0);
-        }
-        __syncthreads();
-        blk_inv(sD, sInv, nbk, unit);
-        store_inv(invd + (int64_t)(jb / IB) * IB * IB, sInv);
-        __syncthreads();
     }
 }
 

@@ -43,71 +43,17 @@ __device__ __forceinline__ double rsqrt_wp(double d) {
 }
 
 // Cholesky of the 32 x 32 lower block at S (shared, ld LDS) by one warp, in
-// place.  Lane i keeps row i in registers; step j (fully unrolled, so every
-// register index is static) needs one pivot shuffle, one reciprocal square
-// root and the shuffles of column j.  Entries above the diagonal are updated
-// too (no per-element predicates): they are never read back.  The block must
-// be identity-padded beyond the matrix.  Returns 0 or the 1-based column of
-// the first non-positive pivot (uniform across the warp); after a failure the
-// remaining steps run on a unit pivot so that the loop stays branch-free.
-template <class T>
-__device__ __noinline__ int warp_chol32(T *S) {
-    const int lane = threadIdx.x & 31;
-    T a[32];
-#pragma unroll
-    for (int c = 0; c < 32; ++c) a[c] = (c <= lane) ? S[lane + c * LDS] : T(0);
-    int info = 0;
-#pragma unroll
-    for (int j = 0; j < 32; ++j) {
-        T d = __shfl_sync(FULL, a[j], j);
-        if (!(d > T(0))) {   // also catches NaN
-            if (info == 0) info = j + 1;
-            d = T(1);
-        }
-        const T r = rsqrt_wp(d);
-        const T lij = (lane == j) ? d * r : a[j] * r;
-        a[j] = lij;
-#pragma unroll
-        for (int c = j + 1; c < 32; ++c) a[c] -= lij * __shfl_sync(FULL, lij, c);
-    }
-#pragma unroll
-    for (int c = 0; c < 32; ++c)
-        if (c <= lane) S[lane + c * LDS] = a[c];
-    __syncwarp();
-    return info;
-}
-
-// X = L^-1 for the 32 x 32 lower block L at S (shared, ld LDS), one warp: lane
-// c solves L x = e_c, right-looking (x_i final, then column i of L updates the
-// rest), with the diagonal reciprocals computed up front; the loads of one
-// column of L do not depend on x and issue together.  X is written in full
-// (zeros above the diagonal) at Xs (shared, ld LDS).
-template <class T>
-__device__ __noinline__ void warp_trinv32(const T *S, T *Xs) {
-    const int lane = threadIdx.x & 31;
-    T rd[32], x[32];
-#pragma unroll
-    for (int k = 0; k < 32; ++k) {
-        rd[k] = T(1) / S[k + k * LDS];
-        x[k] = (k == lane) ? T(1) : T(0);
-    }
-#pragma unroll
-    for (int i = 0; i < 32; ++i) {
-        x[i] *= rd[i];
-#pragma unroll
-        for (int k = i + 1; k < 32; ++k) x[k] -= S[k + i * LDS] * x[i];
-    }
-#pragma unroll
-    for (int k = 0; k < 32; ++k) Xs[k + lane * LDS] = x[k];
-    __syncwarp();
-}
-
-// Rolled forms of the two warp kernels above: the same arithmetic per entry,
-// in a loop of 32 identical steps whose code (~1-2 KB) stays in the
-// instruction cache.  Register indices stay static by shifting: at step j,
-// slot k of a lane holds the entry of column (row) j + k, and the update of
-// slot k writes slot k - 1, so slot 0 is always the current column (row) and
-// the shift costs no moves.
+// place: lane i keeps row i in registers.  Each of the 32 steps needs the
+// pivot, one reciprocal square root and the broadcast of column j.  Entries
+// above the diagonal are updated too (no per-element predicates): they are
+// never read back.  The block must be identity-padded beyond the matrix.
+// Returns 0 or the 1-based column of the first non-positive pivot (uniform
+// across the warp); after a failure the remaining steps run on a unit pivot
+// so that the loop stays branch-free.  The loop is rolled (its ~1-2 KB of
+// code stays in the instruction cache); register indices stay static by
+// shifting: at step j, slot k of a lane holds the entry of column (row)
+// j + k, and the update of slot k writes slot k - 1, so slot 0 is always the
+// current column (row) and the shift costs no moves.
 template <class T>
 __device__ __noinline__ int warp_chol32r(T *S, T *bc) {
     const int lane = threadIdx.x & 31;
