@@ -123,9 +123,10 @@ __global__ void sym_diag_kernel(SymTiles a) {
     }
 }
 
-// Residual GEMM tile: 128 x 64 FP64 outputs, 3-stage cp.async pipeline (the
-// block row of A is a long K sweep).
-using CfgRes = GemmCfg<double, 128, 64, 4, 2, SPLIT_BF16X3, 3>;
+// Residual GEMM tile: 128 x 64 FP64 outputs, 2-stage cp.async pipeline, two
+// CTAs per SM (16 warps feed the DMMA pipe; 111 KB of stages each).
+using CfgRes = GemmCfg<double, 128, 64, 4, 2, SPLIT_BF16X3, 2>;
+constexpr int RES_CTAS_PER_SM = 2;
 
 // R = B - A X for symmetric A (one triangle stored), FP64 on DMMA.  One CTA
 // per (tile row m, 128-row block, 64-column block of the right-hand sides, K
@@ -133,7 +134,7 @@ using CfgRes = GemmCfg<double, 128, 64, 4, 2, SPLIT_BF16X3, 3>;
 // block row of A.  ksplit == 1: writes R and the per-column max |R|; else the
 // partial product goes to part[kp] (N x nrhs, ld N) for residual_reduce_kernel,
 // which adds the parts in a fixed order (deterministic).
-__global__ void __launch_bounds__(NT_CTA, 1) sym_residual_kernel(SymTiles a, TileMapD xb, TileMapD bb, TileMapD rb,
+__global__ void __launch_bounds__(NT_CTA, RES_CTAS_PER_SM) sym_residual_kernel(SymTiles a, TileMapD xb, TileMapD bb, TileMapD rb,
                                                                  int nrhs, int nrb, int ncb, int ksplit,
                                                                  double *part, unsigned long long *rmax) {
     extern __shared__ __align__(128) double smem[];
@@ -438,7 +439,7 @@ static int residual(CHAM_desc_t *A, cham_uplo_t uplo, CHAM_desc_t *B, CHAM_desc_
     const int nrb = (A->nb + 127) / 128;
     const int ncb = X->nt * ((X->nb + 63) / 64);
     // split the K sweep so that the working CTAs fill whole waves of SMs
-    const int sms = ctx().num_sms;
+    const int sms = ctx().num_sms * RES_CTAS_PER_SM;
     int nwork = 0;
     for (int mm = 0; mm < A->nt; ++mm) nwork += (desc_tile_rows(A, mm) + 127) / 128;
     nwork *= (nrhs + 63) / 64;
