@@ -718,10 +718,14 @@ def b200_arm(args, world, rank, local):
     if args.compare_fp64 and rank == 0:
         dA2 = cb.Desc.create(N, N, NB)
         dB2 = cb.Desc.create(N, nrhs, NB)
-        cb.dplgsy_Tile(float(N), cb.ChamUpperLower, dA2, SEED_A)
-        cb.dplrnt_Tile(dB2, SEED_B)
-        L.CHAM_B200_Event_Record(2)
-        assert cb.dposv_Tile(cb.ChamLower, dA2, dB2) == 0
+        # one untimed call first (the task list of this shape is built and
+        # cached on the first call, as for the mixed arm's warm-up steps)
+        for timed in (False, True):
+            cb.dplgsy_Tile(float(N), cb.ChamUpperLower, dA2, SEED_A)
+            cb.dplrnt_Tile(dB2, SEED_B)
+            if timed:
+                L.CHAM_B200_Event_Record(2)
+            assert cb.dposv_Tile(cb.ChamLower, dA2, dB2) == 0
         L.CHAM_B200_Event_Record(3)
         fms = L.CHAM_B200_Event_Elapsed(2, 3)
         fp64 = {"tflops": flops / (fms * 1e-3) / 1e12, "ms": fms}

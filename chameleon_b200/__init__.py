@@ -38,6 +38,7 @@ CHAMELEON_B200_UPD_GROUP_F64 = 109
 CHAMELEON_B200_UPD_GROUP_F32 = 110
 CHAMELEON_B200_UPD_GROUP_TC = 111
 CHAMELEON_B200_FACTOR_NB = 112
+CHAMELEON_B200_UPD_TAIL_F64 = 113
 PREC_FP64, PREC_FP32, PREC_BF16X3 = 0, 1, 2
 CHAMELEON_SUCCESS = 0
 CHAMELEON_ERR_NOT_INITIALIZED = -101

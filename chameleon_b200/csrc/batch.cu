@@ -66,8 +66,15 @@ __global__ void __launch_bounds__(NT_CTA, MINB) posv_batch_kernel(const BatchIte
             const ViewT<T> X{B + it.b_off, 1, it.ldb};
             for (int c0 = 0; c0 < it.nrhs; c0 += IB) {
                 const int w = min(IB, it.nrhs - c0);
-                trsm_left<T, SPLIT_BF16X3>(X.sub(0, c0), w, Lv, it.n, invd, false, smem);
-                trsm_left<T, SPLIT_BF16X3>(X.sub(0, c0), w, Lv, it.n, invd, true, smem);
+                // a narrow last block (few right-hand sides, the common case)
+                // runs on the narrow tile instead of padding it to 64 columns
+                if (w <= Cfg64N<T>::BN) {
+                    trsm_left<T, SPLIT_BF16X3, Cfg64N<T>>(X.sub(0, c0), w, Lv, it.n, invd, false, smem);
+                    trsm_left<T, SPLIT_BF16X3, Cfg64N<T>>(X.sub(0, c0), w, Lv, it.n, invd, true, smem);
+                } else {
+                    trsm_left<T, SPLIT_BF16X3>(X.sub(0, c0), w, Lv, it.n, invd, false, smem);
+                    trsm_left<T, SPLIT_BF16X3>(X.sub(0, c0), w, Lv, it.n, invd, true, smem);
+                }
             }
         }
         cta_sync_global();

@@ -499,6 +499,10 @@ int CHAMELEON_Set(int param, int value) {
                                                : param == CHAMELEON_B200_UPD_GROUP_F32 ? c.kgroup_f32 : c.kgroup_tc) =
             value;
         return 0;
+    case CHAMELEON_B200_UPD_TAIL_F64:
+        if (value < 0 || value > 8) return CHAMELEON_ERR_ILLEGAL_VALUE;
+        c.utail_f64 = value;
+        return 0;
     case CHAMELEON_B200_FACTOR_NB:
         if (value < 0 || (value > 0 && value % 64 != 0)) return CHAMELEON_ERR_ILLEGAL_VALUE;
         c.factor_nb = value;
@@ -529,6 +533,7 @@ int CHAMELEON_Get(int param, int *value) {
     case CHAMELEON_B200_UPD_GROUP_F32: *value = c.kgroup_f32; return 0;
     case CHAMELEON_B200_UPD_GROUP_TC: *value = c.kgroup_tc; return 0;
     case CHAMELEON_B200_FACTOR_NB: *value = c.factor_nb; return 0;
+    case CHAMELEON_B200_UPD_TAIL_F64: *value = c.utail_f64; return 0;
     }
     return CHAMELEON_ERR_ILLEGAL_VALUE;
 }

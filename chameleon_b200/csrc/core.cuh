@@ -143,9 +143,12 @@ __device__ __forceinline__ uint64_t globaltimer() {
 // ---------------------------------------------------------------------------
 template <class T>
 struct Geom;
+// Fragment reads of an MN-contiguous stage: lanes (g, t) of one 16-lane phase
+// read rows g (0..3) of k rows t (0..3); a leading dimension of 4 mod 16
+// doubles (8 mod 32 floats) puts the four k rows on disjoint banks.
 template <>
 struct Geom<double> {
-    static constexpr int VEC = 2, PAD = 8, LDK = KC + 4;
+    static constexpr int VEC = 2, PAD = 4, LDK = KC + 4;
 };
 template <>
 struct Geom<float> {
@@ -245,6 +248,11 @@ template <class T, int SP = SPLIT_BF16X3>
 using Cfg12864 = GemmCfg<T, 128, 64, 4, 2, SP>;  // panel rows x one inner block
 template <class T, int SP = SPLIT_BF16X3>
 using Cfg64 = GemmCfg<T, 64, 64, 2, 4, SP>;      // inner block x inner block
+// inner block x a narrow right-hand-side block: 8 columns (one DMMA n8 tile per
+// warp) for double, 16 for float (one m16n8 tile per warp)
+template <class T, int SP = SPLIT_BF16X3>
+using Cfg64N = typename std::conditional<std::is_same<T, double>::value, GemmCfg<T, 64, 8, 8, 1, SP>,
+                                         GemmCfg<T, 64, 16, 4, 2, SP>>::type;
 
 template <class C_>
 struct Acc {
@@ -543,10 +551,9 @@ __device__ inline void trsm_rows(const ViewT<T> &X, int rows, const ViewT<T> &L,
 // The solves of compute/pztrsm.c:58-200 (Left, Lower, {NoTrans, Trans}) on
 // one diagonal tile.
 // ---------------------------------------------------------------------------
-template <class T, int SP>
+template <class T, int SP, class C = Cfg64<T, SP>>
 __device__ inline void trsm_left(const ViewT<T> &X, int w, const ViewT<T> &L, int n, const T *invd, bool trans,
                                  T *smem) {
-    using C = Cfg64<T, SP>;
     const int nblk = (n + IB - 1) / IB;
     for (int s = 0; s < nblk; ++s) {
         const int b = trans ? (nblk - 1 - s) : s;

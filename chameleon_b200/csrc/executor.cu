@@ -47,18 +47,23 @@ static const Calib kCalib[3] = {
     {4.2, 2.7, 0.92, 1.9, 4.0, 0.6},   // FP32, tcgen05 updates, full-inverse substitutions (row-block sub-tasks)
 };
 
+// Single-panel update groups at the end of each tile column, per cost profile
+// (CHAMELEON_B200_UPD_TAIL_F64 for the FP64 path).
+int upd_tail(int prof) { return prof == PROF_FP64 ? ctx().utail_f64 : UPD_TAIL; }
+
 struct Shape {
     int mode, N, NB, nrhs, NBB, P, prof, G;   // G: update group size (upd_group_of)
     int h2d_gbs;                              // MODE_CAST: host-to-device bandwidth of the model (GB/s)
+    int tail = UPD_TAIL;                      // single-panel groups at the end of each column
     bool operator==(const Shape &o) const {
         return mode == o.mode && N == o.N && NB == o.NB && nrhs == o.nrhs && NBB == o.NBB && P == o.P &&
-               prof == o.prof && G == o.G && h2d_gbs == o.h2d_gbs;
+               prof == o.prof && G == o.G && h2d_gbs == o.h2d_gbs && tail == o.tail;
     }
 };
 struct ShapeHash {
     size_t operator()(const Shape &s) const {
         size_t h = 1469598103934665603ull;
-        for (int v : {s.mode, s.N, s.NB, s.nrhs, s.NBB, s.P, s.prof, s.G, s.h2d_gbs})
+        for (int v : {s.mode, s.N, s.NB, s.nrhs, s.NBB, s.P, s.prof, s.G, s.h2d_gbs, s.tail})
             h = (h ^ (size_t)v) * 1099511628211ull;
         return h;
     }
@@ -179,7 +184,7 @@ std::vector<Task> build_order(const Shape &s) {
             // (upd_group_of): they become ready with this step's panel solves
             for (int n = k + 1; n < NT; ++n) {
                 int k0, cnt, gi;
-                upd_group_of(n, k, s.G, &k0, &cnt, &gi);
+                upd_group_of(n, k, s.G, s.tail, &k0, &cnt, &gi);
                 if (k0 + cnt - 1 != k) continue;
                 for (int m = n; m < NT; ++m) {
                     const int sub = (m == n) ? nbi(m) * (nbi(m) + 1) / 2 : nbi(m) * nbi(n);
@@ -433,7 +438,9 @@ int run_cholesky_dag(int mode, cham_uplo_t uplo, CHAM_desc_t *A, CHAM_desc_t *B,
     const bool tc = f32 && split == SPLIT_BF16X3 && (mode & MODE_FACT) && (NB % tc05::BK == 0) && NT > 1 &&
                     c.use_tcgen05;
     int rc = 0;
-    const int grid = (grid_req > 0) ? std::min(grid_req, c.num_sms) : c.num_sms;
+    // grid_req counts SMs; FP64 places two executor CTAs on each
+    const int cps = f32 ? 1 : 2;
+    const int grid = cps * ((grid_req > 0) ? std::min(grid_req, c.num_sms) : c.num_sms);
     const int prof = !f32 ? PROF_FP64 : (tc ? PROF_F32_TC05 : PROF_F32_MMA);
     const bool full_inv = f32 && c.rec_tile && NB <= (64 << rec::MAX_LVL);
     // FP32 substitutions with full diagonal-tile inverses: computed off the
@@ -462,7 +469,7 @@ int run_cholesky_dag(int mode, cham_uplo_t uplo, CHAM_desc_t *A, CHAM_desc_t *B,
     // update group size: fused k steps amortize the C round trip and the
     // dispatch of an update over G panels (CHAMELEON_B200_UPD_GROUP per path)
     const int G = t_given ? 1 : std::max(1, prof == PROF_FP64 ? c.kgroup_f64 : (tc ? c.kgroup_tc : c.kgroup_f32));
-    Shape sh{mode, canonN, NB, canonR, NBB, grid, prof, G, cin ? std::max(1, cin->h2d_gbs) : 0};
+    Shape sh{mode, canonN, NB, canonR, NBB, grid, prof, G, cin ? std::max(1, cin->h2d_gbs) : 0, upd_tail(prof)};
     const Schedule *sch = t_given ? t_given : get_schedule(sh);
     if (!sch) return CHAMELEON_ERR_OUT_OF_RESOURCES;
     const int NIB = (NB + IB - 1) / IB;
@@ -542,6 +549,7 @@ int run_cholesky_dag(int mode, cham_uplo_t uplo, CHAM_desc_t *A, CHAM_desc_t *B,
     p.trace = (g_trace_buf && g_trace_cap >= p.ntasks) ? g_trace_buf : nullptr;
     p.wait_budget_ns = (unsigned long long)c.wait_budget_us * 1000ull;
     p.kgroup = G;
+    p.utail = sh.tail;
     if (tc) {
         p.split_nrb = (NB + SUBB - 1) / SUBB;
         p.split_nkc = NB / tc05::BK;
@@ -620,7 +628,8 @@ extern "C" int CHAM_B200_Schedule_Build(int mode, int N, int NB, int nrhs, int N
                                         void *out, int cap) {
     using namespace chb;
     const std::vector<Task> t =
-        build_order(Shape{mode, N, NB, nrhs, NBB, workers, prof, std::max(1, kgroup), (mode & MODE_CAST) ? 50 : 0});
+        build_order(Shape{mode, N, NB, nrhs, NBB, workers, prof, std::max(1, kgroup), (mode & MODE_CAST) ? 50 : 0,
+                          upd_tail(prof)});
     const int n = std::min<int>((int)t.size(), cap);
     memcpy(out, t.data(), sizeof(Task) * (size_t)n);
     return n;
@@ -628,7 +637,8 @@ extern "C" int CHAM_B200_Schedule_Build(int mode, int N, int NB, int nrhs, int N
 // Number of tasks of the schedule of a given shape (for tests and tracing).
 extern "C" int CHAM_B200_Schedule_Size(int mode, int N, int NB, int nrhs, int NBB, int workers, int prof, int kgroup) {
     using namespace chb;
-    return (int)build_order(Shape{mode, N, NB, nrhs, NBB, workers, prof, std::max(1, kgroup), (mode & MODE_CAST) ? 50 : 0})
+    return (int)build_order(Shape{mode, N, NB, nrhs, NBB, workers, prof, std::max(1, kgroup),
+                                  (mode & MODE_CAST) ? 50 : 0, upd_tail(prof)})
         .size();
 }
 

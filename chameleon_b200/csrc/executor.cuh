@@ -38,20 +38,20 @@ struct Task {
 };
 
 // Update groups of tile column n: the panels k < n that update tile (m, n),
-// m >= n, are applied in groups.  The last UPD_TAIL panels (n-2, n-1) are
-// groups of their own: they are on the critical path of steps n-1 and n.  The
-// panels before them form groups of G aligned at the end (the first group
-// takes the remainder), so that every step completes a group for 1/G of the
-// columns and the update work arrives evenly instead of in bursts.
+// m >= n, are applied in groups.  The last `tail` panels (default UPD_TAIL:
+// n-2, n-1) are groups of their own: they are on the critical path of steps
+// n-1 and n.  The panels before them form groups of G aligned at the end (the
+// first group takes the remainder), so that every step completes a group for
+// 1/G of the columns and the update work arrives evenly instead of in bursts.
 constexpr int UPD_TAIL = 2;
-__host__ __device__ __forceinline__ int upd_ngroups(int n, int G) {
-    if (n <= UPD_TAIL) return n > 0 ? n : 0;
-    return (n - UPD_TAIL + G - 1) / G + UPD_TAIL;
+__host__ __device__ __forceinline__ int upd_ngroups(int n, int G, int tail) {
+    if (n <= tail) return n > 0 ? n : 0;
+    return (n - tail + G - 1) / G + tail;
 }
 // The group of column n (n > k) that panel k belongs to: first panel, panel
 // count and index.
-__host__ __device__ __forceinline__ void upd_group_of(int n, int k, int G, int *k0, int *cnt, int *idx) {
-    const int m = n > UPD_TAIL ? n - UPD_TAIL : 0;   // panels in groups of G
+__host__ __device__ __forceinline__ void upd_group_of(int n, int k, int G, int tail, int *k0, int *cnt, int *idx) {
+    const int m = n > tail ? n - tail : 0;   // panels in groups of G
     if (k >= m) {
         *k0 = k;
         *cnt = 1;
@@ -141,6 +141,7 @@ struct ExecParams {
     uint8_t *split;
     int split_nrb, split_nkc;   // 128-row blocks and 64-wide k chunks per panel tile
     int kgroup;                 // update group size G (upd_ngroups / upd_group_of)
+    int utail;                  // single-panel update groups at the end of each column
     // MODE_CAST: the FP64 source (column-major, ld csrc_ld) of the stored
     // triangle; tile column q of it has arrived once carrive[q] >= cepoch
     // (written by the copy engine after the column's data); castDone counts

@@ -20,6 +20,13 @@ namespace chb {
 // ---------------------------------------------------------------------------
 // Device
 // ---------------------------------------------------------------------------
+// CTAs of the persistent executor per SM: FP64 runs two (16 warps feed the
+// DMMA pipe; every FP64 task fits 112 KB of shared memory), FP32 one.
+template <class T, bool TC>
+constexpr int dag_ctas_per_sm() {
+    return (sizeof(T) == 8 && !TC) ? 2 : 1;
+}
+
 template <class T>
 struct Dims {
     const ExecParams &p;
@@ -79,12 +86,12 @@ __device__ Deps task_deps(const Task &t, const ExecParams &p, const Dims<T> &d) 
     };
     switch (t.kind) {
     case TK_POTRF:
-        need(0, &p.updA[t.k + p.NT * t.k], upd_ngroups(t.k, p.kgroup) * d.S(t.k, t.k));
+        need(0, &p.updA[t.k + p.NT * t.k], upd_ngroups(t.k, p.kgroup, p.utail) * d.S(t.k, t.k));
         if ((p.mode & MODE_CAST) && t.k == 0) need(1, &p.castDone[0], 1);
         break;
     case TK_TRSM:
         need(0, &p.panA[t.k + p.NT * t.k], 1);
-        need(1, &p.updA[t.m + p.NT * t.k], upd_ngroups(t.k, p.kgroup) * d.S(t.m, t.k));
+        need(1, &p.updA[t.m + p.NT * t.k], upd_ngroups(t.k, p.kgroup, p.utail) * d.S(t.m, t.k));
         // tile column 0 has no update before its panel solve: wait for its cast
         if ((p.mode & MODE_CAST) && t.k == 0) need(1, &p.castDone[t.m], 1);
         break;
@@ -250,7 +257,9 @@ __device__ void run_task(const Task &t, const ExecParams &p, const Dims<T> &d, T
             else if (d.tm(t.k) <= psm::MAXN) info = psm::potrf(d.A(t.k, t.k), d.tm(t.k), d.inv(t.k), smem, ph);
             else info = rec::tile_potrf_blk<T, SP>(d.A(t.k, t.k), d.tm(t.k), d.inv(t.k), smem, ph);
         } else {
-            info = rec::tile_potrf_blk<T, SP>(d.A(t.k, t.k), d.tm(t.k), d.inv(t.k), smem, ph);
+            // FP64: the lean form (64-row panels, leaf on the staging area) fits
+            // the two-CTAs-per-SM shared memory
+            info = rec::tile_potrf_blk<T, SP, 64, true>(d.A(t.k, t.k), d.tm(t.k), d.inv(t.k), smem, ph);
         }
         if (info && threadIdx.x == 0) {
             atomicMin(&p.st->info, t.k * p.NB + info);
@@ -345,12 +354,28 @@ __device__ void run_task(const Task &t, const ExecParams &p, const Dims<T> &d, T
             }
             break;
         }
-        Acc<Cfg128<T, SP>> acc;
-        acc.zero();
-        for (int k = t.k; k < t.k + t.bn; ++k)
-            cta_gemm(acc, d.A(t.m, k).sub(bi * SUBB, 0), d.A(t.n, k).sub(bj * SUBB, 0), rows, cols, d.tm(k),
-                     smem);
-        acc.sub_from(C, rows, cols, diag);
+        if constexpr (sizeof(T) == 8) {
+            // FP64: two 128 x 64 halves (the 111 KB of stages that let two
+            // CTAs share an SM); on a diagonal block the second half is the
+            // 64 x 64 lower block of rows and columns 64..127
+            for (int h = 0; h < 2; ++h) {
+                const int c0 = 64 * h, r0 = diag ? c0 : 0;
+                if (c0 >= cols || r0 >= rows) break;
+                Acc<Cfg12864<T, SP>> acc;
+                acc.zero();
+                for (int k = t.k; k < t.k + t.bn; ++k)
+                    cta_gemm(acc, d.A(t.m, k).sub(bi * SUBB + r0, 0), d.A(t.n, k).sub(bj * SUBB + c0, 0), rows - r0,
+                             min(64, cols - c0), d.tm(k), smem);
+                acc.sub_from(C.sub(r0, c0), rows - r0, min(64, cols - c0), diag);
+            }
+        } else {
+            Acc<Cfg128<T, SP>> acc;
+            acc.zero();
+            for (int k = t.k; k < t.k + t.bn; ++k)
+                cta_gemm(acc, d.A(t.m, k).sub(bi * SUBB, 0), d.A(t.n, k).sub(bj * SUBB, 0), rows, cols, d.tm(k),
+                         smem);
+            acc.sub_from(C, rows, cols, diag);
+        }
         break;
     }
     case TK_XINV:
@@ -392,9 +417,15 @@ __device__ void run_task(const Task &t, const ExecParams &p, const Dims<T> &d, T
                 break;
             }
         }
-        for (int c0 = 0; c0 < w; c0 += IB)
-            trsm_left<T, SP>(X.sub(0, c0), min(IB, w - c0), d.A(t.k, t.k), d.tm(t.k), d.inv(t.k),
-                      t.kind == TK_BWD_TRSM, smem);
+        for (int c0 = 0; c0 < w; c0 += IB) {
+            const int wc = min(IB, w - c0);
+            if (wc <= Cfg64N<T, SP>::BN)   // few right-hand sides: the narrow tile
+                trsm_left<T, SP, Cfg64N<T, SP>>(X.sub(0, c0), wc, d.A(t.k, t.k), d.tm(t.k), d.inv(t.k),
+                                                t.kind == TK_BWD_TRSM, smem);
+            else
+                trsm_left<T, SP>(X.sub(0, c0), wc, d.A(t.k, t.k), d.tm(t.k), d.inv(t.k), t.kind == TK_BWD_TRSM,
+                                 smem);
+        }
         break;
     }
     case TK_FWD_UPD:
@@ -445,7 +476,7 @@ __device__ inline int *task_counter(const Task &t, const ExecParams &p) {
 }
 
 template <class T, int SP, bool TC>
-__global__ void __launch_bounds__(NT_CTA, 1) cholesky_dag_kernel(ExecParams p) {
+__global__ void __launch_bounds__(NT_CTA, dag_ctas_per_sm<T, TC>()) cholesky_dag_kernel(ExecParams p) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     // 1024-byte aligned base: the tcgen05 stages need it; other tasks share it
     uint8_t *stage = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -524,6 +555,8 @@ __global__ void __launch_bounds__(NT_CTA, 1) cholesky_dag_kernel(ExecParams p) {
 
 template <class T, int SP, bool TC>
 constexpr size_t dag_smem_bytes() {
+    // FP64: two CTAs per SM, each task within a 128 x 64 DMMA tile's stages
+    if (sizeof(T) == 8 && !TC) return Cfg12864<T, SP>::SMEM_BYTES + 1024;
     // one CTA per SM: every variant may use the shared memory its largest task needs
     // (the tcgen05 stages; FP32: the shared-memory diagonal-tile factorization)
     size_t b = tile_smem_bytes<T, SP>() + 1024;

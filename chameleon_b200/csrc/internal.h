@@ -35,7 +35,8 @@ struct Context {
     bool potrf_cta = false;        // one executor CTA dedicated to the diagonal-tile factorizations
     // update group sizes (panels applied per trailing-update task) per path:
     // FP64 DMMA, FP32 split products on mma.sync, FP32 on tcgen05
-    int kgroup_f64 = 1, kgroup_f32 = 1, kgroup_tc = 8;
+    int kgroup_f64 = 8, kgroup_f32 = 1, kgroup_tc = 8;
+    int utail_f64 = 2;             // single-panel update groups closing each tile column, FP64 path
     // tile size of the mixed solver's FP32 copy of A (0: A's own tile size);
     // used when it divides A's tile size
     int factor_nb = 256;

@@ -69,11 +69,13 @@ typedef enum {
                                              diagonal tiles, kept across refinement solves (default) */
 #define CHAMELEON_B200_POTRF_CTA      108 /* 1: one executor CTA runs all diagonal-tile
                                              factorizations; 0: any CTA (default) */
-#define CHAMELEON_B200_UPD_GROUP_F64  109 /* panels applied per trailing-update task, FP64 path (default 1) */
+#define CHAMELEON_B200_UPD_GROUP_F64  109 /* panels applied per trailing-update task, FP64 path (default 8) */
 #define CHAMELEON_B200_UPD_GROUP_F32  110 /* the same, FP32 split products on mma.sync (default 1) */
 #define CHAMELEON_B200_UPD_GROUP_TC   111 /* the same, FP32 BF16x3 on tcgen05 (default 8) */
 #define CHAMELEON_B200_FACTOR_NB      112 /* tile size of the mixed solver's FP32 factorization;
                                              0: the tile size of A (default 256 when it divides A's) */
+#define CHAMELEON_B200_UPD_TAIL_F64   113 /* FP64 path: the last panels of each tile column applied
+                                             one per update task (0..8, default 2) */
 
 /* Factorization precisions for CHAMELEON_B200_PRECISION */
 #define CHAM_B200_PREC_FP64   0
