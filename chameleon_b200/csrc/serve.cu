@@ -95,6 +95,7 @@ struct Slot {
 
 struct Server {
     int small_n = 512;
+    double age_s = 0.05;   // a queued request older than this is served next (CHAMELEON_B200_SERVE_AGE_MS)
     size_t budget = 0;
     size_t used = 0;   // bytes of running requests + kept factors (guarded by mu)
     bool stop = false;
@@ -118,7 +119,6 @@ struct Server {
 int choose_nb(int N) { return N >= 4096 ? 512 : 256; }
 
 constexpr int kReserveSMs = 16;        // SMs left to short kernels next to the slots' launches
-constexpr double kAgeSeconds = 0.05;   // a queued request older than this is served next
 
 size_t kept_bytes(int N) {
     const size_t n = N, nb = choose_nb(N), nt = (n + nb - 1) / nb;
@@ -328,12 +328,12 @@ void slot_worker(Server *sv, int idx) {
             std::unique_lock<std::mutex> lk(sv->mu);
             // Shortest first (a solve with a kept factor counts as a quarter of
             // its order), so that small requests do not wait behind large
-            // ones; a request that has waited kAgeSeconds goes next whatever
+            // ones; a request that has waited age_s goes next whatever
             // its size, so that large ones are not starved.
             size_t pick = 0;
             auto choose = [&]() {
                 pick = 0;
-                if (now_s() - sv->large_q.front()->t_submit > kAgeSeconds) return;
+                if (now_s() - sv->large_q.front()->t_submit > sv->age_s) return;
                 auto cost = [](const CHAM_b200_request_t *q) { return q->A ? (double)q->N : 0.25 * q->N; };
                 for (size_t i = 1; i < sv->large_q.size(); ++i)
                     if (cost(sv->large_q[i]) < cost(sv->large_q[pick])) pick = i;
@@ -449,6 +449,10 @@ int CHAM_B200_Serve_Create(CHAM_b200_server_t *out, int slots, double hbm_budget
     if (!out || slots < 1 || slots > 16 || small_n < 0 || small_n > 4096) return CHAMELEON_ERR_ILLEGAL_VALUE;
     Server *sv = new Server();
     sv->small_n = small_n;
+    if (const char *e = getenv("CHAMELEON_B200_SERVE_AGE_MS")) {
+        const double ms = atof(e);
+        if (ms > 0) sv->age_s = ms * 1e-3;
+    }
     size_t fr = 0, tot = 0;
     cudaMemGetInfo(&fr, &tot);
     sv->budget = hbm_budget_bytes > 0 ? (size_t)hbm_budget_bytes : (size_t)(0.8 * (double)fr);
