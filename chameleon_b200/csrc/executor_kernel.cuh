@@ -479,7 +479,10 @@ template <class T, int SP, bool TC>
 __global__ void __launch_bounds__(NT_CTA, dag_ctas_per_sm<T, TC>()) cholesky_dag_kernel(ExecParams p) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     // 1024-byte aligned base: the tcgen05 stages need it; other tasks share it
-    uint8_t *stage = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    // (an offset added to the __shared__ array, not a rounded integer: the
+    // pointer stays visibly in shared memory, so every access through it is
+    // an ld/st.shared rather than a generic load or store)
+    uint8_t *stage = smem_raw + ((1024u - (unsigned)(reinterpret_cast<uintptr_t>(smem_raw) & 1023u)) & 1023u);
     T *smem = reinterpret_cast<T *>(stage);
     __shared__ int s_task;
     __shared__ int s_ok;

@@ -28,7 +28,10 @@ __global__ void __launch_bounds__(NT_CTA, 1) tc05_test_kernel(const uint8_t *a, 
                                                               int *err) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     __shared__ tc05::Smem tsm;
-    uint8_t *stage = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    // (an offset added to the __shared__ array, not a rounded integer: the
+    // pointer stays visibly in shared memory, so every access through it is
+    // an ld/st.shared rather than a generic load or store)
+    uint8_t *stage = smem_raw + ((1024u - (unsigned)(reinterpret_cast<uintptr_t>(smem_raw) & 1023u)) & 1023u);
     tc05::init(&tsm);
     // two GEMMs in a row exercise the phase bookkeeping across tasks
     for (int rep = 0; rep < 2; ++rep) {
